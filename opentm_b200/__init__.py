@@ -1,0 +1,291 @@
+"""opentm_b200 -- B200-native thermal homogenization hot path of OpenTM.
+
+Python mirror of the reference's host interface (``Homogenization_H``, ``OCOptimizer``,
+``MMAOptimizer``, the density-filter chain) over the C ABI of ``libopentm_b200.so``.
+Device arrays are torch CUDA tensors (or raw device pointers); torch is used only for device
+memory and streams. Every call goes to the sm_100a CUDA library; if it is not built, the
+calls raise -- there is no CPU fallback.
+
+Fields are lexicographic with x fastest: a cell of reso (nx, ny, nz) is a torch tensor of
+shape (nz, ny, nx) (or (nz, ny, pitchT) for pitched fields).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import OtmError, check, default_config, i3, lib
+
+__all__ = [
+    "HomoConfig", "Homogenization_H", "OCOptimizer", "MMAOptimizer", "DensityFilter", "OtmError", "lib",
+    "WEIGHT_SPLINE4", "WEIGHT_LINEAR", "filter_forward", "filter_backward",
+]
+
+WEIGHT_SPLINE4 = 0
+WEIGHT_LINEAR = 1
+
+
+def _ptr(t) -> int:
+    if t is None:
+        return None
+    if isinstance(t, int):
+        return t
+    if not t.is_cuda:
+        raise ValueError("device arrays must be CUDA tensors")
+    return t.data_ptr()
+
+
+def _stream(stream=None):
+    if stream is not None:
+        return stream if isinstance(stream, int) else stream.cuda_stream
+    import torch
+    return torch.cuda.current_stream().cuda_stream
+
+
+@dataclass
+class HomoConfig:
+    """Mirror of cfg::HomoConfig (cmdline.h:12-33) restricted to the solve, with
+    init() defaults (cmdline.cpp:4-35)."""
+    reso: tuple = (128, 128, 128)
+    femRelThres: float = 0.01
+    max_iter: int = 200
+    pre_smooth: int = 1
+    post_smooth: int = 1
+    solver: str = "pcg"
+    precision: str = "fp32"
+    coarsest_max_dof: int = 64
+    power_penal: float = 1.0
+    warm_start: bool = True
+    check_every: int = 4
+    use_graphs: bool = True
+
+    def to_c(self) -> _lib.Config:
+        reso = self.reso if not isinstance(self.reso, int) else (self.reso,) * 3
+        return default_config(
+            reso, fem_rel_thres=float(self.femRelThres), max_iter=int(self.max_iter),
+            pre_smooth=int(self.pre_smooth), post_smooth=int(self.post_smooth), solver=self.solver,
+            precision=self.precision, coarsest_max_dof=int(self.coarsest_max_dof),
+            power_penal=float(self.power_penal), warm_start=int(bool(self.warm_start)),
+            check_every=int(self.check_every), use_graphs=int(bool(self.use_graphs)))
+
+
+class Homogenization_H:
+    """Homogenization_H (homogenization/homogenization.h:15-30) on the B200 library."""
+
+    def __init__(self, config: HomoConfig, stream=None):
+        self.config = config
+        self._h = ctypes.c_void_p()
+        check(lib().otm_homo_create(ctypes.byref(config.to_c()), ctypes.byref(self._h)), "otm_homo_create")
+        reso = config.reso if not isinstance(config.reso, int) else (config.reso,) * 3
+        self.reso = tuple(int(r) for r in reso)
+        if stream is not None:
+            self.set_stream(stream)
+
+    def close(self):
+        if self._h:
+            lib().otm_homo_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream):
+        check(lib().otm_homo_set_stream(self._h, ctypes.c_void_p(_stream(stream))), "otm_homo_set_stream")
+
+    def _sync_stream(self):
+        self.set_stream(None)
+
+    @property
+    def n_cells(self) -> int:
+        return self.reso[0] * self.reso[1] * self.reso[2]
+
+    def set_tolerance(self, tol: float):
+        check(lib().otm_homo_set_tolerance(self._h, float(tol)), "otm_homo_set_tolerance")
+
+    def update(self, rho, pitchT: int = -1):
+        """Homogenization_H::update(float* rho, int pitchT) (homogenization.cpp:76-81)."""
+        self._sync_stream()
+        check(lib().otm_homo_update(self._h, ctypes.c_void_p(_ptr(rho)), int(pitchT)), "otm_homo_update")
+
+    def solve(self, allow_not_converged: bool = False) -> _lib.SolveStats:
+        self._sync_stream()
+        st = _lib.SolveStats()
+        allow = (0, _lib.OTM_ERR_NOT_CONVERGED) if allow_not_converged else (0,)
+        check(lib().otm_homo_solve(self._h, ctypes.byref(st)), "otm_homo_solve", allow)
+        return st
+
+    def heatMatrix(self, allow_not_converged: bool = False) -> np.ndarray:
+        """Homogenization_H::heatMatrix(double C[3][3]) (homogenization.cu:180-252)."""
+        self._sync_stream()
+        C = (ctypes.c_double * 9)()
+        allow = (0, _lib.OTM_ERR_NOT_CONVERGED) if allow_not_converged else (0,)
+        check(lib().otm_homo_heat_matrix(self._h, C), "otm_homo_heat_matrix", allow)
+        return np.array(C[:], dtype=np.float64).reshape(3, 3)
+
+    def heatMatrix_nosolve(self) -> np.ndarray:
+        self._sync_stream()
+        C = (ctypes.c_double * 9)()
+        check(lib().otm_homo_heat_matrix_nosolve(self._h, C), "otm_homo_heat_matrix_nosolve")
+        return np.array(C[:], dtype=np.float64).reshape(3, 3)
+
+    def Sensitivity(self, dC, sens, pitchT: int = -1, lexiOrder: bool = False):
+        """Homogenization_H::Sensitivity(dC, sens, pitchT, lexiOrder) (homogenization.cu:415-479)."""
+        self._sync_stream()
+        d = (ctypes.c_float * 9)(*[float(v) for v in np.asarray(dC, dtype=np.float64).reshape(9)])
+        check(lib().otm_homo_sensitivity(self._h, d, ctypes.c_void_p(_ptr(sens)), int(pitchT), int(bool(lexiOrder))),
+              "otm_homo_sensitivity")
+
+    def element_energy(self, out=None):
+        """dK^H_ab/dk_e for the pairs 00 01 02 11 12 22 as a (6, nz, ny, nx) tensor."""
+        import torch
+        nx, ny, nz = self.reso
+        if out is None:
+            out = torch.empty((6, nz, ny, nx), dtype=torch.float32, device="cuda")
+        self._sync_stream()
+        check(lib().otm_homo_element_energy(self._h, ctypes.c_void_p(_ptr(out))), "otm_homo_element_energy")
+        return out
+
+    def solution(self, lcase: int, out=None):
+        import torch
+        nx, ny, nz = self.reso
+        if out is None:
+            out = torch.empty((nz, ny, nx), dtype=torch.float32, device="cuda")
+        self._sync_stream()
+        check(lib().otm_homo_get_solution(self._h, int(lcase), ctypes.c_void_p(_ptr(out))), "otm_homo_get_solution")
+        return out
+
+    def set_solution(self, lcase: int, src):
+        self._sync_stream()
+        check(lib().otm_homo_set_solution(self._h, int(lcase), ctypes.c_void_p(_ptr(src))), "otm_homo_set_solution")
+
+    def reset_displacement(self):
+        """MG_H::reset_displacement (homogenization/MG.cpp:73-78)."""
+        self._sync_stream()
+        check(lib().otm_homo_reset_displacement(self._h), "otm_homo_reset_displacement")
+
+    def stats(self) -> _lib.SolveStats:
+        st = _lib.SolveStats()
+        check(lib().otm_homo_get_stats(self._h, ctypes.byref(st)), "otm_homo_get_stats")
+        return st
+
+
+def filter_forward(src, reso, radius=2.0, weight=WEIGHT_LINEAR, periodic=True, dst=None, wsum=None,
+                   src_pitchT=-1, dst_pitchT=-1, stream=None):
+    """conv_kernel (AutoDiff/TensorExpression.cuh:304-350)."""
+    import torch
+    nx, ny, nz = reso
+    if dst is None:
+        dst = torch.empty((nz, ny, nx), dtype=torch.float32, device="cuda")
+    if wsum is None:
+        wsum = torch.empty((nz, ny, nx), dtype=torch.float32, device="cuda")
+    check(lib().otm_filter_forward(i3(reso), ctypes.c_void_p(_ptr(src)), int(src_pitchT), ctypes.c_void_p(_ptr(dst)),
+                                   int(dst_pitchT), ctypes.c_void_p(_ptr(wsum)), int(weight), float(radius),
+                                   int(bool(periodic)), ctypes.c_void_p(_stream(stream))), "otm_filter_forward")
+    return dst, wsum
+
+
+def filter_backward(g_dst, wsum, reso, radius=2.0, weight=WEIGHT_LINEAR, periodic=True, g_src=None, stream=None):
+    """conv_backward_kernel (AutoDiff/TensorExpression.cuh:353-385)."""
+    import torch
+    nx, ny, nz = reso
+    if g_src is None:
+        g_src = torch.empty((nz, ny, nx), dtype=torch.float32, device="cuda")
+    check(lib().otm_filter_backward(i3(reso), ctypes.c_void_p(_ptr(g_dst)), -1, ctypes.c_void_p(_ptr(wsum)),
+                                    ctypes.c_void_p(_ptr(g_src)), -1, int(weight), float(radius), int(bool(periodic)),
+                                    ctypes.c_void_p(_stream(stream))), "otm_filter_backward")
+    return g_src
+
+
+class DensityFilter:
+    """rho -> k = (k0 - kmin) conv(rho)^p + kmin and its adjoint, as the expression
+    rho.conv(ker).pow(p) * (k0 - kmin) + kmin of runCustom (Framework.cu:163)."""
+
+    def __init__(self, reso, radius=2.0, weight=WEIGHT_LINEAR, periodic=True, p=3.0, k0=1.0, kmin=1e-3):
+        import torch
+        self.reso = tuple(reso)
+        self.radius, self.weight, self.periodic = float(radius), int(weight), bool(periodic)
+        self.p, self.k0, self.kmin = float(p), float(k0), float(kmin)
+        nx, ny, nz = self.reso
+        shape = (nz, ny, nx)
+        self.rho_f = torch.empty(shape, dtype=torch.float32, device="cuda")
+        self.k = torch.empty(shape, dtype=torch.float32, device="cuda")
+        self.dk = torch.empty(shape, dtype=torch.float32, device="cuda")
+        self.wsum = torch.empty(shape, dtype=torch.float32, device="cuda")
+
+    def forward(self, rho, pitchT=-1, stream=None):
+        check(lib().otm_density_forward(i3(self.reso), ctypes.c_void_p(_ptr(rho)), int(pitchT),
+                                        ctypes.c_void_p(_ptr(self.rho_f)), ctypes.c_void_p(_ptr(self.k)),
+                                        ctypes.c_void_p(_ptr(self.dk)), ctypes.c_void_p(_ptr(self.wsum)),
+                                        self.weight, self.radius, int(self.periodic), self.p, self.k0, self.kmin,
+                                        ctypes.c_void_p(_stream(stream))), "otm_density_forward")
+        return self.k
+
+    def backward(self, g_k, g_rho=None, stream=None):
+        import torch
+        if g_rho is None:
+            g_rho = torch.empty_like(self.k)
+        check(lib().otm_density_backward(i3(self.reso), ctypes.c_void_p(_ptr(g_k)), ctypes.c_void_p(_ptr(self.dk)),
+                                         ctypes.c_void_p(_ptr(self.wsum)), ctypes.c_void_p(_ptr(g_rho)), -1,
+                                         self.weight, self.radius, int(self.periodic),
+                                         ctypes.c_void_p(_stream(stream))), "otm_density_backward")
+        return g_rho
+
+
+class OCOptimizer:
+    """OCOptimizer (optimization/OCOptimizer.h:7-20)."""
+
+    def __init__(self, ne: int, min_density: float = 0.001, stepLimit: float = 0.02, dampExponent: float = 0.5):
+        self.ne, self.minRho, self.step_limit, self.damp = int(ne), float(min_density), float(stepLimit), float(dampExponent)
+        self.last_iters = None
+
+    def filterSens(self, sens, rho, pitchT, reso, radius: float = 2.0, stream=None):
+        check(lib().otm_oc_filter_sens(ctypes.c_void_p(_ptr(sens)), ctypes.c_void_p(_ptr(rho)), int(pitchT), i3(reso),
+                                       float(radius), ctypes.c_void_p(_stream(stream))), "otm_oc_filter_sens")
+
+    def update(self, sens, rho, volratio: float, stream=None, want_iters: bool = False):
+        it = ctypes.c_int(0)
+        check(lib().otm_oc_update(self.ne, ctypes.c_void_p(_ptr(sens)), ctypes.c_void_p(_ptr(rho)), float(volratio),
+                                  self.minRho, self.step_limit, self.damp, ctypes.c_void_p(_stream(stream)),
+                                  ctypes.byref(it) if want_iters else None), "otm_oc_update")
+        self.last_iters = it.value if want_iters else None
+        return self.last_iters
+
+
+class MMAOptimizer:
+    """MMAOptimizer (optimization/mmaOptimizer.h:12-35): FP64 method of moving asymptotes on
+    the device; x, dfdx and dgdx rows are float32 device arrays of n values."""
+
+    def __init__(self, nconstrain: int, nvar: int, a0: float, a: float, c: float, d: float, stream=None):
+        self.m, self.n = int(nconstrain), int(nvar)
+        self._h = ctypes.c_void_p()
+        check(lib().otm_mma_create(self.m, self.n, float(a0), float(a), float(c), float(d), ctypes.byref(self._h)),
+              "otm_mma_create")
+        if stream is not None:
+            check(lib().otm_mma_set_stream(self._h, ctypes.c_void_p(_stream(stream))), "otm_mma_set_stream")
+
+    def __del__(self):
+        try:
+            if self._h:
+                lib().otm_mma_destroy(self._h)
+        except Exception:
+            pass
+
+    def setBound(self, xmin, xmax):
+        if isinstance(xmin, (int, float)):
+            check(lib().otm_mma_set_bound_scalar(self._h, float(xmin), float(xmax)), "otm_mma_set_bound_scalar")
+        else:
+            check(lib().otm_mma_set_bound(self._h, ctypes.c_void_p(_ptr(xmin)), ctypes.c_void_p(_ptr(xmax))),
+                  "otm_mma_set_bound")
+
+    def update(self, itn: int, x, dfdx, gval, dgdx):
+        check(lib().otm_mma_set_stream(self._h, ctypes.c_void_p(_stream(None))), "otm_mma_set_stream")
+        g = (ctypes.c_float * self.m)(*[float(v) for v in np.asarray(gval, dtype=np.float64).reshape(self.m)])
+        rows = (ctypes.c_void_p * self.m)(*[_ptr(r) for r in dgdx])
+        check(lib().otm_mma_update(self._h, int(itn), ctypes.c_void_p(_ptr(x)), ctypes.c_void_p(_ptr(dfdx)), g, rows),
+              "otm_mma_update")

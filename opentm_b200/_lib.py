@@ -1,0 +1,186 @@
+"""ctypes binding of ``libopentm_b200.so`` (the C ABI declared in include/opentm_b200*.h).
+
+The library is loaded from the package directory. If it is missing the import of the
+product entry points fails loudly: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+LIB_PATH = os.path.join(HERE, "libopentm_b200.so")
+HEADERS = [os.path.join(ROOT, "include", f) for f in ("opentm_b200.h", "opentm_b200_mma.h", "opentm_b200_server.h")]
+
+OTM_OK = 0
+STATUS_NAMES = {
+    0: "OTM_OK", 1: "OTM_ERR_INVALID_ARGUMENT", 2: "OTM_ERR_UNSUPPORTED", 3: "OTM_ERR_CUDA",
+    4: "OTM_ERR_OUT_OF_MEMORY", 5: "OTM_ERR_NOT_CONVERGED", 6: "OTM_ERR_DIVERGED", 7: "OTM_ERR_NAN",
+    8: "OTM_ERR_BUDGET", 9: "OTM_ERR_STATE", 10: "OTM_ERR_TIMEOUT", 11: "OTM_ERR_CANCELLED",
+    12: "OTM_ERR_NOT_READY",
+}
+OTM_ERR_NOT_CONVERGED = 5
+OTM_ERR_NOT_READY = 12
+
+PRECISION = {"fp32": 0, "bf16": 1, "fp16": 2}
+SOLVER = {"pcg": 0, "vcycle": 1}
+
+
+class OtmError(RuntimeError):
+    def __init__(self, status: int, where: str, message: str = ""):
+        self.status = status
+        super().__init__(f"{where}: {STATUS_NAMES.get(status, status)} ({message})")
+
+
+class Config(ctypes.Structure):
+    _fields_ = [
+        ("reso", ctypes.c_int * 3),
+        ("fem_rel_thres", ctypes.c_double),
+        ("max_iter", ctypes.c_int),
+        ("pre_smooth", ctypes.c_int),
+        ("post_smooth", ctypes.c_int),
+        ("solver", ctypes.c_int),
+        ("precision", ctypes.c_int),
+        ("coarsest_max_dof", ctypes.c_int),
+        ("power_penal", ctypes.c_float),
+        ("warm_start", ctypes.c_int),
+        ("check_every", ctypes.c_int),
+        ("use_graphs", ctypes.c_int),
+    ]
+
+
+class SolveStats(ctypes.Structure):
+    _fields_ = [
+        ("iterations", ctypes.c_int),
+        ("refinements", ctypes.c_int),
+        ("rel_res", ctypes.c_double * 3),
+        ("status", ctypes.c_int),
+        ("levels", ctypes.c_int),
+        ("coarsest_reso", ctypes.c_int * 3),
+    ]
+
+
+class PitchedPtr(ctypes.Structure):
+    _fields_ = [("ptr", ctypes.c_void_p), ("pitch", ctypes.c_size_t), ("xsize", ctypes.c_size_t),
+                ("ysize", ctypes.c_size_t)]
+
+
+_P = ctypes.c_void_p
+_I3 = ctypes.POINTER(ctypes.c_int)
+_D = ctypes.POINTER(ctypes.c_double)
+_F = ctypes.POINTER(ctypes.c_float)
+_S = ctypes.c_int  # otm_status
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "otm_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "otm_last_error": (ctypes.c_char_p, []),
+    "otm_abi_version": (ctypes.c_int, []),
+    "otm_config_init": (_S, [ctypes.POINTER(Config)]),
+    "otm_homo_create": (_S, [ctypes.POINTER(Config), ctypes.POINTER(_P)]),
+    "otm_homo_destroy": (_S, [_P]),
+    "otm_homo_set_stream": (_S, [_P, _P]),
+    "otm_homo_get_config": (_S, [_P, ctypes.POINTER(Config)]),
+    "otm_homo_set_tolerance": (_S, [_P, ctypes.c_double]),
+    "otm_homo_update": (_S, [_P, _P, ctypes.c_int]),
+    "otm_homo_solve": (_S, [_P, ctypes.POINTER(SolveStats)]),
+    "otm_homo_heat_matrix": (_S, [_P, _D]),
+    "otm_homo_heat_matrix_nosolve": (_S, [_P, _D]),
+    "otm_homo_sensitivity": (_S, [_P, _F, _P, ctypes.c_int, ctypes.c_int]),
+    "otm_homo_element_energy": (_S, [_P, _P]),
+    "otm_homo_get_solution": (_S, [_P, ctypes.c_int, _P]),
+    "otm_homo_set_solution": (_S, [_P, ctypes.c_int, _P]),
+    "otm_homo_reset_displacement": (_S, [_P]),
+    "otm_homo_get_stats": (_S, [_P, ctypes.POINTER(SolveStats)]),
+    "otm_filter_forward": (_S, [_I3, _P, ctypes.c_int, _P, ctypes.c_int, _P, ctypes.c_int, ctypes.c_float,
+                                ctypes.c_int, _P]),
+    "otm_filter_backward": (_S, [_I3, _P, ctypes.c_int, _P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                 ctypes.c_int, _P]),
+    "otm_density_forward": (_S, [_I3, _P, ctypes.c_int, _P, _P, _P, _P, ctypes.c_int, ctypes.c_float, ctypes.c_int,
+                                 ctypes.c_float, ctypes.c_float, ctypes.c_float, _P]),
+    "otm_density_backward": (_S, [_I3, _P, _P, _P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_int,
+                                  _P]),
+    "otm_oc_filter_sens": (_S, [_P, _P, ctypes.c_size_t, _I3, ctypes.c_float, _P]),
+    "otm_oc_update": (_S, [ctypes.c_int, _P, _P, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                           _P, ctypes.POINTER(ctypes.c_int)]),
+    # MMA (include/opentm_b200_mma.h)
+    "otm_mma_create": (_S, [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                            ctypes.c_double, ctypes.POINTER(_P)]),
+    "otm_mma_destroy": (_S, [_P]),
+    "otm_mma_set_stream": (_S, [_P, _P]),
+    "otm_mma_set_bound_scalar": (_S, [_P, ctypes.c_float, ctypes.c_float]),
+    "otm_mma_set_bound": (_S, [_P, _P, _P]),
+    "otm_mma_update": (_S, [_P, ctypes.c_int, _P, _P, _F, ctypes.POINTER(_P)]),
+    "otm_mmasub_device": (_S, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P, _P, _P, _P, ctypes.c_double, _P,
+                               _P, PitchedPtr, _P, _P, ctypes.c_double, _P, _P, _P, ctypes.c_double, _P]),
+    # serving (include/opentm_b200_server.h)
+}
+
+_lib = None
+
+
+def header_symbols() -> list[str]:
+    """Every function the public headers declare."""
+    names = []
+    for h in HEADERS:
+        if not os.path.exists(h):
+            continue
+        txt = open(h).read()
+        names += re.findall(r"^OTM_API\s+[\w\s\*]+?\b(otm_\w+)\s*\(", txt, flags=re.M)
+    return names
+
+
+def lib() -> ctypes.CDLL:
+    """Load the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            f"{LIB_PATH} is missing: build the sm_100a CUDA library with `python -m opentm_b200.build` "
+            "(there is no CPU fallback)")
+    L = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(L, name, None)
+        if fn is None:
+            continue
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def last_error() -> str:
+    return lib().otm_last_error().decode()
+
+
+def check(status: int, where: str, allow=(OTM_OK,)) -> int:
+    if status not in allow:
+        raise OtmError(status, where, last_error())
+    return status
+
+
+def default_config(reso=(128, 128, 128), **kw) -> Config:
+    cfg = Config()
+    check(lib().otm_config_init(ctypes.byref(cfg)), "otm_config_init")
+    if isinstance(reso, int):
+        reso = (reso, reso, reso)
+    for i in range(3):
+        cfg.reso[i] = int(reso[i])
+    for k, v in kw.items():
+        if k == "precision" and isinstance(v, str):
+            v = PRECISION[v]
+        if k == "solver" and isinstance(v, str):
+            v = SOLVER[v]
+        if not hasattr(cfg, k):
+            raise TypeError(f"unknown config field {k}")
+        setattr(cfg, k, v)
+    return cfg
+
+
+def i3(reso) -> ctypes.Array:
+    if isinstance(reso, int):
+        reso = (reso, reso, reso)
+    return (ctypes.c_int * 3)(*[int(r) for r in reso])

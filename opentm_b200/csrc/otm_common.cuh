@@ -1,0 +1,84 @@
+// otm_common.cuh -- shared host/device helpers of the B200 homogenization library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "opentm_b200.h"
+
+namespace otm {
+
+// Conductivity floor added inside the solver (homogenization/grid.h:429).
+constexpr float kRhoPenalMin = 1e-9f;
+
+// Block size of the stencil kernels and reductions.
+constexpr int kBlock = 256;
+// Fixed upper bound on reduction partial slots per launch (deterministic ordering).
+constexpr int kMaxPartials = 2048;
+
+// Per-thread message of the last failure, returned by otm_last_error().
+void set_error(const std::string& msg);
+otm_status cuda_fail(cudaError_t e, const char* what);
+
+#define OTM_CUDA(call)                                  \
+  do {                                                  \
+    cudaError_t e__ = (call);                           \
+    if (e__ != cudaSuccess) return ::otm::cuda_fail(e__, #call); \
+  } while (0)
+
+#define OTM_CHECK_LAUNCH(what)                          \
+  do {                                                  \
+    cudaError_t e__ = cudaGetLastError();               \
+    if (e__ != cudaSuccess) return ::otm::cuda_fail(e__, what); \
+  } while (0)
+
+#define OTM_TRY(expr)                                   \
+  do {                                                  \
+    otm_status s__ = (expr);                            \
+    if (s__ != OTM_OK) return s__;                      \
+  } while (0)
+
+// Periodic grid dimensions, x fastest: id = x + nx (y + ny z).
+struct Dims {
+  int nx, ny, nz;
+  __host__ __device__ size_t nv() const { return size_t(nx) * ny * nz; }
+};
+
+__device__ __forceinline__ int wrapm(int a, int n) {
+  // a in [-n, 2n)
+  return a < 0 ? a + n : (a >= n ? a - n : a);
+}
+
+// Deterministic FP64 block reduction of NV values per thread (warp shuffles then shared
+// memory, fixed order). The result is valid in thread 0 only.
+template <int NV>
+__device__ __forceinline__ void block_reduce_f64(double (&v)[NV], double* smem /* >= 32*NV */) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nwarps = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int i = 0; i < NV; i++) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v[i] += __shfl_down_sync(0xffffffffu, v[i], off);
+  }
+  __syncthreads();
+  if (lane == 0) {
+#pragma unroll
+    for (int i = 0; i < NV; i++) smem[warp * NV + i] = v[i];
+  }
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int i = 0; i < NV; i++) {
+      double x = lane < nwarps ? smem[lane * NV + i] : 0.0;
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) x += __shfl_down_sync(0xffffffffu, x, off);
+      v[i] = x;
+    }
+  }
+}
+
+inline int ceil_div(size_t a, size_t b) { return int((a + b - 1) / b); }
+
+}  // namespace otm

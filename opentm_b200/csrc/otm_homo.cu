@@ -1,0 +1,595 @@
+// otm_homo.cu -- Homogenization_H / MG_H / Grid_H replacement: hierarchy, solver driver and
+// the homogenization entry points of the C ABI.
+//
+// One otm_homo handle owns its whole multigrid hierarchy on the device (no __constant__
+// symbols, no global buffer registry), runs all its work on a private stream that is
+// ordered after / before the caller's stream with events, and captures the iteration loop in
+// a CUDA graph that is replayed until the device-side convergence flag is set.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "otm_common.cuh"
+#include "otm_homo_impl.h"
+#include "otm_solver_kernels.cuh"
+#include "otm_template.h"
+
+namespace otm {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+otm_status cuda_fail(cudaError_t e, const char* what) {
+  set_error(std::string(what) + ": " + cudaGetErrorString(e));
+  if (e == cudaErrorMemoryAllocation) return OTM_ERR_OUT_OF_MEMORY;
+  return OTM_ERR_CUDA;
+}
+
+static otm_status invalid(const std::string& msg) {
+  set_error(msg);
+  return OTM_ERR_INVALID_ARGUMENT;
+}
+
+// ---------------------------------------------------------------------------------------
+// Hierarchy construction (MG_H::build, homogenization/MG.cpp:13-44; coarsening rule
+// Grid_H::coarse2, homogenization/grid.cpp:92-138, here always by 2 per axis).
+// ---------------------------------------------------------------------------------------
+static std::vector<Dims> level_dims(const int reso[3], int coarsest_max_dof) {
+  std::vector<Dims> out;
+  Dims d{reso[0], reso[1], reso[2]};
+  while (true) {
+    out.push_back(d);
+    const bool can = d.nx % 2 == 0 && d.ny % 2 == 0 && d.nz % 2 == 0 && d.nx >= 8 && d.ny >= 8 && d.nz >= 8 &&
+                     d.nv() > size_t(coarsest_max_dof);
+    if (!can) break;
+    d = Dims{d.nx / 2, d.ny / 2, d.nz / 2};
+  }
+  return out;
+}
+
+static constexpr int kMaxCoarsest = 1024;
+
+otm_status Homo::alloc(void** p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc");
+  allocations.push_back(*p);
+  bytes_allocated += bytes;
+  return OTM_OK;
+}
+
+Homo::~Homo() {
+  for (auto& g : graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  if (stream) cudaStreamDestroy(stream);
+  if (ev_in) cudaEventDestroy(ev_in);
+  if (ev_out) cudaEventDestroy(ev_out);
+  for (void* p : allocations) cudaFree(p);
+  if (sc_host) cudaFreeHost(sc_host);
+}
+
+otm_status Homo::build(const otm_config& c) {
+  cfg = c;
+  for (int i = 0; i < 3; i++) {
+    if (cfg.reso[i] < 2) return invalid("resolution must be >= 2 per axis");
+    if (cfg.reso[i] > 1024) {
+      set_error("axis resolution cannot exceed 1024");  // homogenization/grid.cpp:23-25
+      return OTM_ERR_UNSUPPORTED;
+    }
+  }
+  if (cfg.pre_smooth < 0 || cfg.post_smooth < 0 || cfg.pre_smooth + cfg.post_smooth == 0)
+    return invalid("need at least one smoothing sweep");
+  if (cfg.max_iter < 1) return invalid("max_iter must be >= 1");
+  if (cfg.check_every < 1) cfg.check_every = 1;
+  if (cfg.coarsest_max_dof < 8) cfg.coarsest_max_dof = 8;
+  if (cfg.solver != OTM_SOLVER_PCG && cfg.solver != OTM_SOLVER_VCYCLE) return invalid("unknown solver");
+  if (cfg.precision < OTM_PRECISION_FP32 || cfg.precision > OTM_PRECISION_MIXED_FP16)
+    return invalid("unknown precision");
+  if (cfg.solver == OTM_SOLVER_PCG && cfg.pre_smooth != cfg.post_smooth)
+    return invalid("PCG needs a symmetric V-cycle (pre_smooth == post_smooth)");
+
+  std::vector<Dims> dims = level_dims(cfg.reso, cfg.coarsest_max_dof);
+  if (dims.back().nv() > size_t(kMaxCoarsest)) {
+    set_error("coarsest level too large for the dense direct solve (aspect ratio too extreme)");
+    return OTM_ERR_UNSUPPORTED;
+  }
+  // template matrices, element size 1/reso_x (homogenization/homogenization.cpp:211)
+  template_matrices(1.0 / cfg.reso[0] / 2.0, &tm);
+  if (tm.structure_error > 1e-9) {
+    set_error("element matrix does not have the cube-Laplacian structure");
+    return OTM_ERR_UNSUPPORTED;
+  }
+  op = FineOp{float(tm.c[0]), float(tm.c[1]), float(tm.c[2]), float(tm.c[3])};
+  face = !tm.face_zero;
+  for (int j = 0; j < 8; j++)
+    for (int cc = 0; cc < 3; cc++) {
+      ef.disp[j][cc] = float(tm.disp[j][cc]);
+      ef.feMu[j][cc] = float(tm.feMu[j][cc]);
+    }
+
+  OTM_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  OTM_CUDA(cudaEventCreateWithFlags(&ev_in, cudaEventDisableTiming));
+  OTM_CUDA(cudaEventCreateWithFlags(&ev_out, cudaEventDisableTiming));
+
+  lv.resize(dims.size());
+  for (size_t l = 0; l < dims.size(); l++) {
+    Level& L = lv[l];
+    L.d = dims[l];
+    const size_t nv = L.d.nv();
+    OTM_TRY(alloc((void**)&L.u, 3 * nv * sizeof(float)));
+    OTM_TRY(alloc((void**)&L.f, 3 * nv * sizeof(float)));
+    OTM_TRY(alloc((void**)&L.r, 3 * nv * sizeof(float)));
+    OTM_CUDA(cudaMemsetAsync(L.u, 0, 3 * nv * sizeof(float), stream));
+    OTM_CUDA(cudaMemsetAsync(L.f, 0, 3 * nv * sizeof(float), stream));
+    OTM_CUDA(cudaMemsetAsync(L.r, 0, 3 * nv * sizeof(float), stream));
+    if (l > 0 || dims.size() == 1) OTM_TRY(alloc((void**)&L.st, 27 * nv * sizeof(float)));
+  }
+  const size_t nv = lv[0].d.nv();
+  OTM_TRY(alloc((void**)&ks, nv * sizeof(float)));
+  OTM_TRY(alloc((void**)&kraw, nv * sizeof(float)));
+  OTM_TRY(alloc((void**)&b, 3 * nv * sizeof(float)));
+  OTM_TRY(alloc((void**)&x, 3 * nv * sizeof(float)));
+  OTM_TRY(alloc((void**)&p, 3 * nv * sizeof(float)));
+  OTM_TRY(alloc((void**)&q, 3 * nv * sizeof(float)));
+  OTM_CUDA(cudaMemsetAsync(x, 0, 3 * nv * sizeof(float), stream));
+  OTM_CUDA(cudaMemsetAsync(p, 0, 3 * nv * sizeof(float), stream));
+  nc = int(lv.back().d.nv());
+  OTM_TRY(alloc((void**)&Ainv, size_t(nc) * nc * sizeof(double)));
+  OTM_TRY(alloc((void**)&table, 64 * 27 * sizeof(float)));
+  OTM_TRY(alloc((void**)&sc, sizeof(SolveScalars)));
+  OTM_TRY(alloc((void**)&partials, size_t(kMaxPartials) * 16 * sizeof(double)));
+  OTM_TRY(alloc((void**)&means, 8 * sizeof(double)));
+  OTM_TRY(alloc((void**)&flags, 4 * sizeof(int)));
+  OTM_CUDA(cudaMemsetAsync(sc, 0, sizeof(SolveScalars), stream));
+  OTM_CUDA(cudaMemsetAsync(flags, 0, 4 * sizeof(int), stream));
+  OTM_CUDA(cudaMallocHost((void**)&sc_host, sizeof(SolveScalars)));
+  std::memset(sc_host, 0, sizeof(SolveScalars));
+  std::vector<float> tab(64 * 27);
+  galerkin_level1_table(tm, tab.data());
+  OTM_CUDA(cudaMemcpyAsync(table, tab.data(), tab.size() * sizeof(float), cudaMemcpyHostToDevice, stream));
+  OTM_CUDA(cudaStreamSynchronize(stream));
+  stats.levels = int(lv.size());
+  stats.coarsest_reso[0] = lv.back().d.nx;
+  stats.coarsest_reso[1] = lv.back().d.ny;
+  stats.coarsest_reso[2] = lv.back().d.nz;
+  return OTM_OK;
+}
+
+otm_status Homo::enter() {
+  OTM_CUDA(cudaEventRecord(ev_in, user_stream));
+  OTM_CUDA(cudaStreamWaitEvent(stream, ev_in, 0));
+  return OTM_OK;
+}
+
+otm_status Homo::leave() {
+  OTM_CUDA(cudaEventRecord(ev_out, stream));
+  OTM_CUDA(cudaStreamWaitEvent(user_stream, ev_out, 0));
+  return OTM_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// update: import k, Galerkin stencils of every coarse level, dense coarsest inverse
+// (Homogenization_H::update, homogenization/homogenization.cpp:76-81; MG_H::updateStencils,
+// homogenization/MG.cpp:144-151).
+// ---------------------------------------------------------------------------------------
+otm_status Homo::update(const float* kin, int pitchT) {
+  const Dims d0 = lv[0].d;
+  if (!kin) return invalid("k pointer is NULL");
+  if (pitchT <= 0) pitchT = d0.nx;
+  if (pitchT < d0.nx) return invalid("pitchT smaller than the x resolution");
+  OTM_TRY(enter());
+  const size_t nv = d0.nv();
+  k_import<<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(d0, kin, pitchT, cfg.power_penal, ks, kraw, flags);
+  OTM_CHECK_LAUNCH("k_import");
+  const int L = int(lv.size());
+  for (int l = 1; l < L; l++) {
+    const bool cb = (l < L - 1);  // smoothed levels use the colour-blocked stencil order
+    const size_t nvc = lv[l].d.nv();
+    if (l == 1)
+      k_galerkin_fine<<<ceil_div(nvc, kBlock), kBlock, 0, stream>>>(lv[0].d, lv[1].d, ks, table, lv[1].st, cb);
+    else
+      k_galerkin_coarse<<<ceil_div(nvc, kBlock), kBlock, 0, stream>>>(lv[l - 1].d, lv[l].d, lv[l - 1].st, lv[l].st,
+                                                                      cb);
+    OTM_CHECK_LAUNCH("galerkin");
+  }
+  if (L == 1) {
+    k_fine_stencil<<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(d0, ks, op, lv[0].st);
+    OTM_CHECK_LAUNCH("k_fine_stencil");
+  }
+  k_coarsest_build<<<1, 1024, 0, stream>>>(lv.back().d, lv.back().st, Ainv, flags + 1);
+  OTM_CHECK_LAUNCH("k_coarsest_build");
+  updated = true;
+  solved = false;
+  return leave();
+}
+
+// ---------------------------------------------------------------------------------------
+// V-cycle and iteration (MG_H::v_cycle, homogenization/MG.cpp:46-71).
+// ---------------------------------------------------------------------------------------
+void Homo::gs(int l, int color) {
+  Level& L = lv[l];
+  const size_t nsub = L.d.nv() >> 3;
+  if (l == 0) {
+    if (face)
+      k_gs_fine<true, 3><<<ceil_div(nsub, kBlock), kBlock, 0, stream>>>(L.d, color, ks, op, L.u, L.f, sc);
+    else
+      k_gs_fine<false, 3><<<ceil_div(nsub, kBlock), kBlock, 0, stream>>>(L.d, color, ks, op, L.u, L.f, sc);
+  } else {
+    k_gs_coarse<3><<<ceil_div(nsub, kBlock), kBlock, 0, stream>>>(L.d, color, L.st, L.u, L.f, sc);
+  }
+}
+
+void Homo::vcycle(int l) {
+  Level& L = lv[l];
+  const size_t nv = L.d.nv();
+  if (l == int(lv.size()) - 1) {
+    k_coarsest_solve<<<1, std::min(1024, std::max(32, (nc + 31) / 32 * 32)), 3 * nc * sizeof(double), stream>>>(
+        nc, Ainv, L.f, L.u, sc);
+    return;
+  }
+  cudaMemsetAsync(L.u, 0, 3 * nv * sizeof(float), stream);
+  for (int s = 0; s < cfg.pre_smooth; s++)
+    for (int c = 0; c < 8; c++) gs(l, c);
+  if (l == 0) {
+    if (face)
+      k_resid_fine<true, 3><<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(L.d, ks, op, L.u, L.f, L.r, sc);
+    else
+      k_resid_fine<false, 3><<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(L.d, ks, op, L.u, L.f, L.r, sc);
+  } else {
+    k_resid_coarse<3><<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(L.d, L.st, L.u, L.f, L.r, sc);
+  }
+  Level& C = lv[l + 1];
+  k_restrict<3><<<ceil_div(C.d.nv(), kBlock), kBlock, 0, stream>>>(L.d, C.d, L.r, C.f, sc);
+  vcycle(l + 1);
+  k_prolong<3><<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(L.d, C.d, C.u, L.u, sc);
+  for (int s = 0; s < cfg.post_smooth; s++)
+    for (int c = 7; c >= 0; c--) gs(l, c);
+}
+
+void Homo::iteration() {
+  const Dims d0 = lv[0].d;
+  const size_t nv = d0.nv();
+  const int nb = reduce_blocks(nv);
+  float* r = lv[0].f;  // Krylov residual is the V-cycle's level-0 right-hand side
+  float* z = lv[0].u;  // and the V-cycle's level-0 result is the preconditioned residual
+  if (cfg.solver == OTM_SOLVER_PCG) {
+    vcycle(0);
+    k_dot_rz<<<nb, kBlock, 0, stream>>>(nv, r, z, partials, sc);
+    k_update_p<<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(nv, z, p, sc);
+    if (face)
+      k_apply_dot<true><<<nb, kBlock, 0, stream>>>(d0, ks, op, p, q, partials, sc);
+    else
+      k_apply_dot<false><<<nb, kBlock, 0, stream>>>(d0, ks, op, p, q, partials, sc);
+    k_update_xr<<<nb, kBlock, 0, stream>>>(nv, x, r, p, q, partials, sc, cfg.max_iter);
+  } else {
+    if (face)
+      k_resid_norm<true><<<nb, kBlock, 0, stream>>>(d0, ks, op, x, b, r, partials, sc, cfg.max_iter);
+    else
+      k_resid_norm<false><<<nb, kBlock, 0, stream>>>(d0, ks, op, x, b, r, partials, sc, cfg.max_iter);
+    vcycle(0);
+    k_axpy_x<<<ceil_div(3 * nv, kBlock), kBlock, 0, stream>>>(nv, x, z, sc);
+  }
+}
+
+otm_status Homo::run_chunk(int iters) {
+  if (!cfg.use_graphs) {
+    for (int i = 0; i < iters; i++) iteration();
+    OTM_CHECK_LAUNCH("iteration");
+    return OTM_OK;
+  }
+  ChunkGraph* g = nullptr;
+  for (auto& gg : graphs)
+    if (gg.iters == iters && gg.solver == cfg.solver) g = &gg;
+  if (!g) {
+    graphs.push_back(ChunkGraph{});
+    g = &graphs.back();
+    g->iters = iters;
+    g->solver = cfg.solver;
+    cudaGraph_t graph;
+    OTM_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    for (int i = 0; i < iters; i++) iteration();
+    cudaError_t e = cudaStreamEndCapture(stream, &graph);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&g->exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+  }
+  OTM_CUDA(cudaGraphLaunch(g->exec, stream));
+  return OTM_OK;
+}
+
+// Solve the 3 load cases to the tolerance (MG_H::solveEquation, homogenization/MG.cpp:80-142;
+// per-case warm start from the previous solution, homogenization/homogenization.cu:182-188).
+otm_status Homo::solve_impl() {
+  const Dims d0 = lv[0].d;
+  const size_t nv = d0.nv();
+  const int nb = reduce_blocks(nv);
+  // import / coarsest status from update()
+  int fl[2] = {0, 0};
+  OTM_CUDA(cudaMemcpyAsync(fl, flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream));
+  OTM_CUDA(cudaStreamSynchronize(stream));
+  if (fl[0]) {
+    set_error("conductivity field holds a negative, NaN or Inf value");
+    return OTM_ERR_NAN;
+  }
+  if (fl[1]) {
+    set_error("coarsest-level matrix is not positive definite");
+    return OTM_ERR_NAN;
+  }
+  for (int attempt = 0; attempt < 2; attempt++) {
+    if (!cfg.warm_start || attempt > 0) OTM_CUDA(cudaMemsetAsync(x, 0, 3 * nv * sizeof(float), stream));
+    k_rhs<<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(d0, ks, ef, b);
+    // project RHS and initial guess off the constants
+    k_sums2<<<nb, kBlock, 0, stream>>>(nv, b, x, partials, means, &sc->counter[T_MEAN]);
+    k_sub_means<<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(nv, b, x, means);
+    sc_host->tol = cfg.fem_rel_thres;
+    OTM_CUDA(cudaMemcpyAsync(&sc->tol, &sc_host->tol, sizeof(double), cudaMemcpyHostToDevice, stream));
+    if (face)
+      k_init_residual<true><<<nb, kBlock, 0, stream>>>(d0, ks, op, x, b, lv[0].f, partials, sc);
+    else
+      k_init_residual<false><<<nb, kBlock, 0, stream>>>(d0, ks, op, x, b, lv[0].f, partials, sc);
+    OTM_CHECK_LAUNCH("solve init");
+    int launched = 0;
+    while (true) {
+      OTM_CUDA(cudaMemcpyAsync(sc_host, sc, sizeof(SolveScalars), cudaMemcpyDeviceToHost, stream));
+      OTM_CUDA(cudaStreamSynchronize(stream));
+      if (sc_host->done || launched >= cfg.max_iter) break;
+      const int chunk = std::min(cfg.check_every, cfg.max_iter - launched);
+      OTM_TRY(run_chunk(chunk));
+      launched += chunk;
+    }
+    stats.iterations = sc_host->iter;
+    for (int c = 0; c < 3; c++) stats.rel_res[c] = sc_host->relres[c];
+    if (!sc_host->nan) break;
+    // "numerical explode, resetting initial guess" (homogenization/MG.cpp:392-423): one
+    // retry from a zero initial guess, then give up.
+  }
+  otm_status st = OTM_OK;
+  if (sc_host->nan) {
+    set_error("MG numerical explode");
+    st = OTM_ERR_DIVERGED;
+  } else {
+    for (int c = 0; c < 3; c++)
+      if (!(stats.rel_res[c] <= cfg.fem_rel_thres)) st = OTM_ERR_NOT_CONVERGED;
+    if (st != OTM_OK) set_error("failed to converge within max_iter");
+  }
+  stats.status = st;
+  solved = (st == OTM_OK || st == OTM_ERR_NOT_CONVERGED);
+  return st;
+}
+
+otm_status Homo::solve(otm_solve_stats* out) {
+  if (!updated) {
+    set_error("update() must be called before solving");
+    return OTM_ERR_STATE;
+  }
+  OTM_TRY(enter());
+  otm_status st = solve_impl();
+  otm_status st2 = leave();
+  if (out) *out = stats;
+  return st != OTM_OK ? st : st2;
+}
+
+otm_status Homo::heat_matrix(double C[9], bool do_solve) {
+  if (!C) return invalid("C is NULL");
+  otm_status st = OTM_OK;
+  if (do_solve) {
+    st = solve(nullptr);
+    if (st != OTM_OK && st != OTM_ERR_NOT_CONVERGED) return st;
+  } else if (!solved) {
+    set_error("no solution available");
+    return OTM_ERR_STATE;
+  }
+  OTM_TRY(enter());
+  const Dims d0 = lv[0].d;
+  k_heat_matrix<<<reduce_blocks(d0.nv()), kBlock, 0, stream>>>(d0, ks, x, op, ef, partials, sc);
+  OTM_CHECK_LAUNCH("k_heat_matrix");
+  OTM_CUDA(cudaMemcpyAsync(sc_host->kh, sc->kh, 6 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  OTM_CUDA(cudaStreamSynchronize(stream));
+  int cnt = 0;
+  for (int a = 0; a < 3; a++)
+    for (int bq = a; bq < 3; bq++) {
+      C[a * 3 + bq] = sc_host->kh[cnt];
+      C[bq * 3 + a] = sc_host->kh[cnt];
+      cnt++;
+    }
+  OTM_TRY(leave());
+  return st;
+}
+
+otm_status Homo::sensitivity(const float dC[9], float* sens, int pitchT, int lexi) {
+  if (!dC || !sens) return invalid("NULL argument");
+  if (!solved) {
+    set_error("sensitivity needs a solved state (call heat_matrix first)");
+    return OTM_ERR_STATE;
+  }
+  const Dims d0 = lv[0].d;
+  if (!lexi || pitchT <= 0) pitchT = d0.nx;
+  if (pitchT < d0.nx) return invalid("pitchT smaller than the x resolution");
+  SensWeights sw;
+  int cnt = 0;
+  for (int a = 0; a < 3; a++)
+    for (int bq = a; bq < 3; bq++) sw.w[cnt++] = dC[a * 3 + bq] + (a != bq ? dC[bq * 3 + a] : 0.f);
+  OTM_TRY(enter());
+  const size_t total = size_t(pitchT) * d0.ny * d0.nz;
+  k_sensitivity<<<ceil_div(total, kBlock), kBlock, 0, stream>>>(d0, kraw, x, op, ef, sw, cfg.power_penal, sens,
+                                                                pitchT);
+  OTM_CHECK_LAUNCH("k_sensitivity");
+  return leave();
+}
+
+otm_status Homo::element_energy(float* out) {
+  if (!out) return invalid("NULL argument");
+  if (!solved) {
+    set_error("no solution available");
+    return OTM_ERR_STATE;
+  }
+  OTM_TRY(enter());
+  const Dims d0 = lv[0].d;
+  k_energy_fields<<<ceil_div(d0.nv(), kBlock), kBlock, 0, stream>>>(d0, x, op, ef, out);
+  OTM_CHECK_LAUNCH("k_energy_fields");
+  return leave();
+}
+
+}  // namespace otm
+
+// =========================================================================================
+// C ABI
+// =========================================================================================
+using otm::Homo;
+
+struct otm_homo {
+  Homo impl;
+};
+
+extern "C" {
+
+const char* otm_status_string(otm_status s) {
+  switch (s) {
+    case OTM_OK: return "ok";
+    case OTM_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case OTM_ERR_UNSUPPORTED: return "unsupported";
+    case OTM_ERR_CUDA: return "CUDA error";
+    case OTM_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case OTM_ERR_NOT_CONVERGED: return "not converged";
+    case OTM_ERR_DIVERGED: return "diverged";
+    case OTM_ERR_NAN: return "NaN or Inf";
+    case OTM_ERR_BUDGET: return "over memory budget";
+    case OTM_ERR_STATE: return "call out of order";
+    case OTM_ERR_TIMEOUT: return "timeout";
+    case OTM_ERR_CANCELLED: return "cancelled";
+    case OTM_ERR_NOT_READY: return "not ready";
+  }
+  return "unknown status";
+}
+
+const char* otm_last_error(void) { return otm::g_last_error.c_str(); }
+
+int otm_abi_version(void) { return OTM_ABI_VERSION; }
+
+otm_status otm_config_init(otm_config* cfg) {
+  if (!cfg) return OTM_ERR_INVALID_ARGUMENT;
+  std::memset(cfg, 0, sizeof(*cfg));
+  cfg->reso[0] = cfg->reso[1] = cfg->reso[2] = 128;  // cmdline.cpp:6-8
+  cfg->fem_rel_thres = 0.01;                         // cmdline.cpp:28
+  cfg->max_iter = 200;                               // MG.cpp:382
+  cfg->pre_smooth = 1;
+  cfg->post_smooth = 1;
+  cfg->solver = OTM_SOLVER_PCG;
+  cfg->precision = OTM_PRECISION_FP32;
+  cfg->coarsest_max_dof = 64;
+  cfg->power_penal = 1.0f;  // homogenization.h:22
+  cfg->warm_start = 1;
+  cfg->check_every = 4;
+  cfg->use_graphs = 1;
+  return OTM_OK;
+}
+
+otm_status otm_homo_create(const otm_config* cfg, otm_homo** out) {
+  if (!cfg || !out) return OTM_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  otm_homo* h = new (std::nothrow) otm_homo();
+  if (!h) return OTM_ERR_OUT_OF_MEMORY;
+  otm_status st = h->impl.build(*cfg);
+  if (st != OTM_OK) {
+    delete h;
+    return st;
+  }
+  *out = h;
+  return OTM_OK;
+}
+
+otm_status otm_homo_destroy(otm_homo* h) {
+  if (!h) return OTM_ERR_INVALID_ARGUMENT;
+  cudaStreamSynchronize(h->impl.stream);
+  delete h;
+  return OTM_OK;
+}
+
+otm_status otm_homo_set_stream(otm_homo* h, void* stream) {
+  if (!h) return OTM_ERR_INVALID_ARGUMENT;
+  h->impl.user_stream = (cudaStream_t)stream;
+  return OTM_OK;
+}
+
+otm_status otm_homo_get_config(const otm_homo* h, otm_config* cfg) {
+  if (!h || !cfg) return OTM_ERR_INVALID_ARGUMENT;
+  *cfg = h->impl.cfg;
+  return OTM_OK;
+}
+
+otm_status otm_homo_set_tolerance(otm_homo* h, double tol) {
+  if (!h || !(tol > 0.0)) return OTM_ERR_INVALID_ARGUMENT;
+  h->impl.cfg.fem_rel_thres = tol;
+  return OTM_OK;
+}
+
+otm_status otm_homo_update(otm_homo* h, const float* k_dev, int pitchT) {
+  if (!h) return OTM_ERR_INVALID_ARGUMENT;
+  return h->impl.update(k_dev, pitchT);
+}
+
+otm_status otm_homo_solve(otm_homo* h, otm_solve_stats* stats) {
+  if (!h) return OTM_ERR_INVALID_ARGUMENT;
+  return h->impl.solve(stats);
+}
+
+otm_status otm_homo_heat_matrix(otm_homo* h, double C[9]) {
+  if (!h) return OTM_ERR_INVALID_ARGUMENT;
+  return h->impl.heat_matrix(C, true);
+}
+
+otm_status otm_homo_heat_matrix_nosolve(otm_homo* h, double C[9]) {
+  if (!h) return OTM_ERR_INVALID_ARGUMENT;
+  return h->impl.heat_matrix(C, false);
+}
+
+otm_status otm_homo_sensitivity(otm_homo* h, const float dC[9], float* sens_dev, int pitchT, int lexi) {
+  if (!h) return OTM_ERR_INVALID_ARGUMENT;
+  return h->impl.sensitivity(dC, sens_dev, pitchT, lexi);
+}
+
+otm_status otm_homo_element_energy(otm_homo* h, float* energy_dev) {
+  if (!h) return OTM_ERR_INVALID_ARGUMENT;
+  return h->impl.element_energy(energy_dev);
+}
+
+otm_status otm_homo_get_solution(otm_homo* h, int lcase, float* dst_dev) {
+  if (!h || !dst_dev || lcase < 0 || lcase > 2) return OTM_ERR_INVALID_ARGUMENT;
+  Homo& H = h->impl;
+  const size_t nv = H.lv[0].d.nv();
+  OTM_TRY(H.enter());
+  OTM_CUDA(cudaMemcpyAsync(dst_dev, H.x + lcase * nv, nv * sizeof(float), cudaMemcpyDeviceToDevice, H.stream));
+  return H.leave();
+}
+
+otm_status otm_homo_set_solution(otm_homo* h, int lcase, const float* src_dev) {
+  if (!h || !src_dev || lcase < 0 || lcase > 2) return OTM_ERR_INVALID_ARGUMENT;
+  Homo& H = h->impl;
+  const size_t nv = H.lv[0].d.nv();
+  OTM_TRY(H.enter());
+  OTM_CUDA(cudaMemcpyAsync(H.x + lcase * nv, src_dev, nv * sizeof(float), cudaMemcpyDeviceToDevice, H.stream));
+  return H.leave();
+}
+
+otm_status otm_homo_reset_displacement(otm_homo* h) {
+  if (!h) return OTM_ERR_INVALID_ARGUMENT;
+  Homo& H = h->impl;
+  OTM_TRY(H.enter());
+  OTM_CUDA(cudaMemsetAsync(H.x, 0, 3 * H.lv[0].d.nv() * sizeof(float), H.stream));
+  H.solved = false;
+  return H.leave();
+}
+
+otm_status otm_homo_get_stats(const otm_homo* h, otm_solve_stats* stats) {
+  if (!h || !stats) return OTM_ERR_INVALID_ARGUMENT;
+  *stats = h->impl.stats;
+  return OTM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,78 @@
+// otm_homo_impl.h -- the homogenization handle (internal).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "otm_mg_kernels.cuh"
+#include "otm_solver_kernels.cuh"
+#include "otm_template.h"
+
+namespace otm {
+
+// One multigrid level: 3 load cases of u (correction / solution), f (right-hand side) and
+// r (residual scratch), plus the 27-point stencil on coarse levels.
+struct Level {
+  Dims d{};
+  float* u = nullptr;
+  float* f = nullptr;
+  float* r = nullptr;
+  float* st = nullptr;
+};
+
+struct ChunkGraph {
+  int iters = 0;
+  int solver = 0;
+  cudaGraphExec_t exec = nullptr;
+};
+
+struct Homo {
+  otm_config cfg{};
+  cudaStream_t stream = nullptr;       // private stream (graph capture needs a non-legacy stream)
+  cudaStream_t user_stream = nullptr;  // ordering with the caller
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  std::vector<Level> lv;
+  TemplateMatrices tm{};
+  FineOp op{};
+  ElemFields ef{};
+  bool face = false;
+  float* ks = nullptr;    // solver conductivity 1e-9 + k^p
+  float* kraw = nullptr;  // conductivity as imported
+  float* b = nullptr;     // right-hand sides
+  float* x = nullptr;     // solutions chi (kept for warm starts)
+  float* p = nullptr;
+  float* q = nullptr;
+  double* Ainv = nullptr;
+  int nc = 0;
+  float* table = nullptr;
+  SolveScalars* sc = nullptr;
+  SolveScalars* sc_host = nullptr;
+  double* partials = nullptr;
+  double* means = nullptr;
+  int* flags = nullptr;  // [0] bad import value, [1] coarsest not SPD
+  std::vector<void*> allocations;
+  size_t bytes_allocated = 0;
+  std::vector<ChunkGraph> graphs;
+  bool updated = false;
+  bool solved = false;
+  otm_solve_stats stats{};
+
+  ~Homo();
+  otm_status alloc(void** p, size_t bytes);
+  otm_status build(const otm_config& c);
+  otm_status enter();
+  otm_status leave();
+  otm_status update(const float* kin, int pitchT);
+  void gs(int l, int color);
+  void vcycle(int l);
+  void iteration();
+  otm_status run_chunk(int iters);
+  otm_status solve_impl();
+  otm_status solve(otm_solve_stats* out);
+  otm_status heat_matrix(double C[9], bool do_solve);
+  otm_status sensitivity(const float dC[9], float* sens, int pitchT, int lexi);
+  otm_status element_energy(float* out);
+};
+
+}  // namespace otm

@@ -1,0 +1,445 @@
+// otm_mg_kernels.cuh -- sm_100a kernels of the periodic multigrid solver.
+//
+// Layout (all levels): vectors are lexicographic, x fastest, one periodic unknown per
+// vertex, the 3 load cases stored case-major (case c at offset c * nv). The fine level is
+// matrix-free from the element conductivity k_e (homogenization/grid.cu:318-471); coarse
+// levels hold 27-point Galerkin stencils (homogenization/grid_ex.cu:16-227) in the
+// "colour-blocked" order: stencil entry o of vertex (x,y,z) sits at
+// st[o * nv + colour * nv/8 + sub], colour = x%2 + 2(y%2) + 4(z%2), sub the lexicographic
+// index of (x/2, y/2, z/2), so that one Gauss-Seidel colour pass streams its coefficients.
+// Stencil offset o = (ox+1) + 3(oy+1) + 9(oz+1).
+#pragma once
+
+#include "otm_common.cuh"
+
+namespace otm {
+
+// Entries of the trilinear element Laplacian by Hamming distance between local nodes:
+// KE[i][j] = c[popc(i ^ j)] (templateMatrix.cpp:21-87 gives exactly this structure).
+struct FineOp {
+  float c0, c1, c2, c3;
+};
+
+// Scalars of an iterative solve kept on the device so no host round trip is needed per
+// iteration.
+struct SolveScalars {
+  double bb[3];      // ||b||^2 per case
+  double rz[3];      // r . z (projected) of the current iteration
+  double alpha[3];
+  double beta[3];
+  double zmean[3];
+  double rr[3];      // ||r||^2
+  double relres[3];  // ||r|| / (||b|| + 1e-10)
+  double tol;
+  double kh[6];      // K^H unique entries 00 01 02 11 12 22
+  double mean[3];    // scratch means
+  int done;          // 1 once every case meets tol
+  int iter;          // iterations performed
+  int nan;           // 1 if a NaN/Inf appeared
+  int first;         // 1 before the first beta
+  unsigned int counter[8];  // last-block tickets
+};
+
+enum Ticket { T_RZ = 0, T_PQ = 1, T_RR = 2, T_KH = 3, T_MEAN = 4, T_INIT = 5, T_RES = 6 };
+
+__device__ __forceinline__ bool solve_done(const SolveScalars* sc) {
+  return *((volatile const int*)&sc->done) != 0;
+}
+
+// Last-block ticket: returns true in every thread of the block that arrives last. The
+// partial sums written before are visible to it (threadfence before the ticket).
+__device__ __forceinline__ bool last_block(unsigned int* counter) {
+  __shared__ bool is_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned int prev = atomicAdd(counter, 1u);
+    is_last = (prev == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (is_last) __threadfence();
+  return is_last;
+}
+
+// Fixed-order sum of NV partial columns (partials[b * NV + i], b < nb) inside one block.
+template <int NV>
+__device__ __forceinline__ void reduce_partials(const double* partials, int nb, double (&out)[NV], double* smem) {
+  double v[NV];
+#pragma unroll
+  for (int i = 0; i < NV; i++) v[i] = 0.0;
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+#pragma unroll
+    for (int i = 0; i < NV; i++) v[i] += ((volatile const double*)partials)[b * NV + i];
+  }
+  block_reduce_f64<NV>(v, smem);
+#pragma unroll
+  for (int i = 0; i < NV; i++) out[i] = v[i];  // valid in thread 0
+}
+
+// ------------------------------------------------------------------------------------
+// Fine level: operator coefficients from the 8 element conductivities around a vertex.
+// k8[b] is the element whose lower corner is v - 1 + bits(b); it holds v as local node
+// 7 - b (homogenization/homoCommon.cuh:287-355). A(v, v+o) = c[|o|_0] * (sum of k8[b] over
+// the elements that contain both v and v+o): per axis o>0 needs bit 1, o<0 bit 0, o=0 any.
+// ------------------------------------------------------------------------------------
+template <int OX, int OY, int OZ>
+__device__ __forceinline__ float ksum(const float (&k8)[8]) {
+  float s = 0.f;
+#pragma unroll
+  for (int b = 0; b < 8; b++) {
+    const int bx = b & 1, by = (b >> 1) & 1, bz = b >> 2;
+    const bool okx = OX > 0 ? bx == 1 : (OX < 0 ? bx == 0 : true);
+    const bool oky = OY > 0 ? by == 1 : (OY < 0 ? by == 0 : true);
+    const bool okz = OZ > 0 ? bz == 1 : (OZ < 0 ? bz == 0 : true);
+    if (okx && oky && okz) s += k8[b];
+  }
+  return s;
+}
+
+template <int O>
+__device__ __forceinline__ float fine_coef(const float (&k8)[8], const FineOp& op) {
+  constexpr int ox = O % 3 - 1, oy = (O / 3) % 3 - 1, oz = O / 9 - 1;
+  constexpr int nzc = (ox != 0) + (oy != 0) + (oz != 0);
+  const float c = nzc == 0 ? op.c0 : (nzc == 1 ? op.c1 : (nzc == 2 ? op.c2 : op.c3));
+  return c * ksum<ox, oy, oz>(k8);
+}
+
+// Neighbour indices of (x,y,z) on a periodic grid: idx[o] for the 27 offsets.
+struct Nbr {
+  int xs[3];
+  size_t rows[9];  // (ys[b] + ny * zs[c]) * nx for b,c in 0..2, index b + 3c
+  __device__ __forceinline__ void init(const Dims& d, int x, int y, int z) {
+    xs[0] = wrapm(x - 1, d.nx);
+    xs[1] = x;
+    xs[2] = wrapm(x + 1, d.nx);
+    int ys[3] = {wrapm(y - 1, d.ny), y, wrapm(y + 1, d.ny)};
+    int zs[3] = {wrapm(z - 1, d.nz), z, wrapm(z + 1, d.nz)};
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+      for (int b = 0; b < 3; b++) rows[b + 3 * c] = (size_t(ys[b]) + size_t(d.ny) * zs[c]) * d.nx;
+  }
+  __device__ __forceinline__ size_t at(int o) const { return rows[o / 3] + xs[o % 3]; }
+};
+
+// The 8 element conductivities around vertex (x,y,z): element lower corners x-1..x etc.
+__device__ __forceinline__ void load_k8(const float* __restrict__ ks, const Nbr& nb, float (&k8)[8]) {
+#pragma unroll
+  for (int b = 0; b < 8; b++) {
+    const int bx = b & 1, by = (b >> 1) & 1, bz = b >> 2;
+    // element lower corner (x-1+bx, y-1+by, z-1+bz) = neighbour offset (bx-1, by-1, bz-1)
+    k8[b] = __ldg(ks + nb.rows[by + 3 * bz] + nb.xs[bx]);
+  }
+}
+
+template <int O>
+struct FineTerm {
+  // whether offset O carries a coefficient when face entries (c1) are structurally zero
+  static constexpr int ox = O % 3 - 1, oy = (O / 3) % 3 - 1, oz = O / 9 - 1;
+  static constexpr int nzc = (ox != 0) + (oy != 0) + (oz != 0);
+};
+
+// acc[c] -= sum_{o != 0} A(v, v+o) u_c[v+o] over the 3 cases; returns the diagonal.
+template <bool kFace, int NC>
+__device__ __forceinline__ float fine_offdiag(const float (&k8)[8], const FineOp& op, const Nbr& nb,
+                                              const float* u, size_t nv, float (&acc)[NC]) {
+#pragma unroll
+  for (int o = 0; o < 27; o++) {
+    if (o == 13) continue;
+    const int nzc = (o % 3 != 1) + ((o / 3) % 3 != 1) + (o / 9 != 1);
+    if (!kFace && nzc == 1) continue;
+    float coef;
+    switch (o) {
+#define OTM_FC(OO) \
+  case OO:         \
+    coef = fine_coef<OO>(k8, op); \
+    break;
+      OTM_FC(0) OTM_FC(1) OTM_FC(2) OTM_FC(3) OTM_FC(4) OTM_FC(5) OTM_FC(6) OTM_FC(7) OTM_FC(8)
+      OTM_FC(9) OTM_FC(10) OTM_FC(11) OTM_FC(12) OTM_FC(14) OTM_FC(15) OTM_FC(16) OTM_FC(17)
+      OTM_FC(18) OTM_FC(19) OTM_FC(20) OTM_FC(21) OTM_FC(22) OTM_FC(23) OTM_FC(24) OTM_FC(25) OTM_FC(26)
+#undef OTM_FC
+      default: coef = 0.f;
+    }
+    const size_t j = nb.at(o);
+#pragma unroll
+    for (int c = 0; c < NC; c++) acc[c] -= coef * u[c * nv + j];
+  }
+  float ksum8 = 0.f;
+#pragma unroll
+  for (int b = 0; b < 8; b++) ksum8 += k8[b];
+  return op.c0 * ksum8;
+}
+
+// One Gauss-Seidel colour pass on the fine level, omega = 1, all NC load cases
+// (homogenization/grid.cu:318-471 without the periodic padding; the pinned Dirichlet vertex
+// is replaced by mean projection in the outer solver).
+template <bool kFace, int NC>
+__global__ void __launch_bounds__(kBlock) k_gs_fine(Dims d, int color, const float* __restrict__ ks, FineOp op,
+                                                     float* u, const float* __restrict__ f, const SolveScalars* sc) {
+  if (sc && solve_done(sc)) return;
+  const int hx = d.nx >> 1, hy = d.ny >> 1;
+  const size_t nsub = d.nv() >> 3;
+  const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= nsub) return;
+  const int i = int(t % hx), j = int((t / hx) % hy), kq = int(t / (size_t(hx) * hy));
+  const int x = 2 * i + (color & 1), y = 2 * j + ((color >> 1) & 1), z = 2 * kq + (color >> 2);
+  Nbr nb;
+  nb.init(d, x, y, z);
+  float k8[8];
+  load_k8(ks, nb, k8);
+  const size_t nv = d.nv();
+  const size_t v = nb.at(13);
+  float acc[NC];
+#pragma unroll
+  for (int c = 0; c < NC; c++) acc[c] = __ldg(f + c * nv + v);
+  const float diag = fine_offdiag<kFace, NC>(k8, op, nb, u, nv, acc);
+  const float inv = 1.0f / diag;
+#pragma unroll
+  for (int c = 0; c < NC; c++) u[c * nv + v] = acc[c] * inv;
+}
+
+// r = f - A u on the fine level for every vertex.
+template <bool kFace, int NC>
+__global__ void __launch_bounds__(kBlock) k_resid_fine(Dims d, const float* __restrict__ ks, FineOp op,
+                                                        const float* __restrict__ u, const float* __restrict__ f,
+                                                        float* __restrict__ r, const SolveScalars* sc) {
+  if (sc && solve_done(sc)) return;
+  const size_t nv = d.nv();
+  const size_t v = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  const int x = int(v % d.nx), y = int((v / d.nx) % d.ny), z = int(v / (size_t(d.nx) * d.ny));
+  Nbr nb;
+  nb.init(d, x, y, z);
+  float k8[8];
+  load_k8(ks, nb, k8);
+  float acc[NC];
+#pragma unroll
+  for (int c = 0; c < NC; c++) acc[c] = __ldg(f + c * nv + v);
+  const float diag = fine_offdiag<kFace, NC>(k8, op, nb, u, nv, acc);
+#pragma unroll
+  for (int c = 0; c < NC; c++) r[c * nv + v] = acc[c] - diag * __ldg(u + c * nv + v);
+}
+
+// ------------------------------------------------------------------------------------
+// Coarse levels (27-point stencils, colour-blocked).
+// ------------------------------------------------------------------------------------
+__device__ __forceinline__ size_t cb_index(const Dims& d, int x, int y, int z) {
+  const int hx = d.nx >> 1, hy = d.ny >> 1;
+  const int color = (x & 1) + 2 * (y & 1) + 4 * (z & 1);
+  return size_t(color) * (d.nv() >> 3) + size_t(x >> 1) + size_t(hx) * (size_t(y >> 1) + size_t(hy) * (z >> 1));
+}
+
+template <int NC>
+__global__ void __launch_bounds__(kBlock) k_gs_coarse(Dims d, int color, const float* __restrict__ st, float* u,
+                                                       const float* __restrict__ f, const SolveScalars* sc) {
+  if (sc && solve_done(sc)) return;
+  const int hx = d.nx >> 1, hy = d.ny >> 1;
+  const size_t nsub = d.nv() >> 3;
+  const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= nsub) return;
+  const int i = int(t % hx), j = int((t / hx) % hy), kq = int(t / (size_t(hx) * hy));
+  const int x = 2 * i + (color & 1), y = 2 * j + ((color >> 1) & 1), z = 2 * kq + (color >> 2);
+  Nbr nb;
+  nb.init(d, x, y, z);
+  const size_t nv = d.nv();
+  const size_t v = nb.at(13);
+  const size_t sbase = size_t(color) * nsub + t;
+  float acc[NC];
+#pragma unroll
+  for (int c = 0; c < NC; c++) acc[c] = __ldg(f + c * nv + v);
+#pragma unroll
+  for (int o = 0; o < 27; o++) {
+    if (o == 13) continue;
+    const float s = __ldg(st + size_t(o) * nv + sbase);
+    const size_t jn = nb.at(o);
+#pragma unroll
+    for (int c = 0; c < NC; c++) acc[c] -= s * u[c * nv + jn];
+  }
+  const float inv = 1.0f / __ldg(st + size_t(13) * nv + sbase);
+#pragma unroll
+  for (int c = 0; c < NC; c++) u[c * nv + v] = acc[c] * inv;
+}
+
+template <int NC>
+__global__ void __launch_bounds__(kBlock) k_resid_coarse(Dims d, const float* __restrict__ st,
+                                                          const float* __restrict__ u, const float* __restrict__ f,
+                                                          float* __restrict__ r, const SolveScalars* sc) {
+  if (sc && solve_done(sc)) return;
+  const size_t nv = d.nv();
+  const size_t v = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  const int x = int(v % d.nx), y = int((v / d.nx) % d.ny), z = int(v / (size_t(d.nx) * d.ny));
+  Nbr nb;
+  nb.init(d, x, y, z);
+  const size_t sb = cb_index(d, x, y, z);
+  float acc[NC];
+#pragma unroll
+  for (int c = 0; c < NC; c++) acc[c] = __ldg(f + c * nv + v);
+#pragma unroll
+  for (int o = 0; o < 27; o++) {
+    const float s = __ldg(st + size_t(o) * nv + sb);
+    const size_t jn = nb.at(o);
+#pragma unroll
+    for (int c = 0; c < NC; c++) acc[c] -= s * __ldg(u + c * nv + jn);
+  }
+#pragma unroll
+  for (int c = 0; c < NC; c++) r[c * nv + v] = acc[c];
+}
+
+// f_c(V) = sum_d w(d) r_f(2V + d), w = prod (1 - |d|/2): full weighting = P^T
+// (homogenization/grid.cu:811-878).
+template <int NC>
+__global__ void __launch_bounds__(kBlock) k_restrict(Dims df, Dims dc, const float* __restrict__ r,
+                                                      float* __restrict__ fc, const SolveScalars* sc) {
+  if (sc && solve_done(sc)) return;
+  const size_t nvc = dc.nv(), nvf = df.nv();
+  const size_t V = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (V >= nvc) return;
+  const int X = int(V % dc.nx), Y = int((V / dc.nx) % dc.ny), Z = int(V / (size_t(dc.nx) * dc.ny));
+  Nbr nb;
+  nb.init(df, 2 * X, 2 * Y, 2 * Z);
+  float acc[NC];
+#pragma unroll
+  for (int c = 0; c < NC; c++) acc[c] = 0.f;
+#pragma unroll
+  for (int o = 0; o < 27; o++) {
+    const int ox = o % 3 - 1, oy = (o / 3) % 3 - 1, oz = o / 9 - 1;
+    const float w = (ox ? 0.5f : 1.f) * (oy ? 0.5f : 1.f) * (oz ? 0.5f : 1.f);
+    const size_t j = nb.at(o);
+#pragma unroll
+    for (int c = 0; c < NC; c++) acc[c] += w * __ldg(r + c * nvf + j);
+  }
+#pragma unroll
+  for (int c = 0; c < NC; c++) fc[c * nvc + V] = acc[c];
+}
+
+// u_f += P u_c, trilinear interpolation (homogenization/grid.cu:881-940).
+template <int NC>
+__global__ void __launch_bounds__(kBlock) k_prolong(Dims df, Dims dc, const float* __restrict__ uc, float* uf,
+                                                     const SolveScalars* sc) {
+  if (sc && solve_done(sc)) return;
+  const size_t nvc = dc.nv(), nvf = df.nv();
+  const size_t v = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (v >= nvf) return;
+  const int x = int(v % df.nx), y = int((v / df.nx) % df.ny), z = int(v / (size_t(df.nx) * df.ny));
+  const int X0 = x >> 1, Y0 = y >> 1, Z0 = z >> 1;
+  const int X1 = (x & 1) ? wrapm(X0 + 1, dc.nx) : X0;
+  const int Y1 = (y & 1) ? wrapm(Y0 + 1, dc.ny) : Y0;
+  const int Z1 = (z & 1) ? wrapm(Z0 + 1, dc.nz) : Z0;
+  const float wx1 = (x & 1) ? 0.5f : 0.f, wy1 = (y & 1) ? 0.5f : 0.f, wz1 = (z & 1) ? 0.5f : 0.f;
+  const float wx0 = 1.f - wx1, wy0 = 1.f - wy1, wz0 = 1.f - wz1;
+  const size_t r00 = (size_t(Y0) + size_t(dc.ny) * Z0) * dc.nx, r10 = (size_t(Y1) + size_t(dc.ny) * Z0) * dc.nx;
+  const size_t r01 = (size_t(Y0) + size_t(dc.ny) * Z1) * dc.nx, r11 = (size_t(Y1) + size_t(dc.ny) * Z1) * dc.nx;
+#pragma unroll
+  for (int c = 0; c < NC; c++) {
+    const float* u = uc + c * nvc;
+    const float a = wz0 * (wy0 * (wx0 * __ldg(u + r00 + X0) + wx1 * __ldg(u + r00 + X1)) +
+                           wy1 * (wx0 * __ldg(u + r10 + X0) + wx1 * __ldg(u + r10 + X1))) +
+                    wz1 * (wy0 * (wx0 * __ldg(u + r01 + X0) + wx1 * __ldg(u + r01 + X1)) +
+                           wy1 * (wx0 * __ldg(u + r11 + X0) + wx1 * __ldg(u + r11 + X1)));
+    uf[c * nvf + v] += a;
+  }
+}
+
+// ------------------------------------------------------------------------------------
+// Galerkin coarse operators (homogenization/grid_ex.cu:16-227, restrict_stencil_*).
+// ------------------------------------------------------------------------------------
+
+// Level 1 from the fine conductivity: A_1(V, V+O) = sum over the 4^3 fine elements around
+// 2V of k_e T[e][O], where T[e][O] = sum_ij P(p_i, V) KE_ij P(p_j, V+O) depends only on the
+// element's position relative to 2V (tabulated on the host, 64 x 27, scaled by the element
+// size). Element e = (ex,ey,ez) in 0..3 has its lower corner at 2V - 2 + (ex,ey,ez).
+static __global__ void __launch_bounds__(kBlock) k_galerkin_fine(Dims df, Dims dc, const float* __restrict__ ks,
+                                                           const float* __restrict__ table, float* __restrict__ st,
+                                                           int cb_out) {
+  __shared__ float T[64 * 27];
+  for (int i = threadIdx.x; i < 64 * 27; i += blockDim.x) T[i] = table[i];
+  __syncthreads();
+  const size_t nvc = dc.nv();
+  const size_t V = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (V >= nvc) return;
+  const int X = int(V % dc.nx), Y = int((V / dc.nx) % dc.ny), Z = int(V / (size_t(dc.nx) * dc.ny));
+  int xs[4], ys[4], zs[4];
+#pragma unroll
+  for (int a = 0; a < 4; a++) {
+    xs[a] = wrapm(2 * X - 2 + a, df.nx);
+    ys[a] = wrapm(2 * Y - 2 + a, df.ny);
+    zs[a] = wrapm(2 * Z - 2 + a, df.nz);
+  }
+  float acc[27];
+#pragma unroll
+  for (int o = 0; o < 27; o++) acc[o] = 0.f;
+#pragma unroll 1
+  for (int ez = 0; ez < 4; ez++)
+#pragma unroll
+    for (int ey = 0; ey < 4; ey++) {
+      const size_t row = (size_t(ys[ey]) + size_t(df.ny) * zs[ez]) * df.nx;
+#pragma unroll
+      for (int ex = 0; ex < 4; ex++) {
+        const float k = __ldg(ks + row + xs[ex]);
+        const float* Te = T + (ex + 4 * ey + 16 * ez) * 27;
+#pragma unroll
+        for (int o = 0; o < 27; o++) acc[o] += k * Te[o];
+      }
+    }
+  const size_t out = cb_out ? cb_index(dc, X, Y, Z) : V;
+#pragma unroll
+  for (int o = 0; o < 27; o++) st[size_t(o) * nvc + out] = acc[o];
+}
+
+// Per-axis coarse targets of a fine offset t = d + o in [-2, 2]: the coarse offsets O with
+// |t - 2 O| <= 1 and their trilinear weights.
+__device__ __forceinline__ int axis_targets(int t, int (&O)[2], float (&w)[2]) {
+  switch (t) {
+    case -2: O[0] = -1; w[0] = 1.f; return 1;
+    case -1: O[0] = -1; w[0] = 0.5f; O[1] = 0; w[1] = 0.5f; return 2;
+    case 0: O[0] = 0; w[0] = 1.f; return 1;
+    case 1: O[0] = 0; w[0] = 0.5f; O[1] = 1; w[1] = 0.5f; return 2;
+    default: O[0] = 1; w[0] = 1.f; return 1;
+  }
+}
+
+// Deeper levels: A_c(V, V+O) = sum_{d,o} P(2V+d, V) A_f(2V+d, o) P(2V+d+o, V+O).
+static __global__ void __launch_bounds__(kBlock) k_galerkin_coarse(Dims df, Dims dc, const float* __restrict__ stf,
+                                                             float* __restrict__ stc, int cb_out) {
+  const size_t nvc = dc.nv(), nvf = df.nv();
+  const size_t V = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (V >= nvc) return;
+  const int X = int(V % dc.nx), Y = int((V / dc.nx) % dc.ny), Z = int(V / (size_t(dc.nx) * dc.ny));
+  float acc[27];
+#pragma unroll
+  for (int o = 0; o < 27; o++) acc[o] = 0.f;
+#pragma unroll
+  for (int dd = 0; dd < 27; dd++) {
+    const int dx = dd % 3 - 1, dy = (dd / 3) % 3 - 1, dz = dd / 9 - 1;
+    const float wv = (dx ? 0.5f : 1.f) * (dy ? 0.5f : 1.f) * (dz ? 0.5f : 1.f);
+    const int fx = wrapm(2 * X + dx, df.nx), fy = wrapm(2 * Y + dy, df.ny), fz = wrapm(2 * Z + dz, df.nz);
+    const size_t sb = cb_index(df, fx, fy, fz);
+#pragma unroll
+    for (int o = 0; o < 27; o++) {
+      const float s = wv * __ldg(stf + size_t(o) * nvf + sb);
+      const int ox = o % 3 - 1, oy = (o / 3) % 3 - 1, oz = o / 9 - 1;
+      int Ox[2], Oy[2], Oz[2];
+      float wx[2], wy[2], wz[2];
+      const int nx = axis_targets(dx + ox, Ox, wx);
+      const int ny = axis_targets(dy + oy, Oy, wy);
+      const int nz = axis_targets(dz + oz, Oz, wz);
+#pragma unroll
+      for (int iz = 0; iz < 2; iz++)
+#pragma unroll
+        for (int iy = 0; iy < 2; iy++)
+#pragma unroll
+          for (int ix = 0; ix < 2; ix++) {
+            if (ix < nx && iy < ny && iz < nz) {
+              const int O = (Ox[ix] + 1) + 3 * (Oy[iy] + 1) + 9 * (Oz[iz] + 1);
+              acc[O] += s * wx[ix] * wy[iy] * wz[iz];
+            }
+          }
+    }
+  }
+  const size_t out = cb_out ? cb_index(dc, X, Y, Z) : V;
+#pragma unroll
+  for (int o = 0; o < 27; o++) stc[size_t(o) * nvc + out] = acc[o];
+}
+
+}  // namespace otm

@@ -1,0 +1,208 @@
+// otm_oc.cu -- OCOptimizer on the device (optimization/OCOptimizer.cu:12-152).
+//
+// The reference runs 20 host-driven bisection steps, each one kernel, one FP32 reduction and
+// one device-to-host copy. Here the whole bisection is a fixed sequence of kernels that keep
+// the multiplier bracket on the device (last-block finalisation, FP64 volume sums), so the
+// host never waits; a converged bisection turns the remaining steps into no-ops.
+#include <cuda_runtime.h>
+
+#include <cmath>
+
+#include "otm_common.cuh"
+#include "otm_mg_kernels.cuh"
+
+namespace otm {
+
+struct OcState {
+  double gmax, gmin, g, vol;
+  int done;
+  int iters;
+  unsigned int counter;
+  int pad;
+};
+
+constexpr int kOcSteps = 20;  // OCOptimizer.cu:69
+
+__device__ __forceinline__ float oc_new_rho(float s, float r, float g, float min_rho, float step, float damp) {
+  float B = -s / g;
+  if (B < 0.f) B = 0.01f;
+  float nr = (damp == 0.5f ? sqrtf(B) : powf(B, damp)) * r;
+  if (nr - r < -step) nr = r - step;
+  if (nr - r > step) nr = r + step;
+  if (nr < min_rho) nr = min_rho;
+  if (nr > 1.f) nr = 1.f;
+  return nr;
+}
+
+__global__ void __launch_bounds__(kBlock) k_oc_maxabs(int ne, const float* __restrict__ sens, double* partials,
+                                                      OcState* st) {
+  __shared__ double smem[32];
+  double m = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ne; i += gridDim.x * blockDim.x)
+    m = fmax(m, fabs(double(sens[i])));
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, off));
+  if ((threadIdx.x & 31) == 0) smem[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double b = 0.0;
+    for (int w = 0; w < (blockDim.x + 31) / 32; w++) b = fmax(b, smem[w]);
+    partials[blockIdx.x] = b;
+  }
+  if (last_block(&st->counter)) {
+    if (threadIdx.x == 0) {
+      double b = 0.0;
+      for (int i = 0; i < int(gridDim.x); i++) b = fmax(b, ((volatile double*)partials)[i]);
+      st->gmax = b;
+      st->gmin = 0.0;
+      st->g = b / 2;
+      st->done = 0;
+      st->iters = 0;
+      st->counter = 0;
+    }
+  }
+}
+
+// One bisection step: volume of the candidate density at g = (gmax + gmin) / 2.
+__global__ void __launch_bounds__(kBlock) k_oc_pass(int ne, const float* __restrict__ sens,
+                                                    const float* __restrict__ rho, float volratio, float min_rho,
+                                                    float step, float damp, double* partials, OcState* st) {
+  if (*((volatile int*)&st->done)) return;
+  __shared__ double smem[32];
+  const float g = float((st->gmax + st->gmin) / 2);
+  double v[1] = {0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ne; i += gridDim.x * blockDim.x)
+    v[0] += oc_new_rho(__ldg(sens + i), __ldg(rho + i), g, min_rho, step, damp);
+  block_reduce_f64<1>(v, smem);
+  if (threadIdx.x == 0) partials[blockIdx.x] = v[0];
+  if (last_block(&st->counter)) {
+    double t[1];
+    reduce_partials<1>(partials, gridDim.x, t, smem);
+    if (threadIdx.x == 0) {
+      const double vol = t[0] / ne;
+      st->vol = vol;
+      st->g = double(g);
+      st->iters += 1;
+      if (vol < volratio - 0.0001)
+        st->gmax = double(g);
+      else if (vol > volratio + 0.0001)
+        st->gmin = double(g);
+      else
+        st->done = 1;
+      if (st->iters >= kOcSteps) st->done = 1;
+      st->counter = 0;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_oc_apply(int ne, const float* __restrict__ sens, float* rho,
+                                                     float min_rho, float step, float damp, const OcState* st) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ne) return;
+  rho[i] = oc_new_rho(sens[i], rho[i], float(st->g), min_rho, step, damp);
+}
+
+// Sensitivity filter: periodic Linear weights, s_e <- sum w s rho / (sum w * rho_e).
+struct OcFilterWeights {
+  int half, taps;
+  float w[13 * 13 * 13];
+};
+
+__global__ void __launch_bounds__(256) k_oc_filter(Dims d, const float* __restrict__ sens,
+                                                   const float* __restrict__ rho, size_t pitch, float* __restrict__ out,
+                                                   OcFilterWeights fw) {
+  const size_t nv = d.nv();
+  const size_t v = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  const int x = int(v % d.nx), y = int((v / d.nx) % d.ny), z = int(v / (size_t(d.nx) * d.ny));
+  const int h = fw.half, w1 = 2 * h + 1;
+  float sum = 0.f, ws = 0.f;
+  for (int t = 0; t < fw.taps; t++) {
+    const int ox = t % w1 - h, oy = (t / w1) % w1 - h, oz = t / (w1 * w1) - h;
+    const int px = ((x + ox) % d.nx + d.nx) % d.nx, py = ((y + oy) % d.ny + d.ny) % d.ny,
+              pz = ((z + oz) % d.nz + d.nz) % d.nz;
+    const size_t q = (size_t(py) + size_t(d.ny) * pz) * pitch + px;
+    const float w = fw.w[t];
+    sum += __ldg(sens + q) * __ldg(rho + q) * w;
+    ws += w;
+  }
+  const size_t e = (size_t(y) + size_t(d.ny) * z) * pitch + x;
+  out[v] = sum / (ws * __ldg(rho + e));
+}
+
+__global__ void __launch_bounds__(256) k_copy_pitched(Dims d, const float* __restrict__ src, float* dst,
+                                                      size_t pitch) {
+  const size_t nv = d.nv();
+  const size_t v = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  const int x = int(v % d.nx);
+  dst[(v / d.nx) * pitch + x] = src[v];
+}
+
+}  // namespace otm
+
+using namespace otm;
+
+extern "C" {
+
+otm_status otm_oc_filter_sens(float* sens, const float* rho, size_t pitchT, const int reso[3], float radius,
+                              void* stream) {
+  if (!sens || !rho || !reso || reso[0] < 1 || reso[1] < 1 || reso[2] < 1) return OTM_ERR_INVALID_ARGUMENT;
+  const Dims d{reso[0], reso[1], reso[2]};
+  if (pitchT == 0) pitchT = size_t(d.nx);
+  if (pitchT < size_t(d.nx)) return OTM_ERR_INVALID_ARGUMENT;
+  const int h = int(radius + 0.5f);
+  if (!(radius > 0.f) || h > 6) {
+    set_error("filter radius must be in (0, 6.5)");
+    return OTM_ERR_INVALID_ARGUMENT;
+  }
+  OcFilterWeights fw;
+  fw.half = h;
+  fw.taps = (2 * h + 1) * (2 * h + 1) * (2 * h + 1);
+  float wsum = 0.f;
+  for (int t = 0; t < fw.taps; t++) {
+    const int ox = t % (2 * h + 1) - h, oy = t / (2 * h + 1) % (2 * h + 1) - h, oz = t / ((2 * h + 1) * (2 * h + 1)) - h;
+    const float q2 = float(ox * ox + oy * oy + oz * oz) / (radius * radius);
+    fw.w[t] = q2 < 1.f ? 1.f - std::sqrt(q2) : 0.f;  // WeightFunc<Linear>
+    wsum += fw.w[t];
+  }
+  for (int t = 0; t < fw.taps; t++) fw.w[t] /= wsum;
+  cudaStream_t s = (cudaStream_t)stream;
+  float* tmp = nullptr;
+  OTM_CUDA(cudaMallocAsync((void**)&tmp, d.nv() * sizeof(float), s));
+  k_oc_filter<<<ceil_div(d.nv(), 256), 256, 0, s>>>(d, sens, rho, pitchT, tmp, fw);
+  k_copy_pitched<<<ceil_div(d.nv(), 256), 256, 0, s>>>(d, tmp, sens, pitchT);
+  cudaError_t e = cudaGetLastError();
+  cudaFreeAsync(tmp, s);
+  if (e != cudaSuccess) return cuda_fail(e, "k_oc_filter");
+  return OTM_OK;
+}
+
+otm_status otm_oc_update(int ne, const float* sens, float* rho, float volratio, float min_rho, float step_limit,
+                         float damp, void* stream, int* iters_out) {
+  if (ne <= 0 || !sens || !rho) return OTM_ERR_INVALID_ARGUMENT;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int nb = std::min(kMaxPartials, std::max(1, (ne + kBlock - 1) / kBlock));
+  char* scratch = nullptr;
+  const size_t bytes = sizeof(OcState) + size_t(nb) * sizeof(double);
+  OTM_CUDA(cudaMallocAsync((void**)&scratch, bytes, s));
+  OcState* st = (OcState*)scratch;
+  double* partials = (double*)(scratch + sizeof(OcState));
+  cudaMemsetAsync(st, 0, sizeof(OcState), s);
+  k_oc_maxabs<<<nb, kBlock, 0, s>>>(ne, sens, partials, st);
+  for (int i = 0; i < kOcSteps; i++)
+    k_oc_pass<<<nb, kBlock, 0, s>>>(ne, sens, rho, volratio, min_rho, step_limit, damp, partials, st);
+  k_oc_apply<<<ceil_div(size_t(ne), kBlock), kBlock, 0, s>>>(ne, sens, rho, min_rho, step_limit, damp, st);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess && iters_out) {
+    OcState h;
+    e = cudaMemcpyAsync(&h, st, sizeof(OcState), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    *iters_out = h.iters;
+  }
+  cudaFreeAsync(scratch, s);
+  if (e != cudaSuccess) return cuda_fail(e, "otm_oc_update");
+  return OTM_OK;
+}
+
+}  // extern "C"

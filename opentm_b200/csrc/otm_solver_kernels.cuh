@@ -1,0 +1,568 @@
+// otm_solver_kernels.cuh -- import, right-hand sides, coarsest direct solve, Krylov vector
+// updates with deterministic FP64 reductions, K^H and sensitivity kernels.
+#pragma once
+
+#include "otm_mg_kernels.cuh"
+
+namespace otm {
+
+// Element macro field (disp, 8 x 3) and load matrix (feMu, 8 x 3) of the template matrix,
+// passed by value (homogenization/templateMatrix.cpp:84-85).
+struct ElemFields {
+  float disp[8][3];
+  float feMu[8][3];
+};
+
+// Grid-stride partition with a fixed block count so reductions are deterministic.
+__host__ __device__ inline int reduce_blocks(size_t n) {
+  size_t b = (n + kBlock - 1) / kBlock;
+  if (b > size_t(kMaxPartials)) b = kMaxPartials;
+  if (b < 1) b = 1;
+  return int(b);
+}
+
+// k_solver = 1e-9 + k^p from a pitched lexicographic field, k_raw keeps the input
+// (Grid_H::update + update_rho_kernel, homogenization/grid.cu:2465-2504, 2646-2662; the
+// floor is applied where the reference evaluates rho_penal, grid.cu:405).
+static __global__ void k_import(Dims d, const float* __restrict__ kin, int pitchT, float p, float* __restrict__ ks,
+                         float* __restrict__ kraw, int* bad) {
+  const size_t nv = d.nv();
+  const size_t e = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (e >= nv) return;
+  const int x = int(e % d.nx);
+  const size_t yz = e / d.nx;
+  const float k = __ldg(kin + yz * size_t(pitchT) + x);
+  if (!(k >= 0.f) || !isfinite(k)) atomicOr(bad, 1);
+  kraw[e] = k;
+  ks[e] = kRhoPenalMin + (p == 1.f ? k : powf(k, p));
+}
+
+// f_c(v) = sum_{elements e around v} k_e feMu[local(v)][c] for the 3 load cases
+// (enforce_unit_macro_strain_kernel_H, homogenization/grid.cu:1282-1327).
+static __global__ void __launch_bounds__(kBlock) k_rhs(Dims d, const float* __restrict__ ks, ElemFields ef,
+                                                 float* __restrict__ b) {
+  const size_t nv = d.nv();
+  const size_t v = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  const int x = int(v % d.nx), y = int((v / d.nx) % d.ny), z = int(v / (size_t(d.nx) * d.ny));
+  Nbr nb;
+  nb.init(d, x, y, z);
+  float k8[8];
+  load_k8(ks, nb, k8);
+  float acc[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+  for (int bb = 0; bb < 8; bb++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) acc[c] += k8[bb] * ef.feMu[7 - bb][c];
+#pragma unroll
+  for (int c = 0; c < 3; c++) b[c * nv + v] = acc[c];
+}
+
+// ---------------------------------------------------------------------------------------
+// Deterministic reductions (fixed grid, fixed order, last-block finalisation).
+// ---------------------------------------------------------------------------------------
+
+// Means of the 3 case vectors of a and b -> sc->mean[] (a), and the result of
+// subtracting them is done by k_sub_means. Used to project the RHS and the initial guess
+// onto the complement of the periodic nullspace (constants).
+static __global__ void __launch_bounds__(kBlock) k_sums2(size_t nv, const float* __restrict__ a,
+                                                  const float* __restrict__ b, double* partials,
+                                                  double* out6, unsigned int* counter) {
+  __shared__ double smem[32 * 6];
+  double v[6] = {0, 0, 0, 0, 0, 0};
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nv; i += size_t(gridDim.x) * blockDim.x) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      v[c] += a[c * nv + i];
+      v[3 + c] += b[c * nv + i];
+    }
+  }
+  block_reduce_f64<6>(v, smem);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int i = 0; i < 6; i++) partials[blockIdx.x * 6 + i] = v[i];
+  if (last_block(counter)) {
+    double r[6];
+    reduce_partials<6>(partials, gridDim.x, r, smem);
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int i = 0; i < 6; i++) out6[i] = r[i] / double(nv);
+      *counter = 0;
+    }
+  }
+}
+
+// a -= mean_a, b -= mean_b (per case), then ||a||^2 partials -> sc->bb when a is the RHS.
+static __global__ void __launch_bounds__(kBlock) k_sub_means(size_t nv, float* a, float* b, const double* means6) {
+  const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    a[c * nv + i] -= float(means6[c]);
+    b[c * nv + i] -= float(means6[3 + c]);
+  }
+}
+
+// r = b - A x on the fine level plus ||b||^2 and ||r||^2 -> sc (start of a Krylov solve).
+template <bool kFace>
+__global__ void __launch_bounds__(kBlock) k_init_residual(Dims d, const float* __restrict__ ks, FineOp op,
+                                                          const float* __restrict__ x, const float* __restrict__ b,
+                                                          float* __restrict__ r, double* partials,
+                                                          SolveScalars* sc) {
+  __shared__ double smem[32 * 6];
+  const size_t nv = d.nv();
+  double v[6] = {0, 0, 0, 0, 0, 0};
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nv; i += size_t(gridDim.x) * blockDim.x) {
+    const int xx = int(i % d.nx), yy = int((i / d.nx) % d.ny), zz = int(i / (size_t(d.nx) * d.ny));
+    Nbr nb;
+    nb.init(d, xx, yy, zz);
+    float k8[8];
+    load_k8(ks, nb, k8);
+    float acc[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) acc[c] = b[c * nv + i];
+    const float diag = fine_offdiag<kFace, 3>(k8, op, nb, x, nv, acc);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const float rc = acc[c] - diag * x[c * nv + i];
+      r[c * nv + i] = rc;
+      const double bc = b[c * nv + i];
+      v[c] += bc * bc;
+      v[3 + c] += double(rc) * rc;
+    }
+  }
+  block_reduce_f64<6>(v, smem);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int i = 0; i < 6; i++) partials[blockIdx.x * 6 + i] = v[i];
+  if (last_block(&sc->counter[T_INIT])) {
+    double t[6];
+    reduce_partials<6>(partials, gridDim.x, t, smem);
+    if (threadIdx.x == 0) {
+      bool all = true, bad = false;
+      for (int c = 0; c < 3; c++) {
+        sc->bb[c] = t[c];
+        sc->rr[c] = t[3 + c];
+        const double rel = sqrt(t[3 + c]) / (sqrt(t[c]) + 1e-10);
+        sc->relres[c] = rel;
+        if (!(rel <= sc->tol)) all = false;
+        if (!isfinite(rel)) bad = true;
+      }
+      sc->done = all ? 1 : 0;
+      sc->nan = bad ? 1 : 0;
+      sc->iter = 0;
+      sc->first = 1;
+      sc->counter[T_INIT] = 0;
+    }
+  }
+}
+
+// rho = r . z, zbar = mean z, rbar-correction; beta = rho / rho_old (0 on the first step).
+static __global__ void __launch_bounds__(kBlock) k_dot_rz(size_t nv, const float* __restrict__ r,
+                                                   const float* __restrict__ z, double* partials, SolveScalars* sc) {
+  if (solve_done(sc)) return;
+  __shared__ double smem[32 * 9];
+  double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nv; i += size_t(gridDim.x) * blockDim.x) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const double rc = r[c * nv + i], zc = z[c * nv + i];
+      v[c] += rc * zc;
+      v[3 + c] += zc;
+      v[6 + c] += rc;
+    }
+  }
+  block_reduce_f64<9>(v, smem);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int i = 0; i < 9; i++) partials[blockIdx.x * 9 + i] = v[i];
+  if (last_block(&sc->counter[T_RZ])) {
+    double t[9];
+    reduce_partials<9>(partials, gridDim.x, t, smem);
+    if (threadIdx.x == 0) {
+      for (int c = 0; c < 3; c++) {
+        const double zbar = t[3 + c] / double(nv);
+        // (z - zbar) . r = z . r - zbar * sum r
+        const double rz = t[c] - zbar * t[6 + c];
+        sc->zmean[c] = zbar;
+        sc->beta[c] = sc->first ? 0.0 : (sc->rz[c] != 0.0 ? rz / sc->rz[c] : 0.0);
+        sc->rz[c] = rz;
+      }
+      sc->first = 0;
+      sc->counter[T_RZ] = 0;
+    }
+  }
+}
+
+// p = (z - zbar) + beta p
+static __global__ void __launch_bounds__(kBlock) k_update_p(size_t nv, const float* __restrict__ z, float* p,
+                                                     const SolveScalars* sc) {
+  if (solve_done(sc)) return;
+  const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const float zb = float(sc->zmean[c]), be = float(sc->beta[c]);
+    p[c * nv + i] = (z[c * nv + i] - zb) + be * p[c * nv + i];
+  }
+}
+
+// q = A p on the fine level and alpha = rho / (p . q).
+template <bool kFace>
+__global__ void __launch_bounds__(kBlock) k_apply_dot(Dims d, const float* __restrict__ ks, FineOp op,
+                                                      const float* __restrict__ p, float* __restrict__ q,
+                                                      double* partials, SolveScalars* sc) {
+  if (solve_done(sc)) return;
+  __shared__ double smem[32 * 3];
+  const size_t nv = d.nv();
+  double v[3] = {0, 0, 0};
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nv; i += size_t(gridDim.x) * blockDim.x) {
+    const int xx = int(i % d.nx), yy = int((i / d.nx) % d.ny), zz = int(i / (size_t(d.nx) * d.ny));
+    Nbr nb;
+    nb.init(d, xx, yy, zz);
+    float k8[8];
+    load_k8(ks, nb, k8);
+    float acc[3] = {0.f, 0.f, 0.f};
+    const float diag = fine_offdiag<kFace, 3>(k8, op, nb, p, nv, acc);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const float pc = __ldg(p + c * nv + i);
+      const float qc = diag * pc - acc[c];
+      q[c * nv + i] = qc;
+      v[c] += double(pc) * qc;
+    }
+  }
+  block_reduce_f64<3>(v, smem);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int i = 0; i < 3; i++) partials[blockIdx.x * 3 + i] = v[i];
+  if (last_block(&sc->counter[T_PQ])) {
+    double t[3];
+    reduce_partials<3>(partials, gridDim.x, t, smem);
+    if (threadIdx.x == 0) {
+      for (int c = 0; c < 3; c++) sc->alpha[c] = t[c] != 0.0 ? sc->rz[c] / t[c] : 0.0;
+      sc->counter[T_PQ] = 0;
+    }
+  }
+}
+
+// x += alpha p, r -= alpha q, ||r||^2 -> relative residual and the done flag.
+static __global__ void __launch_bounds__(kBlock) k_update_xr(size_t nv, float* x, float* r, const float* __restrict__ p,
+                                                      const float* __restrict__ q, double* partials,
+                                                      SolveScalars* sc, int max_iter) {
+  if (solve_done(sc)) return;
+  __shared__ double smem[32 * 3];
+  float al[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) al[c] = float(sc->alpha[c]);
+  double v[3] = {0, 0, 0};
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nv; i += size_t(gridDim.x) * blockDim.x) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      x[c * nv + i] += al[c] * p[c * nv + i];
+      const float rc = r[c * nv + i] - al[c] * q[c * nv + i];
+      r[c * nv + i] = rc;
+      v[c] += double(rc) * rc;
+    }
+  }
+  block_reduce_f64<3>(v, smem);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int i = 0; i < 3; i++) partials[blockIdx.x * 3 + i] = v[i];
+  if (last_block(&sc->counter[T_RR])) {
+    double t[3];
+    reduce_partials<3>(partials, gridDim.x, t, smem);
+    if (threadIdx.x == 0) {
+      bool all = true, bad = false;
+      for (int c = 0; c < 3; c++) {
+        sc->rr[c] = t[c];
+        const double rel = sqrt(t[c]) / (sqrt(sc->bb[c]) + 1e-10);
+        sc->relres[c] = rel;
+        if (!(rel <= sc->tol)) all = false;
+        if (!isfinite(rel) || rel > 1e10) bad = true;
+      }
+      sc->iter += 1;
+      if (bad) sc->nan = 1;
+      if (all || bad || sc->iter >= max_iter) sc->done = 1;
+      sc->counter[T_RR] = 0;
+    }
+  }
+}
+
+// Stationary V-cycle iteration: r = b - A x with ||r||^2 -> relres/done (MG_H::solveEquation,
+// homogenization/MG.cpp:80-142), then x += z after the cycle (k_axpy_x).
+template <bool kFace>
+__global__ void __launch_bounds__(kBlock) k_resid_norm(Dims d, const float* __restrict__ ks, FineOp op,
+                                                       const float* __restrict__ x, const float* __restrict__ b,
+                                                       float* __restrict__ r, double* partials, SolveScalars* sc,
+                                                       int max_iter) {
+  if (solve_done(sc)) return;
+  __shared__ double smem[32 * 3];
+  const size_t nv = d.nv();
+  double v[3] = {0, 0, 0};
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nv; i += size_t(gridDim.x) * blockDim.x) {
+    const int xx = int(i % d.nx), yy = int((i / d.nx) % d.ny), zz = int(i / (size_t(d.nx) * d.ny));
+    Nbr nb;
+    nb.init(d, xx, yy, zz);
+    float k8[8];
+    load_k8(ks, nb, k8);
+    float acc[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) acc[c] = b[c * nv + i];
+    const float diag = fine_offdiag<kFace, 3>(k8, op, nb, x, nv, acc);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const float rc = acc[c] - diag * x[c * nv + i];
+      r[c * nv + i] = rc;
+      v[c] += double(rc) * rc;
+    }
+  }
+  block_reduce_f64<3>(v, smem);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int i = 0; i < 3; i++) partials[blockIdx.x * 3 + i] = v[i];
+  if (last_block(&sc->counter[T_RES])) {
+    double t[3];
+    reduce_partials<3>(partials, gridDim.x, t, smem);
+    if (threadIdx.x == 0) {
+      bool all = true, bad = false;
+      for (int c = 0; c < 3; c++) {
+        sc->rr[c] = t[c];
+        const double rel = sqrt(t[c]) / (sqrt(sc->bb[c]) + 1e-10);
+        sc->relres[c] = rel;
+        if (!(rel <= sc->tol)) all = false;
+        if (!isfinite(rel) || rel > 10.0) bad = true;  // "numerical explode", MG.cpp:392
+      }
+      if (bad) sc->nan = 1;
+      if (all || bad || sc->iter >= max_iter) sc->done = 1;
+      sc->counter[T_RES] = 0;
+    }
+  }
+}
+
+static __global__ void __launch_bounds__(kBlock) k_axpy_x(size_t nv, float* x, const float* __restrict__ z,
+                                                   SolveScalars* sc) {
+  if (solve_done(sc)) return;
+  const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < 3 * nv) x[i] += z[i];
+  if (i == 0) sc->iter += 1;
+}
+
+
+// 27-point stencil of the fine operator in lexicographic order (used when the fine level is
+// also the coarsest and is solved directly).
+static __global__ void __launch_bounds__(kBlock) k_fine_stencil(Dims d, const float* __restrict__ ks, FineOp op,
+                                                         float* __restrict__ st) {
+  const size_t nv = d.nv();
+  const size_t v = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  const int x = int(v % d.nx), y = int((v / d.nx) % d.ny), z = int(v / (size_t(d.nx) * d.ny));
+  Nbr nb;
+  nb.init(d, x, y, z);
+  float k8[8];
+  load_k8(ks, nb, k8);
+#define OTM_ST(OO) st[size_t(OO) * nv + v] = fine_coef<OO>(k8, op);
+  OTM_ST(0) OTM_ST(1) OTM_ST(2) OTM_ST(3) OTM_ST(4) OTM_ST(5) OTM_ST(6) OTM_ST(7) OTM_ST(8)
+  OTM_ST(9) OTM_ST(10) OTM_ST(11) OTM_ST(12) OTM_ST(13) OTM_ST(14) OTM_ST(15) OTM_ST(16) OTM_ST(17)
+  OTM_ST(18) OTM_ST(19) OTM_ST(20) OTM_ST(21) OTM_ST(22) OTM_ST(23) OTM_ST(24) OTM_ST(25) OTM_ST(26)
+#undef OTM_ST
+}
+
+// ---------------------------------------------------------------------------------------
+// Coarsest level: dense FP64 inverse of A_c + (alpha/n) 1 1^T (SPD on the periodic
+// nullspace), built once per update; each V-cycle applies it as a mat-vec. Replaces the
+// host BiCGSTAB(ILUT) + nullspace projection of Grid_H::solveHostEquation
+// (homogenization/grid.cpp:272-310).
+// ---------------------------------------------------------------------------------------
+static __global__ void k_coarsest_build(Dims d, const float* __restrict__ st, double* A, int* status) {
+  const int n = int(d.nv());
+  for (size_t i = threadIdx.x; i < size_t(n) * n; i += blockDim.x) A[i] = 0.0;
+  __syncthreads();
+  __shared__ double dsum;
+  if (threadIdx.x == 0) dsum = 0.0;
+  __syncthreads();
+  // row v assembled by one thread (handles periodic aliasing of small dims)
+  for (int v = threadIdx.x; v < n; v += blockDim.x) {
+    const int x = v % d.nx, y = (v / d.nx) % d.ny, z = v / (d.nx * d.ny);
+    for (int o = 0; o < 27; o++) {
+      const int jx = (x + o % 3 - 1 + d.nx) % d.nx, jy = (y + (o / 3) % 3 - 1 + d.ny) % d.ny,
+                jz = (z + o / 9 - 1 + d.nz) % d.nz;
+      const int j = jx + d.nx * (jy + d.ny * jz);
+      A[size_t(v) * n + j] += double(st[size_t(o) * n + v]);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int v = 0; v < n; v++) s += A[size_t(v) * n + v];
+    dsum = s;
+  }
+  __syncthreads();
+  const double alpha = dsum / double(n) / double(n);
+  for (size_t i = threadIdx.x; i < size_t(n) * n; i += blockDim.x) A[i] += alpha;
+  __syncthreads();
+  // in-place Gauss-Jordan inversion without pivoting (SPD)
+  __shared__ double piv_inv;
+  for (int k = 0; k < n; k++) {
+    if (threadIdx.x == 0) {
+      const double pv = A[size_t(k) * n + k];
+      if (!(pv > 0.0)) *status = 1;
+      piv_inv = 1.0 / pv;
+    }
+    __syncthreads();
+    const double pinv = piv_inv;
+    for (int j = threadIdx.x; j < n; j += blockDim.x)
+      if (j != k) A[size_t(k) * n + j] *= pinv;
+    __syncthreads();
+    for (size_t idx = threadIdx.x; idx < size_t(n) * n; idx += blockDim.x) {
+      const int i = int(idx / n), j = int(idx % n);
+      if (i != k && j != k) A[idx] -= A[size_t(i) * n + k] * A[size_t(k) * n + j];
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+      if (i != k) A[size_t(i) * n + k] *= -pinv;
+    __syncthreads();
+    if (threadIdx.x == 0) A[size_t(k) * n + k] = pinv;
+    __syncthreads();
+  }
+}
+
+// u = Ainv (f - mean f) for the 3 cases (one block).
+static __global__ void k_coarsest_solve(int n, const double* __restrict__ Ainv, const float* __restrict__ f, float* u,
+                                 const SolveScalars* sc) {
+  if (sc && solve_done(sc)) return;
+  extern __shared__ double bsh[];  // 3 * n
+  __shared__ double mean[3];
+  for (int i = threadIdx.x; i < 3 * n; i += blockDim.x) bsh[i] = f[i];
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double s = 0.0;
+    for (int i = 0; i < n; i++) s += bsh[threadIdx.x * n + i];
+    mean[threadIdx.x] = s / n;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    for (int j = 0; j < n; j++) {
+      const double m = Ainv[size_t(j) * n + i];  // symmetric: column read is coalesced
+      a0 += m * (bsh[j] - mean[0]);
+      a1 += m * (bsh[n + j] - mean[1]);
+      a2 += m * (bsh[2 * n + j] - mean[2]);
+    }
+    u[i] = float(a0);
+    u[n + i] = float(a1);
+    u[2 * n + i] = float(a2);
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// K^H and sensitivity (homogenization/homogenization.cu:13-153, 255-412).
+// ---------------------------------------------------------------------------------------
+
+// E_ab = d_a^T KE d_b for the 6 unique pairs, d_c = disp[:,c] - chi_c at the 8 corners.
+__device__ __forceinline__ void elem_energy(const Dims& d, size_t e, const float* __restrict__ chi, const FineOp& op,
+                                            const ElemFields& ef, float (&E)[6]) {
+  const size_t nv = d.nv();
+  const int x = int(e % d.nx), y = int((e / d.nx) % d.ny), z = int(e / (size_t(d.nx) * d.ny));
+  const int x1 = wrapm(x + 1, d.nx), y1 = wrapm(y + 1, d.ny), z1 = wrapm(z + 1, d.nz);
+  const size_t r00 = (size_t(y) + size_t(d.ny) * z) * d.nx, r10 = (size_t(y1) + size_t(d.ny) * z) * d.nx;
+  const size_t r01 = (size_t(y) + size_t(d.ny) * z1) * d.nx, r11 = (size_t(y1) + size_t(d.ny) * z1) * d.nx;
+  const size_t idx[8] = {r00 + x, r00 + x1, r10 + x, r10 + x1, r01 + x, r01 + x1, r11 + x, r11 + x1};
+  float dv[3][8];
+#pragma unroll
+  for (int c = 0; c < 3; c++)
+#pragma unroll
+    for (int j = 0; j < 8; j++) dv[c][j] = ef.disp[j][c] - __ldg(chi + c * nv + idx[j]);
+  // KE d using the Hamming structure: (KE d)_i = c0 d_i + c1 sum_{|i^j|=1} d_j + c2 sum_{|i^j|=2} d_j + c3 d_{7-i}
+  float Kd[3][8];
+#pragma unroll
+  for (int c = 0; c < 3; c++)
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const float s1 = dv[c][i ^ 1] + dv[c][i ^ 2] + dv[c][i ^ 4];
+      const float s2 = dv[c][i ^ 3] + dv[c][i ^ 5] + dv[c][i ^ 6];
+      Kd[c][i] = op.c0 * dv[c][i] + op.c1 * s1 + op.c2 * s2 + op.c3 * dv[c][i ^ 7];
+    }
+  int cnt = 0;
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int bq = a; bq < 3; bq++) {
+      float s = 0.f;
+#pragma unroll
+      for (int i = 0; i < 8; i++) s += dv[a][i] * Kd[bq][i];
+      E[cnt++] = s;
+    }
+}
+
+// K^H_ab = sum_e k_e E_ab(e) / vol with FP64 accumulation (vol = 1), -> sc->kh.
+static __global__ void __launch_bounds__(kBlock) k_heat_matrix(Dims d, const float* __restrict__ ks,
+                                                        const float* __restrict__ chi, FineOp op, ElemFields ef,
+                                                        double* partials, SolveScalars* sc) {
+  __shared__ double smem[32 * 6];
+  const size_t nv = d.nv();
+  double v[6] = {0, 0, 0, 0, 0, 0};
+  for (size_t e = size_t(blockIdx.x) * blockDim.x + threadIdx.x; e < nv; e += size_t(gridDim.x) * blockDim.x) {
+    float E[6];
+    elem_energy(d, e, chi, op, ef, E);
+    const double k = __ldg(ks + e);
+#pragma unroll
+    for (int i = 0; i < 6; i++) v[i] += k * double(E[i]);
+  }
+  block_reduce_f64<6>(v, smem);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int i = 0; i < 6; i++) partials[blockIdx.x * 6 + i] = v[i];
+  if (last_block(&sc->counter[T_KH])) {
+    double t[6];
+    reduce_partials<6>(partials, gridDim.x, t, smem);
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int i = 0; i < 6; i++) sc->kh[i] = t[i];
+      sc->counter[T_KH] = 0;
+    }
+  }
+}
+
+// sens_e = p k^(p-1) sum_{a<=b} E_ab (dC_ab + [a != b] dC_ba); pitched lexicographic output
+// with zeroed pitch padding (Sensitivity_kernel_opt_2_H + init_array, homogenization.cu:415-479).
+struct SensWeights {
+  float w[6];
+};
+
+static __global__ void __launch_bounds__(kBlock) k_sensitivity(Dims d, const float* __restrict__ kraw,
+                                                        const float* __restrict__ chi, FineOp op, ElemFields ef,
+                                                        SensWeights sw, float p, float* __restrict__ sens,
+                                                        int pitchT) {
+  const size_t total = size_t(pitchT) * d.ny * d.nz;
+  const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= total) return;
+  const int x = int(t % pitchT);
+  const size_t yz = t / pitchT;
+  if (x >= d.nx) {
+    sens[t] = 0.f;
+    return;
+  }
+  const size_t e = yz * d.nx + x;
+  float E[6];
+  elem_energy(d, e, chi, op, ef, E);
+  float s = 0.f;
+#pragma unroll
+  for (int i = 0; i < 6; i++) s += E[i] * sw.w[i];
+  const float pr = (p == 1.f) ? 1.f : p * powf(__ldg(kraw + e), p - 1.f);
+  sens[t] = s * pr;
+}
+
+// 6 unpitched fields of dK^H_ab / dk_e.
+static __global__ void __launch_bounds__(kBlock) k_energy_fields(Dims d, const float* __restrict__ chi, FineOp op,
+                                                          ElemFields ef, float* __restrict__ out) {
+  const size_t nv = d.nv();
+  const size_t e = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (e >= nv) return;
+  float E[6];
+  elem_energy(d, e, chi, op, ef, E);
+#pragma unroll
+  for (int i = 0; i < 6; i++) out[i * nv + e] = E[i];
+}
+
+}  // namespace otm

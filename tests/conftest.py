@@ -1,0 +1,11 @@
+"""Test configuration: the `gpu` marker selects tests that need a B200 (CUDA) device."""
+import os
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA (B200) device; parity tests through the C ABI")

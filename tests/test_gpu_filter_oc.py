@@ -1,0 +1,83 @@
+"""GPU parity of the density filter chain and the OC optimizer against the FP64 oracle."""
+import numpy as np
+import pytest
+
+import oracle as ora
+from opentm_b200 import workloads as wl
+from tests.helpers import rel_field
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+FILTER_TOL = 1e-5  # FP32 filter vs FP64 oracle, max-relative
+
+
+@pytest.mark.parametrize("weight,radius,periodic", [(1, 2.0, True), (1, 2.0, False), (0, 1.5, False),
+                                                     (0, 1.5, True), (1, 3.0, True)])
+def test_filter_forward_backward(weight, radius, periodic):
+    from opentm_b200 import filter_backward, filter_forward
+    shape = (12, 10, 14)
+    src = wl.uniform(21, int(np.prod(shape))).reshape(shape).astype(np.float32)
+    g = wl.uniform(22, int(np.prod(shape))).reshape(shape).astype(np.float32) - 0.5
+    reso = (shape[2], shape[1], shape[0])
+    dst, ws = filter_forward(torch.from_numpy(src).cuda(), reso, radius, weight, periodic)
+    ref, ref_ws = ora.conv_forward(src, weight, radius, periodic)
+    assert rel_field(dst.cpu().numpy(), ref)[0] <= FILTER_TOL
+    assert rel_field(ws.cpu().numpy(), ref_ws)[0] <= FILTER_TOL
+    gs = filter_backward(torch.from_numpy(g).cuda(), ws, reso, radius, weight, periodic)
+    ref_g = ora.conv_backward(g, ref_ws, weight, radius, periodic)
+    assert rel_field(gs.cpu().numpy(), ref_g)[0] <= FILTER_TOL
+
+
+def test_filter_pitched_source():
+    from opentm_b200 import filter_forward
+    shape = (8, 8, 8)
+    src = wl.uniform(23, 512).reshape(shape).astype(np.float32)
+    padded = torch.full((8, 8, 32), 99.0, device="cuda")
+    padded[:, :, :8] = torch.from_numpy(src).cuda()
+    dst, _ = filter_forward(padded, (8, 8, 8), 2.0, 1, True, src_pitchT=32)
+    ref, _ = ora.conv_forward(src, 1, 2.0, True)
+    assert rel_field(dst.cpu().numpy(), ref)[0] <= FILTER_TOL
+
+
+def test_density_chain_forward_backward():
+    from opentm_b200 import DensityFilter
+    shape = (16, 16, 16)
+    rho = wl.config2_density(16, seed=1)
+    df = DensityFilter((16, 16, 16), radius=2.0, weight=1, periodic=True, p=3.0, k0=1.0, kmin=1e-3)
+    k = df.forward(torch.from_numpy(rho).cuda()).cpu().numpy()
+    rf, ws = ora.conv_forward(rho, 1, 2.0, True)
+    k_ref = 1e-3 + rf ** 3 * (1 - 1e-3)
+    assert rel_field(k, k_ref)[0] <= FILTER_TOL
+    gk = wl.uniform(24, rho.size).reshape(shape).astype(np.float32)
+    g = df.backward(torch.from_numpy(gk).cuda()).cpu().numpy()
+    g_ref = ora.conv_backward(gk * 3 * rf ** 2 * (1 - 1e-3), ws, 1, 2.0, True)
+    assert rel_field(g, g_ref)[0] <= FILTER_TOL
+
+
+def test_oc_filter_sens():
+    from opentm_b200 import OCOptimizer
+    shape = (12, 12, 12)
+    rho = (0.1 + 0.9 * wl.uniform(25, 1728)).reshape(shape).astype(np.float32)
+    s = -wl.uniform(26, 1728).reshape(shape).astype(np.float32)
+    oc = OCOptimizer(1728)
+    st = torch.from_numpy(s.copy()).cuda()
+    oc.filterSens(st, torch.from_numpy(rho).cuda(), 12, (12, 12, 12), 2.0)
+    ref = ora.oc_filter_sens(s, rho, 2.0)
+    assert rel_field(st.cpu().numpy(), ref)[0] <= FILTER_TOL
+
+
+@pytest.mark.parametrize("vol,step", [(0.3, 0.2), (0.5, 0.02), (0.25, 0.05)])
+def test_oc_update(vol, step):
+    from opentm_b200 import OCOptimizer
+    n = 20 ** 3
+    rho = (0.2 + 0.3 * wl.uniform(27, n)).astype(np.float32)
+    s = (-wl.uniform(28, n) ** 2).astype(np.float32)
+    oc = OCOptimizer(n, 0.001, step, 0.5)
+    r = torch.from_numpy(rho.copy()).cuda()
+    it = oc.update(torch.from_numpy(s).cuda(), r, vol, want_iters=True)
+    ref, it_ref = ora.oc_update(s, rho, vol, 0.001, step, 0.5)
+    assert it == it_ref
+    np.testing.assert_allclose(r.cpu().numpy(), ref, rtol=2e-6, atol=2e-7)
+    assert abs(float(r.mean()) - vol) <= 1e-4 + 1e-6

@@ -1,0 +1,187 @@
+"""GPU parity of the homogenization path (K^H, element energies, sensitivity) against the FP64
+oracle, through the C ABI. Tolerances: K^H 1e-5 (norm-relative and per diagonal entry),
+sensitivity 1e-4 (max-relative and relative L2); see tests/helpers.py."""
+import numpy as np
+import pytest
+
+import oracle as ora
+from tests.helpers import DC_TEST, KH_TOL, SENS_TOL, oracle_solution, random_k, rel_c, rel_diag, rel_field
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu_run(k, tol=1e-6, pre=2, post=2, dC=DC_TEST, pitchT=-1, **kw):
+    from opentm_b200 import HomoConfig, Homogenization_H
+    nz, ny, nx = k.shape
+    H = Homogenization_H(HomoConfig(reso=(nx, ny, nz), femRelThres=tol, pre_smooth=pre, post_smooth=post,
+                                    max_iter=kw.pop("max_iter", 200), **kw))
+    if pitchT > 0:
+        kp = torch.zeros((nz, ny, pitchT), dtype=torch.float32, device="cuda")
+        kp[:, :, :nx] = torch.from_numpy(k).cuda()
+        H.update(kp, pitchT)
+    else:
+        H.update(torch.from_numpy(np.ascontiguousarray(k)).cuda())
+    C = H.heatMatrix()
+    E = H.element_energy().cpu().numpy()
+    sens = torch.empty(k.shape, dtype=torch.float32, device="cuda")
+    H.Sensitivity(dC, sens, -1, False)
+    torch.cuda.synchronize()
+    return H, C, E, sens.cpu().numpy()
+
+
+def check_against_oracle(k, C, E, sens, dC=DC_TEST):
+    ref = oracle_solution(k)
+    assert rel_c(C, ref["C"]) <= KH_TOL, (C, ref["C"])
+    assert rel_diag(C, ref["C"]) <= KH_TOL
+    for a in range(6):
+        mx, l2 = rel_field(E[a], ref["energy"][a])
+        assert mx <= SENS_TOL and l2 <= SENS_TOL, (a, mx, l2)
+    s_ref = ora.sensitivity(ref["energy"], k, dC)
+    mx, l2 = rel_field(sens, s_ref)
+    assert mx <= SENS_TOL and l2 <= SENS_TOL, (mx, l2)
+    return ref
+
+
+def test_uniform_density_gives_identity():
+    k = np.ones((16, 16, 16), dtype=np.float32)
+    _, C, _, _ = gpu_run(k)
+    np.testing.assert_allclose(C, np.eye(3), atol=1e-6)
+
+
+def test_laminate_closed_form():
+    # layers along storage x: reference K[1][1] (load case -x) is the harmonic mean,
+    # K[0][0] and K[2][2] the arithmetic mean (templateMatrix.cpp:74-85 axis convention)
+    k = np.ones((16, 16, 16), dtype=np.float32)
+    k[:, :, 0::2] = 1.0
+    k[:, :, 1::2] = 0.1
+    _, C, _, _ = gpu_run(k, tol=1e-7)
+    k1, k2 = 1.0 + 1e-9, 0.1 + 1e-9
+    arith, harm = (k1 + k2) / 2, 2.0 / (1 / k1 + 1 / k2)
+    assert abs(C[0, 0] - arith) / arith < 1e-5
+    assert abs(C[2, 2] - arith) / arith < 1e-5
+    assert abs(C[1, 1] - harm) / harm < 1e-5
+
+
+def test_config1_32_parity():
+    """Configuration 1: 32^3, rho ~ U(0.001,1) seed 0, SIMP p=3, V(2,2), tol 1e-6."""
+    k, _ = random_k((32, 32, 32), seed=0)
+    H, C, E, sens = gpu_run(k, tol=1e-6)
+    check_against_oracle(k, C, E, sens)
+    st = H.stats()
+    assert st.levels >= 3 and max(st.rel_res) <= 1e-6
+
+
+@pytest.mark.parametrize("shape", [(8, 8, 8), (16, 16, 16), (32, 16, 8), (24, 24, 24), (20, 20, 20), (4, 4, 4),
+                                   (6, 6, 6)])
+def test_shapes_parity(shape):
+    k, _ = random_k(shape, seed=sum(shape))
+    _, C, E, sens = gpu_run(k, tol=1e-7)
+    check_against_oracle(k, C, E, sens)
+
+
+def test_vcycle_solver_parity():
+    k, _ = random_k((16, 16, 16), seed=5)
+    _, C, E, sens = gpu_run(k, tol=1e-7, solver="vcycle")
+    check_against_oracle(k, C, E, sens)
+
+
+def test_v11_and_v33_cycles():
+    k, _ = random_k((16, 16, 16), seed=6)
+    for s in (1, 3):
+        _, C, E, sens = gpu_run(k, tol=1e-7, pre=s, post=s)
+        check_against_oracle(k, C, E, sens)
+
+
+def test_graphs_match_direct_launches_bitwise():
+    k, _ = random_k((16, 16, 16), seed=7)
+    _, C1, E1, s1 = gpu_run(k, use_graphs=True)
+    _, C2, E2, s2 = gpu_run(k, use_graphs=False)
+    assert np.array_equal(C1, C2) and np.array_equal(E1, E2) and np.array_equal(s1, s2)
+
+
+def test_deterministic_repeat():
+    k, _ = random_k((32, 32, 32), seed=8)
+    _, C1, _, s1 = gpu_run(k)
+    _, C2, _, s2 = gpu_run(k)
+    assert np.array_equal(C1, C2) and np.array_equal(s1, s2)
+
+
+def test_pitched_input_and_lexi_sensitivity():
+    k, _ = random_k((16, 16, 16), seed=9)
+    H, C, E, sens = gpu_run(k, pitchT=128)
+    check_against_oracle(k, C, E, sens)
+    pitched = torch.full((16, 16, 128), 7.0, dtype=torch.float32, device="cuda")
+    H.Sensitivity(DC_TEST, pitched, 128, True)
+    p = pitched.cpu().numpy()
+    np.testing.assert_array_equal(p[:, :, :16], sens)
+    assert np.all(p[:, :, 16:] == 0.0)  # pitch padding zeroed like init_array in the reference
+
+
+def test_warm_start_reduces_iterations():
+    from opentm_b200 import HomoConfig, Homogenization_H
+    k, _ = random_k((32, 32, 32), seed=10)
+    H = Homogenization_H(HomoConfig(reso=32, femRelThres=1e-6, pre_smooth=2, post_smooth=2))
+    H.update(torch.from_numpy(k).cuda())
+    H.heatMatrix()
+    cold = H.stats().iterations
+    k2 = (k * (1.0 + 0.01 * np.cos(np.arange(k.size)).reshape(k.shape))).astype(np.float32)
+    H.update(torch.from_numpy(k2).cuda())
+    C = H.heatMatrix()
+    warm = H.stats().iterations
+    assert warm < cold
+    ref = oracle_solution(k2)
+    assert rel_c(C, ref["C"]) <= KH_TOL
+
+
+def test_power_penal_sensitivity():
+    # power_penal != 1: solver uses 1e-9 + k^p, sensitivity carries p k^(p-1)
+    k, _ = random_k((8, 8, 8), seed=11)
+    from opentm_b200 import HomoConfig, Homogenization_H
+    H = Homogenization_H(HomoConfig(reso=8, femRelThres=1e-8, pre_smooth=2, post_smooth=2, power_penal=2.0))
+    H.update(torch.from_numpy(k).cuda())
+    C = H.heatMatrix()
+    sens = torch.empty(k.shape, dtype=torch.float32, device="cuda")
+    H.Sensitivity(DC_TEST, sens)
+    ref = ora.homogenize(k.astype(np.float64), power_penal=2.0, tol=1e-12, want_energy=True)
+    assert rel_c(C, ref["C"]) <= KH_TOL
+    s_ref = ora.sensitivity(ref["energy"], k, DC_TEST, power_penal=2.0)
+    mx, l2 = rel_field(sens.cpu().numpy(), s_ref)
+    assert mx <= SENS_TOL and l2 <= SENS_TOL
+
+
+def test_nan_input_is_rejected():
+    from opentm_b200 import HomoConfig, Homogenization_H, OtmError
+    k = np.ones((8, 8, 8), dtype=np.float32)
+    k[3, 3, 3] = np.nan
+    H = Homogenization_H(HomoConfig(reso=8))
+    H.update(torch.from_numpy(k).cuda())
+    with pytest.raises(OtmError) as ei:
+        H.heatMatrix()
+    assert ei.value.status == 7  # OTM_ERR_NAN
+
+
+def test_iteration_cap_reports_not_converged():
+    from opentm_b200 import HomoConfig, Homogenization_H, OtmError
+    k, _ = random_k((16, 16, 16), seed=12)
+    H = Homogenization_H(HomoConfig(reso=16, femRelThres=1e-12, max_iter=2, pre_smooth=1, post_smooth=1))
+    H.update(torch.from_numpy(k).cuda())
+    with pytest.raises(OtmError) as ei:
+        H.heatMatrix()
+    assert ei.value.status == 5  # OTM_ERR_NOT_CONVERGED
+    C = H.heatMatrix(allow_not_converged=True)
+    assert np.all(np.isfinite(C))
+
+
+def test_two_handles_are_independent():
+    from opentm_b200 import HomoConfig, Homogenization_H
+    ka, _ = random_k((16, 16, 16), seed=13)
+    kb, _ = random_k((8, 8, 8), seed=14)
+    Ha = Homogenization_H(HomoConfig(reso=16, femRelThres=1e-7, pre_smooth=2, post_smooth=2))
+    Hb = Homogenization_H(HomoConfig(reso=8, femRelThres=1e-7, pre_smooth=2, post_smooth=2))
+    Ha.update(torch.from_numpy(ka).cuda())
+    Hb.update(torch.from_numpy(kb).cuda())
+    Ca, Cb = Ha.heatMatrix(), Hb.heatMatrix()
+    assert rel_c(Ca, oracle_solution(ka)["C"]) <= KH_TOL
+    assert rel_c(Cb, oracle_solution(kb)["C"]) <= KH_TOL
