@@ -1,0 +1,357 @@
+"""Benchmark of the OpenTM homogenization hot path on B200.
+
+Workload (the configuration the headline metric is quoted on): the OC optimisation loop on a
+128^3 periodic cell -- rho0 = 0.3 + 0.05 U(-1,1) (seed 1), Linear density filter of radius 2
+(periodic), SIMP p = 3 (k0 = 1, kmin = 1e-3), maximise trace(K^H) at volume fraction 0.3,
+OC move limit 0.2, warm-started load cases, V(2,2)-preconditioned CG to ||r||/||f|| <= 1e-6.
+One step = one OC iteration = one homogenization solve (3 load cases, K^H, sensitivity,
+filter adjoint, OC update). The metric is solves/s with p50/p99 step latency.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Ours: every rank runs an independent replica on its own GPU (weak scaling, no data-path
+collective); the timed region is bracketed by barrier + synchronize, the per-rank device
+time is max-reduced, rank 0 prints one JSON line. The L2 cache (126 MB) is flushed by writing
+a 256 MB buffer before every timed step, outside the timed events.
+
+Reference arm (--impl reference): the reference cannot be built offline, so the FP64 CPU
+restatement of its algorithm (oracle/) runs the same loop on the host cores with all
+threads; each step is a bounded sample: the solve of one of the three load cases (cycling)
+plus the filter/OC work, so three steps make one OC iteration.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_CELL = 128
+TOL = 1e-6
+VOLFRAC = 0.3
+MOVE = 0.2
+DAMP = 0.5
+FILTER_R = 2.0
+P_SIMP, K0, KMIN = 3.0, 1.0, 1e-3
+METRIC = "solves/s & p50/p99 latency, mixed vs FP32 MG on one B200 at K^H err<=1e-5"
+UNIT = "solves/s"
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = [l.split(",") for l in open(self.path).read().strip().splitlines() if l.strip()]
+        os.unlink(self.path)
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax = max(smax, float(r[2]))
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------------
+# Our arm
+# ---------------------------------------------------------------------------------------
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    from opentm_b200 import DensityFilter, HomoConfig, Homogenization_H, OCOptimizer, launch_count
+    from opentm_b200 import workloads as wl
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    n = args.n
+    ne = n ** 3
+    rho0 = wl.config2_density(n, seed=1)
+
+    def make(precision):
+        H = Homogenization_H(HomoConfig(reso=n, femRelThres=TOL, pre_smooth=2, post_smooth=2, max_iter=200,
+                                        precision=precision, profile=True))
+        df = DensityFilter((n, n, n), FILTER_R, 1, True, P_SIMP, K0, KMIN)
+        oc = OCOptimizer(ne, 0.001, MOVE, DAMP)
+        return H, df, oc
+
+    dC = -np.eye(3)  # objective -trace(K^H)
+    g_k = torch.empty((n, n, n), dtype=torch.float32, device=dev)
+    g_rho = torch.empty_like(g_k)
+
+    def step(H, df, oc, rho):
+        k = df.forward(rho)
+        H.update(k)
+        C = H.heatMatrix()
+        H.Sensitivity(dC, g_k)
+        df.backward(g_k, g_rho)
+        oc.update(g_rho, rho, VOLFRAC)
+        return C
+
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > L2
+
+    def timed_loop(precision, steps, warmup, e2e=False):
+        H, df, oc = make(precision)
+        rho = torch.from_numpy(rho0).to(dev)
+        rho_host = torch.from_numpy(rho0.copy()).pin_memory()
+        out_host = torch.empty_like(rho_host).pin_memory()
+        for _ in range(warmup):
+            step(H, df, oc, rho)
+        H.profile(reset=True)
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        lat, Cs = [], []
+        l0 = launch_count()
+        for _ in range(steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            if e2e:
+                rho.copy_(rho_host, non_blocking=True)
+            C = step(H, df, oc, rho)
+            if e2e:
+                out_host.copy_(rho, non_blocking=True)
+            e1.record()
+            e1.synchronize()
+            if e2e:
+                rho_host.copy_(out_host)
+            lat.append(e0.elapsed_time(e1))
+            Cs.append(C)
+        torch.cuda.synchronize()
+        launches = launch_count() - l0
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        prof = H.profile(reset=True)
+        k_last = df.k.detach().cpu().numpy()
+        return {"lat_ms": lat, "C": Cs, "launches": launches, "prof": prof, "k_last": k_last,
+                "iters": H.stats().iterations}
+
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    main = timed_loop("fp32", args.steps, args.warmup)
+    clk = clocks.stop()
+    e2e = timed_loop("fp32", args.steps, args.warmup, e2e=True)
+    mixed = None
+    if args.mixed:
+        try:
+            mixed = timed_loop("bf16", args.steps, args.warmup)
+        except Exception as ex:  # precision form not available
+            mixed = {"error": str(ex)}
+
+    def total_s(res):
+        t = torch.tensor([sum(res["lat_ms"]) / 1e3], dtype=torch.float64, device=dev)
+        if world > 1:
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    t_main = total_s(main)
+    t_e2e = total_s(e2e)
+    t_mixed = total_s(mixed) if mixed and "lat_ms" in mixed else None
+    if rank != 0:
+        return None
+
+    value = args.steps * world / t_main
+    lat = np.array(main["lat_ms"])
+    hbm, peak_kind = load_peaks()
+    pr = main["prof"]
+    roofline = None
+    if pr.sweeps > 0:
+        launch_ms = pr.sweep_ms / pr.sweeps / pr.launches_per_sweep
+        bytes_launch = pr.sweep_bytes / pr.launches_per_sweep
+        achieved = bytes_launch / (launch_ms * 1e-3) / 1e9
+        traffic = None
+        tp = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tp):
+            traffic = json.load(open(tp)).get("k_gs_fine_bytes_per_launch_n128")
+        roofline = {"bound": "hbm", "kernel": "k_gs_fine (one colour pass, 3 load cases)",
+                    "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                    "frac": round(achieved / hbm, 4), "traffic": traffic,
+                    "peak_kind": f"{peak_kind} hbm_gbs", "launch_us": round(launch_ms * 1e3, 3),
+                    "algorithmic_bytes_per_launch": bytes_launch, "launches_timed": pr.sweeps * pr.launches_per_sweep}
+
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(t_main * 1e3 / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"OC loop, {n}^3 periodic cell, 3 load cases, V(2,2)-PCG to rel.res {TOL}",
+                   "reso": n, "tol": TOL, "l2": "flushed (256 MB write) before every timed step",
+                   "replicas": world, "precision": "fp32"},
+        "p50_ms": round(float(np.percentile(lat, 50)), 4), "p99_ms": round(float(np.percentile(lat, 99)), 4),
+        "pcg_iterations_last_step": main["iters"],
+        "e2e": {"value": round(args.steps * world / t_e2e, 3), "unit": UNIT, "h2d_bytes_per_step": 4 * ne,
+                "d2h_bytes_per_step": 4 * ne + 72},
+        "gpu_launches": int(main["launches"]),
+        "roofline": roofline,
+    }
+    if mixed is not None:
+        line["mixed"] = ({"value": round(args.steps * world / t_mixed, 3), "unit": UNIT, "precision": "bf16"}
+                         if t_mixed else mixed)
+    if clk:
+        line["clocks"] = clk
+    if world == 1 and not args.no_cpu:
+        line["cpu_baseline"], line["kh_err"] = cpu_baseline(main["k_last"], main["C"][-1])
+    print(json.dumps(line), flush=True)
+    return line
+
+
+def cpu_baseline(k_last, C_gpu):
+    """FP64 oracle (the reference algorithm restated) timed on the host cores for one solve of
+    the same workload (the density the GPU saw in its last timed step), and the K^H error of the
+    GPU result against it."""
+    import oracle as ora
+    ora.build()
+    k = k_last.astype(np.float64)
+    t = time.perf_counter()
+    r = ora.homogenize(k, tol=TOL, want_energy=True)
+    s = ora.sensitivity(r["energy"], k, -np.eye(3))
+    t_solve = time.perf_counter() - t
+    ref = ora.homogenize(k, tol=1e-10)
+    kh_err = float(np.abs(np.asarray(C_gpu) - ref["C"]).max() / np.abs(ref["C"]).max())
+    base = {"value": round(1.0 / t_solve, 5), "unit": UNIT, "cores": ora.num_threads(), "kind": "port",
+            "sample": f"one {k.shape[0]}^3 homogenization solve (3 load cases to {TOL}, K^H, sensitivity) in FP64 "
+                      f"with the multigrid-PCG restatement, {t_solve:.2f} s"}
+    del s
+    return base, kh_err
+
+
+# ---------------------------------------------------------------------------------------
+# Reference arm: the FP64 CPU restatement of the reference algorithm
+# ---------------------------------------------------------------------------------------
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    import oracle as ora
+    from opentm_b200 import workloads as wl
+
+    ora.build()
+    n = args.n
+    rho = wl.config2_density(n, seed=1).astype(np.float64)
+    state = {"k": None, "wsum": None, "rho_f": None, "energy": np.zeros((6,) + rho.shape)}
+
+    def sample(i):
+        c = i % 3
+        if c == 0:
+            rho_f, ws = ora.conv_forward(rho, 1, FILTER_R, True)
+            state["rho_f"], state["wsum"] = rho_f, ws
+            state["k"] = KMIN + rho_f ** P_SIMP * (K0 - KMIN)
+        r = ora.homogenize(state["k"], tol=TOL, want_energy=True, case_mask=1 << c)
+        state["energy"] += r["energy"]
+        if c == 2:
+            sk = ora.sensitivity(state["energy"], state["k"], -np.eye(3))
+            g = ora.conv_backward(sk * P_SIMP * state["rho_f"] ** (P_SIMP - 1) * (K0 - KMIN), state["wsum"], 1,
+                                  FILTER_R, True)
+            new, _ = ora.oc_update(g, rho, VOLFRAC, 0.001, MOVE, DAMP)
+            rho[...] = new
+            state["energy"][...] = 0.0
+
+    for i in range(args.warmup):
+        sample(i)
+    lat = []
+    for i in range(args.steps):
+        t = time.perf_counter()
+        sample(args.warmup + i)
+        lat.append(time.perf_counter() - t)
+    total = sum(lat)
+    value = (args.steps / 3.0) / total
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 5), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total * 1e3 / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"OC loop, {n}^3 periodic cell, 3 load cases, V(2,2)-PCG to rel.res {TOL}",
+                       "reso": n, "tol": TOL},
+            "cpu_baseline": {"value": round(value, 5), "unit": UNIT, "cores": ora.num_threads(), "kind": "port",
+                             "sample": "each step solves one of the 3 load cases (cycling) plus the filter/OC work "
+                                       "of the FP64 multigrid-PCG restatement; 3 steps = 1 solve"},
+            "e2e": {"value": round(value, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_CELL)
+    ap.add_argument("--mixed", type=int, default=1)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                             device_id=torch.device("cuda", local_rank))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -69,6 +69,8 @@ typedef struct otm_config {
   int warm_start;        /* reuse the previous solutions as initial guesses; default 1 (homogenization.cu:184) */
   int check_every;       /* iterations between host convergence checks; default 4 */
   int use_graphs;        /* capture the iteration loop in a CUDA graph; default 1 */
+  int profile;           /* time the first fine-level smoothing sweep of every iteration with CUDA
+                            events recorded inside the graph; default 0 */
 } otm_config;
 
 typedef struct otm_solve_stats {
@@ -79,6 +81,14 @@ typedef struct otm_solve_stats {
   int levels;             /* multigrid levels */
   int coarsest_reso[3];   /* coarsest level cells per axis */
 } otm_solve_stats;
+
+/* Event-timed fine-level smoother sweeps collected while profile != 0. */
+typedef struct otm_profile {
+  int sweeps;             /* sweeps timed (iterations that ran) */
+  double sweep_ms;        /* total milliseconds of those sweeps (8 colour launches each) */
+  double sweep_bytes;     /* algorithmic bytes of one sweep: nv * (4 + 3 * (4 + 4 + 4)) in FP32 */
+  int launches_per_sweep; /* kernel launches per sweep */
+} otm_profile;
 
 /* Pitched 3-D device array, layout-identical to cudaPitchedPtr. */
 typedef struct otm_pitched_ptr {
@@ -143,6 +153,11 @@ OTM_API otm_status otm_homo_set_solution(otm_homo* h, int lcase, const float* sr
 /* MG_H::reset_displacement (homogenization/MG.cpp:73-78): zero the kept solutions. */
 OTM_API otm_status otm_homo_reset_displacement(otm_homo* h);
 OTM_API otm_status otm_homo_get_stats(const otm_homo* h, otm_solve_stats* stats);
+/* Profile counters (see otm_config.profile); reset != 0 clears them after reading. */
+OTM_API otm_status otm_homo_get_profile(otm_homo* h, otm_profile* prof, int reset);
+
+/* Kernels this library has launched in the process (graph replays count their kernel nodes). */
+OTM_API uint64_t otm_launch_count(void);
 
 /* ---- density filter chain (AutoDiff/TensorExpression.h:640-644, 993-1185; .cuh:281-385) ---- */
 #define OTM_WEIGHT_SPLINE4 0

@@ -19,7 +19,12 @@ import numpy as np
 from . import _lib
 from ._lib import OtmError, check, default_config, i3, lib
 
-__all__ = [
+def launch_count() -> int:
+    """Kernels launched by the CUDA library in this process (graph replays count their nodes)."""
+    return int(lib().otm_launch_count())
+
+
+__all__ = ["launch_count", 
     "HomoConfig", "Homogenization_H", "OCOptimizer", "MMAOptimizer", "DensityFilter", "OtmError", "lib",
     "WEIGHT_SPLINE4", "WEIGHT_LINEAR", "filter_forward", "filter_backward",
 ]
@@ -61,6 +66,7 @@ class HomoConfig:
     warm_start: bool = True
     check_every: int = 4
     use_graphs: bool = True
+    profile: bool = False
 
     def to_c(self) -> _lib.Config:
         reso = self.reso if not isinstance(self.reso, int) else (self.reso,) * 3
@@ -69,7 +75,8 @@ class HomoConfig:
             pre_smooth=int(self.pre_smooth), post_smooth=int(self.post_smooth), solver=self.solver,
             precision=self.precision, coarsest_max_dof=int(self.coarsest_max_dof),
             power_penal=float(self.power_penal), warm_start=int(bool(self.warm_start)),
-            check_every=int(self.check_every), use_graphs=int(bool(self.use_graphs)))
+            check_every=int(self.check_every), use_graphs=int(bool(self.use_graphs)),
+            profile=int(bool(self.profile)))
 
 
 class Homogenization_H:
@@ -168,6 +175,11 @@ class Homogenization_H:
         """MG_H::reset_displacement (homogenization/MG.cpp:73-78)."""
         self._sync_stream()
         check(lib().otm_homo_reset_displacement(self._h), "otm_homo_reset_displacement")
+
+    def profile(self, reset: bool = True) -> _lib.Profile:
+        pr = _lib.Profile()
+        check(lib().otm_homo_get_profile(self._h, ctypes.byref(pr), int(bool(reset))), "otm_homo_get_profile")
+        return pr
 
     def stats(self) -> _lib.SolveStats:
         st = _lib.SolveStats()

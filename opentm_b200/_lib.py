@@ -48,6 +48,7 @@ class Config(ctypes.Structure):
         ("warm_start", ctypes.c_int),
         ("check_every", ctypes.c_int),
         ("use_graphs", ctypes.c_int),
+        ("profile", ctypes.c_int),
     ]
 
 
@@ -60,6 +61,11 @@ class SolveStats(ctypes.Structure):
         ("levels", ctypes.c_int),
         ("coarsest_reso", ctypes.c_int * 3),
     ]
+
+
+class Profile(ctypes.Structure):
+    _fields_ = [("sweeps", ctypes.c_int), ("sweep_ms", ctypes.c_double), ("sweep_bytes", ctypes.c_double),
+                ("launches_per_sweep", ctypes.c_int)]
 
 
 class PitchedPtr(ctypes.Structure):
@@ -94,6 +100,8 @@ SIGNATURES = {
     "otm_homo_set_solution": (_S, [_P, ctypes.c_int, _P]),
     "otm_homo_reset_displacement": (_S, [_P]),
     "otm_homo_get_stats": (_S, [_P, ctypes.POINTER(SolveStats)]),
+    "otm_homo_get_profile": (_S, [_P, ctypes.POINTER(Profile), ctypes.c_int]),
+    "otm_launch_count": (ctypes.c_uint64, []),
     "otm_filter_forward": (_S, [_I3, _P, ctypes.c_int, _P, ctypes.c_int, _P, ctypes.c_int, ctypes.c_float,
                                 ctypes.c_int, _P]),
     "otm_filter_backward": (_S, [_I3, _P, ctypes.c_int, _P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_float,

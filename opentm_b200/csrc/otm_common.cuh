@@ -18,6 +18,9 @@ constexpr int kBlock = 256;
 // Fixed upper bound on reduction partial slots per launch (deterministic ordering).
 constexpr int kMaxPartials = 2048;
 
+// Process-wide count of kernel launches issued by the library.
+void count_launches(uint64_t n);
+
 // Per-thread message of the last failure, returned by otm_last_error().
 void set_error(const std::string& msg);
 otm_status cuda_fail(cudaError_t e, const char* what);

@@ -154,6 +154,7 @@ otm_status otm_filter_forward(const int reso[3], const float* src, int src_pitch
   k_conv_forward<false><<<ceil_div(d.nv(), 256), 256, 0, (cudaStream_t)stream>>>(
       d, src, src_pitchT, dst, dst_pitchT, wsum, periodic, cw, 1.f, 1.f, 0.f, nullptr, nullptr);
   OTM_CHECK_LAUNCH("k_conv_forward");
+  count_launches(1);
   return OTM_OK;
 }
 
@@ -171,6 +172,7 @@ otm_status otm_filter_backward(const int reso[3], const float* g_dst, int g_dst_
   k_conv_backward<false><<<ceil_div(d.nv(), 256), 256, 0, (cudaStream_t)stream>>>(
       d, g_dst, g_dst_pitchT, nullptr, wsum, g_src, g_src_pitchT, periodic, cw);
   OTM_CHECK_LAUNCH("k_conv_backward");
+  count_launches(1);
   return OTM_OK;
 }
 
@@ -187,6 +189,7 @@ otm_status otm_density_forward(const int reso[3], const float* rho, int rho_pitc
   k_conv_forward<true><<<ceil_div(d.nv(), 256), 256, 0, (cudaStream_t)stream>>>(
       d, rho, rho_pitchT, rho_f, d.nx, wsum, periodic, cw, p, k0, kmin, k, dk);
   OTM_CHECK_LAUNCH("k_conv_forward<simp>");
+  count_launches(1);
   return OTM_OK;
 }
 
@@ -203,6 +206,7 @@ otm_status otm_density_backward(const int reso[3], const float* g_k, const float
   k_conv_backward<true><<<ceil_div(d.nv(), 256), 256, 0, (cudaStream_t)stream>>>(
       d, g_k, d.nx, dk, wsum, g_rho, g_rho_pitchT, periodic, cw);
   OTM_CHECK_LAUNCH("k_conv_backward<chain>");
+  count_launches(1);
   return OTM_OK;
 }
 

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -22,6 +23,9 @@
 namespace otm {
 
 static thread_local std::string g_last_error;
+static std::atomic<uint64_t> g_launches{0};
+
+void count_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 void set_error(const std::string& msg) { g_last_error = msg; }
 
@@ -55,6 +59,8 @@ static std::vector<Dims> level_dims(const int reso[3], int coarsest_max_dof) {
 
 static constexpr int kMaxCoarsest = 1024;
 
+static bool mixed_supported() { return false; }
+
 otm_status Homo::alloc(void** p, size_t bytes) {
   cudaError_t e = cudaMalloc(p, bytes);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc");
@@ -69,6 +75,9 @@ Homo::~Homo() {
   if (stream) cudaStreamDestroy(stream);
   if (ev_in) cudaEventDestroy(ev_in);
   if (ev_out) cudaEventDestroy(ev_out);
+  for (int a = 0; a < 2; a++)
+    for (int j = 0; j < kMaxChunk; j++)
+      if (prof_ev[a][j]) cudaEventDestroy(prof_ev[a][j]);
   for (void* p : allocations) cudaFree(p);
   if (sc_host) cudaFreeHost(sc_host);
 }
@@ -86,10 +95,15 @@ otm_status Homo::build(const otm_config& c) {
     return invalid("need at least one smoothing sweep");
   if (cfg.max_iter < 1) return invalid("max_iter must be >= 1");
   if (cfg.check_every < 1) cfg.check_every = 1;
+  if (cfg.check_every > kMaxChunk) cfg.check_every = kMaxChunk;
   if (cfg.coarsest_max_dof < 8) cfg.coarsest_max_dof = 8;
   if (cfg.solver != OTM_SOLVER_PCG && cfg.solver != OTM_SOLVER_VCYCLE) return invalid("unknown solver");
   if (cfg.precision < OTM_PRECISION_FP32 || cfg.precision > OTM_PRECISION_MIXED_FP16)
     return invalid("unknown precision");
+  if (cfg.precision != OTM_PRECISION_FP32 && !mixed_supported()) {
+    set_error("mixed-precision storage is not available in this build");
+    return OTM_ERR_UNSUPPORTED;
+  }
   if (cfg.solver == OTM_SOLVER_PCG && cfg.pre_smooth != cfg.post_smooth)
     return invalid("PCG needs a symmetric V-cycle (pre_smooth == post_smooth)");
 
@@ -115,6 +129,9 @@ otm_status Homo::build(const otm_config& c) {
   OTM_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   OTM_CUDA(cudaEventCreateWithFlags(&ev_in, cudaEventDisableTiming));
   OTM_CUDA(cudaEventCreateWithFlags(&ev_out, cudaEventDisableTiming));
+  if (cfg.profile)
+    for (int a = 0; a < 2; a++)
+      for (int j = 0; j < kMaxChunk; j++) OTM_CUDA(cudaEventCreate(&prof_ev[a][j]));
 
   lv.resize(dims.size());
   for (size_t l = 0; l < dims.size(); l++) {
@@ -186,6 +203,7 @@ otm_status Homo::update(const float* kin, int pitchT) {
   const size_t nv = d0.nv();
   k_import<<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(d0, kin, pitchT, cfg.power_penal, ks, kraw, flags);
   OTM_CHECK_LAUNCH("k_import");
+  launched(1);
   const int L = int(lv.size());
   for (int l = 1; l < L; l++) {
     const bool cb = (l < L - 1);  // smoothed levels use the colour-blocked stencil order
@@ -196,13 +214,16 @@ otm_status Homo::update(const float* kin, int pitchT) {
       k_galerkin_coarse<<<ceil_div(nvc, kBlock), kBlock, 0, stream>>>(lv[l - 1].d, lv[l].d, lv[l - 1].st, lv[l].st,
                                                                       cb);
     OTM_CHECK_LAUNCH("galerkin");
+    launched(1);
   }
   if (L == 1) {
     k_fine_stencil<<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(d0, ks, op, lv[0].st);
     OTM_CHECK_LAUNCH("k_fine_stencil");
+    launched(1);
   }
   k_coarsest_build<<<1, 1024, 0, stream>>>(lv.back().d, lv.back().st, Ainv, flags + 1);
   OTM_CHECK_LAUNCH("k_coarsest_build");
+  launched(1);
   updated = true;
   solved = false;
   return leave();
@@ -222,6 +243,7 @@ void Homo::gs(int l, int color) {
   } else {
     k_gs_coarse<3><<<ceil_div(nsub, kBlock), kBlock, 0, stream>>>(L.d, color, L.st, L.u, L.f, sc);
   }
+  launched(1);
 }
 
 void Homo::vcycle(int l) {
@@ -230,11 +252,16 @@ void Homo::vcycle(int l) {
   if (l == int(lv.size()) - 1) {
     k_coarsest_solve<<<1, std::min(1024, std::max(32, (nc + 31) / 32 * 32)), 3 * nc * sizeof(double), stream>>>(
         nc, Ainv, L.f, L.u, sc);
+    launched(1);
     return;
   }
   cudaMemsetAsync(L.u, 0, 3 * nv * sizeof(float), stream);
-  for (int s = 0; s < cfg.pre_smooth; s++)
+  for (int s = 0; s < cfg.pre_smooth; s++) {
+    const bool timed = cfg.profile && l == 0 && s == 0 && prof_slot >= 0;
+    if (timed) cudaEventRecord(prof_ev[0][prof_slot], stream);
     for (int c = 0; c < 8; c++) gs(l, c);
+    if (timed) cudaEventRecord(prof_ev[1][prof_slot], stream);
+  }
   if (l == 0) {
     if (face)
       k_resid_fine<true, 3><<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(L.d, ks, op, L.u, L.f, L.r, sc);
@@ -245,13 +272,16 @@ void Homo::vcycle(int l) {
   }
   Level& C = lv[l + 1];
   k_restrict<3><<<ceil_div(C.d.nv(), kBlock), kBlock, 0, stream>>>(L.d, C.d, L.r, C.f, sc);
+  launched(2);  // residual + restriction
   vcycle(l + 1);
   k_prolong<3><<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(L.d, C.d, C.u, L.u, sc);
+  launched(1);
   for (int s = 0; s < cfg.post_smooth; s++)
     for (int c = 7; c >= 0; c--) gs(l, c);
 }
 
-void Homo::iteration() {
+void Homo::iteration(int j) {
+  prof_slot = j;
   const Dims d0 = lv[0].d;
   const size_t nv = d0.nv();
   const int nb = reduce_blocks(nv);
@@ -266,6 +296,7 @@ void Homo::iteration() {
     else
       k_apply_dot<false><<<nb, kBlock, 0, stream>>>(d0, ks, op, p, q, partials, sc);
     k_update_xr<<<nb, kBlock, 0, stream>>>(nv, x, r, p, q, partials, sc, cfg.max_iter);
+    launched(4);
   } else {
     if (face)
       k_resid_norm<true><<<nb, kBlock, 0, stream>>>(d0, ks, op, x, b, r, partials, sc, cfg.max_iter);
@@ -273,12 +304,13 @@ void Homo::iteration() {
       k_resid_norm<false><<<nb, kBlock, 0, stream>>>(d0, ks, op, x, b, r, partials, sc, cfg.max_iter);
     vcycle(0);
     k_axpy_x<<<ceil_div(3 * nv, kBlock), kBlock, 0, stream>>>(nv, x, z, sc);
+    launched(2);
   }
 }
 
 otm_status Homo::run_chunk(int iters) {
   if (!cfg.use_graphs) {
-    for (int i = 0; i < iters; i++) iteration();
+    for (int i = 0; i < iters; i++) iteration(i);
     OTM_CHECK_LAUNCH("iteration");
     return OTM_OK;
   }
@@ -292,14 +324,25 @@ otm_status Homo::run_chunk(int iters) {
     g->solver = cfg.solver;
     cudaGraph_t graph;
     OTM_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-    for (int i = 0; i < iters; i++) iteration();
+    capturing = true;
+    for (int i = 0; i < iters; i++) iteration(i);
+    capturing = false;
     cudaError_t e = cudaStreamEndCapture(stream, &graph);
     if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    size_t nn = 0;
+    cudaGraphGetNodes(graph, nullptr, &nn);
+    std::vector<cudaGraphNode_t> nodes(nn);
+    cudaGraphGetNodes(graph, nodes.data(), &nn);
+    for (auto& nd : nodes) {
+      cudaGraphNodeType t;
+      if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) g->kernel_nodes++;
+    }
     e = cudaGraphInstantiate(&g->exec, graph, 0);
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
   }
   OTM_CUDA(cudaGraphLaunch(g->exec, stream));
+  count_launches(g->kernel_nodes);
   return OTM_OK;
 }
 
@@ -334,14 +377,28 @@ otm_status Homo::solve_impl() {
     else
       k_init_residual<false><<<nb, kBlock, 0, stream>>>(d0, ks, op, x, b, lv[0].f, partials, sc);
     OTM_CHECK_LAUNCH("solve init");
-    int launched = 0;
+    launched(4);
+    int nlaunched = 0, iter_before = 0;
+    bool first_check = true;
     while (true) {
       OTM_CUDA(cudaMemcpyAsync(sc_host, sc, sizeof(SolveScalars), cudaMemcpyDeviceToHost, stream));
       OTM_CUDA(cudaStreamSynchronize(stream));
-      if (sc_host->done || launched >= cfg.max_iter) break;
-      const int chunk = std::min(cfg.check_every, cfg.max_iter - launched);
+      if (cfg.profile && !first_check) {
+        const int ran = sc_host->iter - iter_before;
+        for (int j = 0; j < ran && j < kMaxChunk; j++) {
+          float ms = 0.f;
+          if (cudaEventElapsedTime(&ms, prof_ev[0][j], prof_ev[1][j]) == cudaSuccess) {
+            prof_ms += ms;
+            prof_sweeps++;
+          }
+        }
+      }
+      first_check = false;
+      iter_before = sc_host->iter;
+      if (sc_host->done || nlaunched >= cfg.max_iter) break;
+      const int chunk = std::min(cfg.check_every, cfg.max_iter - nlaunched);
       OTM_TRY(run_chunk(chunk));
-      launched += chunk;
+      nlaunched += chunk;
     }
     stats.iterations = sc_host->iter;
     for (int c = 0; c < 3; c++) stats.rel_res[c] = sc_host->relres[c];
@@ -389,6 +446,7 @@ otm_status Homo::heat_matrix(double C[9], bool do_solve) {
   const Dims d0 = lv[0].d;
   k_heat_matrix<<<reduce_blocks(d0.nv()), kBlock, 0, stream>>>(d0, ks, x, op, ef, partials, sc);
   OTM_CHECK_LAUNCH("k_heat_matrix");
+  launched(1);
   OTM_CUDA(cudaMemcpyAsync(sc_host->kh, sc->kh, 6 * sizeof(double), cudaMemcpyDeviceToHost, stream));
   OTM_CUDA(cudaStreamSynchronize(stream));
   int cnt = 0;
@@ -420,6 +478,7 @@ otm_status Homo::sensitivity(const float dC[9], float* sens, int pitchT, int lex
   k_sensitivity<<<ceil_div(total, kBlock), kBlock, 0, stream>>>(d0, kraw, x, op, ef, sw, cfg.power_penal, sens,
                                                                 pitchT);
   OTM_CHECK_LAUNCH("k_sensitivity");
+  launched(1);
   return leave();
 }
 
@@ -433,6 +492,7 @@ otm_status Homo::element_energy(float* out) {
   const Dims d0 = lv[0].d;
   k_energy_fields<<<ceil_div(d0.nv(), kBlock), kBlock, 0, stream>>>(d0, x, op, ef, out);
   OTM_CHECK_LAUNCH("k_energy_fields");
+  launched(1);
   return leave();
 }
 
@@ -487,6 +547,7 @@ otm_status otm_config_init(otm_config* cfg) {
   cfg->warm_start = 1;
   cfg->check_every = 4;
   cfg->use_graphs = 1;
+  cfg->profile = 0;
   return OTM_OK;
 }
 
@@ -585,6 +646,23 @@ otm_status otm_homo_reset_displacement(otm_homo* h) {
   H.solved = false;
   return H.leave();
 }
+
+otm_status otm_homo_get_profile(otm_homo* h, otm_profile* prof, int reset) {
+  if (!h || !prof) return OTM_ERR_INVALID_ARGUMENT;
+  Homo& H = h->impl;
+  const double nv = double(H.lv[0].d.nv());
+  prof->sweeps = H.prof_sweeps;
+  prof->sweep_ms = H.prof_ms;
+  prof->sweep_bytes = nv * (4.0 + 3.0 * (4.0 + 4.0 + 4.0));
+  prof->launches_per_sweep = 8;
+  if (reset) {
+    H.prof_sweeps = 0;
+    H.prof_ms = 0.0;
+  }
+  return OTM_OK;
+}
+
+uint64_t otm_launch_count(void) { return otm::g_launches.load(); }
 
 otm_status otm_homo_get_stats(const otm_homo* h, otm_solve_stats* stats) {
   if (!h || !stats) return OTM_ERR_INVALID_ARGUMENT;

@@ -24,8 +24,11 @@ struct Level {
 struct ChunkGraph {
   int iters = 0;
   int solver = 0;
+  uint64_t kernel_nodes = 0;
   cudaGraphExec_t exec = nullptr;
 };
+
+constexpr int kMaxChunk = 64;
 
 struct Homo {
   otm_config cfg{};
@@ -54,6 +57,12 @@ struct Homo {
   std::vector<void*> allocations;
   size_t bytes_allocated = 0;
   std::vector<ChunkGraph> graphs;
+  bool capturing = false;
+  // profiling: events around the first fine-level sweep of iteration j of a chunk
+  cudaEvent_t prof_ev[2][kMaxChunk] = {};
+  int prof_slot = -1;
+  int prof_sweeps = 0;
+  double prof_ms = 0.0;
   bool updated = false;
   bool solved = false;
   otm_solve_stats stats{};
@@ -66,7 +75,10 @@ struct Homo {
   otm_status update(const float* kin, int pitchT);
   void gs(int l, int color);
   void vcycle(int l);
-  void iteration();
+  void iteration(int j);
+  void launched(uint64_t n) {
+    if (!capturing) count_launches(n);
+  }
   otm_status run_chunk(int iters);
   otm_status solve_impl();
   otm_status solve(otm_solve_stats* out);

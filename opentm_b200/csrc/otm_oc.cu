@@ -175,6 +175,7 @@ otm_status otm_oc_filter_sens(float* sens, const float* rho, size_t pitchT, cons
   cudaError_t e = cudaGetLastError();
   cudaFreeAsync(tmp, s);
   if (e != cudaSuccess) return cuda_fail(e, "k_oc_filter");
+  count_launches(2);
   return OTM_OK;
 }
 
@@ -202,6 +203,7 @@ otm_status otm_oc_update(int ne, const float* sens, float* rho, float volratio, 
   }
   cudaFreeAsync(scratch, s);
   if (e != cudaSuccess) return cuda_fail(e, "otm_oc_update");
+  count_launches(2 + kOcSteps);
   return OTM_OK;
 }
 

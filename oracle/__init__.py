@@ -47,6 +47,9 @@ def lib():
         L.ora_homogenize.argtypes = [_I, _D, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                      ctypes.c_int, _D, _D, _D, _D]
         L.ora_homogenize.restype = ctypes.c_int
+        L.ora_homogenize_cases.argtypes = [_I, _D, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_int, ctypes.c_int, _D, _D, _D, _D]
+        L.ora_homogenize_cases.restype = ctypes.c_int
         L.ora_element_energy.argtypes = [_I, _D, _D]
         L.ora_sensitivity.argtypes = [_I, _D, _D, ctypes.c_double, _D, _D]
         L.ora_conv_forward.argtypes = [_I, _D, _D, _D, ctypes.c_int, ctypes.c_double, ctypes.c_int]
@@ -109,7 +112,8 @@ def rhs(k_solver: np.ndarray) -> np.ndarray:
 
 
 def homogenize(k: np.ndarray, power_penal: float = 1.0, tol: float = 1e-12, max_iter: int = 2000,
-               precond: int = 1, coarsest_max_dof: int = 64, want_chi: bool = False, want_energy: bool = False):
+               precond: int = 1, coarsest_max_dof: int = 64, want_chi: bool = False, want_energy: bool = False,
+               case_mask: int = 7):
     """K^H (3x3), and optionally chi (3, nz, ny, nx) and element energies (6, nz, ny, nx).
 
     ``k`` is the conductivity handed to the reference's ``update``; the solver adds the 1e-9
@@ -120,9 +124,10 @@ def homogenize(k: np.ndarray, power_penal: float = 1.0, tol: float = 1e-12, max_
     chi = np.zeros((3,) + kk.shape) if want_chi else None
     en = np.zeros((6,) + kk.shape) if want_energy else None
     rr = np.zeros(3)
-    it = lib().ora_homogenize(_dims(kk.shape), _dp(kk), float(power_penal), float(tol), int(max_iter), int(precond),
-                              int(coarsest_max_dof), _dp(C), _dp(chi) if chi is not None else None,
-                              _dp(en) if en is not None else None, _dp(rr))
+    it = lib().ora_homogenize_cases(_dims(kk.shape), _dp(kk), float(power_penal), float(tol), int(max_iter),
+                                    int(precond), int(coarsest_max_dof), int(case_mask), _dp(C),
+                                    _dp(chi) if chi is not None else None, _dp(en) if en is not None else None,
+                                    _dp(rr))
     return {"C": C.reshape(3, 3), "chi": chi, "energy": en, "iters": it, "relres": rr}
 
 

@@ -80,4 +80,5 @@ def test_oc_update(vol, step):
     ref, it_ref = ora.oc_update(s, rho, vol, 0.001, step, 0.5)
     assert it == it_ref
     np.testing.assert_allclose(r.cpu().numpy(), ref, rtol=2e-6, atol=2e-7)
-    assert abs(float(r.mean()) - vol) <= 1e-4 + 1e-6
+    if it < 20:  # bisection stopped inside the volume band (the move limit may make it unreachable)
+        assert abs(float(r.mean()) - vol) <= 1e-4 + 1e-6
