@@ -258,9 +258,11 @@ void Homo::vcycle(int l) {
   cudaMemsetAsync(L.u, 0, 3 * nv * sizeof(float), stream);
   for (int s = 0; s < cfg.pre_smooth; s++) {
     const bool timed = cfg.profile && l == 0 && s == 0 && prof_slot >= 0;
-    if (timed) cudaEventRecord(prof_ev[0][prof_slot], stream);
+    // inside a stream capture only an "external" event record becomes a graph node
+    const unsigned int evflag = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
+    if (timed) cudaEventRecordWithFlags(prof_ev[0][prof_slot], stream, evflag);
     for (int c = 0; c < 8; c++) gs(l, c);
-    if (timed) cudaEventRecord(prof_ev[1][prof_slot], stream);
+    if (timed) cudaEventRecordWithFlags(prof_ev[1][prof_slot], stream, evflag);
   }
   if (l == 0) {
     if (face)
@@ -390,6 +392,8 @@ otm_status Homo::solve_impl() {
           if (cudaEventElapsedTime(&ms, prof_ev[0][j], prof_ev[1][j]) == cudaSuccess) {
             prof_ms += ms;
             prof_sweeps++;
+          } else {
+            cudaGetLastError();  // a failed query must not surface at the next launch check
           }
         }
       }

@@ -139,7 +139,7 @@ def test_power_penal_sensitivity():
     # power_penal != 1: solver uses 1e-9 + k^p, sensitivity carries p k^(p-1)
     k, _ = random_k((8, 8, 8), seed=11)
     from opentm_b200 import HomoConfig, Homogenization_H
-    H = Homogenization_H(HomoConfig(reso=8, femRelThres=1e-8, pre_smooth=2, post_smooth=2, power_penal=2.0))
+    H = Homogenization_H(HomoConfig(reso=8, femRelThres=1e-6, pre_smooth=2, post_smooth=2, power_penal=2.0))
     H.update(torch.from_numpy(k).cuda())
     C = H.heatMatrix()
     sens = torch.empty(k.shape, dtype=torch.float32, device="cuda")
@@ -185,3 +185,18 @@ def test_two_handles_are_independent():
     Ca, Cb = Ha.heatMatrix(), Hb.heatMatrix()
     assert rel_c(Ca, oracle_solution(ka)["C"]) <= KH_TOL
     assert rel_c(Cb, oracle_solution(kb)["C"]) <= KH_TOL
+
+
+def test_profile_events_inside_graphs():
+    from opentm_b200 import HomoConfig, Homogenization_H
+    k, _ = random_k((32, 32, 32), seed=15)
+    for graphs in (True, False):
+        H = Homogenization_H(HomoConfig(reso=32, femRelThres=1e-6, pre_smooth=2, post_smooth=2, profile=True,
+                                        use_graphs=graphs))
+        H.update(torch.from_numpy(k).cuda())
+        H.heatMatrix()
+        pr = H.profile()
+        assert pr.sweeps == H.stats().iterations > 0
+        assert pr.sweep_ms > 0 and pr.sweep_bytes == 32 ** 3 * 40
+        # a following library call still works (no stale error from the event queries)
+        H.heatMatrix_nosolve()
