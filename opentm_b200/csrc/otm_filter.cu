@@ -57,74 +57,134 @@ static otm_status make_weights(int type, float radius, ConvWeights* cw) {
   return OTM_OK;
 }
 
-// Forward: out = sum_valid w src / sum_valid w; with fuse_simp it also writes
-// k = (k0 - kmin) out^p + kmin and dk = dk/dout.
-template <bool kSimp>
-__global__ void __launch_bounds__(256) k_conv_forward(Dims d, const float* __restrict__ src, int src_pitch,
-                                                      float* __restrict__ dst, int dst_pitch, float* __restrict__ wsum,
-                                                      int periodic, ConvWeights cw, float p, float k0, float kmin,
-                                                      float* __restrict__ kout, float* __restrict__ dkout) {
-  const size_t nv = d.nv();
-  const size_t v = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (v >= nv) return;
-  const int x = int(v % d.nx), y = int((v / d.nx) % d.ny), z = int(v / (size_t(d.nx) * d.ny));
-  const int h = cw.half, w1 = 2 * h + 1;
-  float sum = 0.f, ws = 0.f;
-  for (int t = 0; t < cw.taps; t++) {
-    const int ox = t % w1 - h, oy = (t / w1) % w1 - h, oz = t / (w1 * w1) - h;
-    int px = x + ox, py = y + oy, pz = z + oz;
-    const bool in = px >= 0 && px < d.nx && py >= 0 && py < d.ny && pz >= 0 && pz < d.nz;
-    if (!in) {
-      if (!periodic) continue;  // zero padding contributes nothing and no weight
-      px = ((px % d.nx) + d.nx) % d.nx;
-      py = ((py % d.ny) + d.ny) % d.ny;
-      pz = ((pz % d.nz) + d.nz) % d.nz;
+// Shared-memory tiled convolution: a 256-thread block produces a 32 x 8 x 4 tile of outputs
+// from the (32+2h) x (8+2h) x (4+2h) input tile it stages in shared memory (with periodic wrap
+// or a validity mask for zero padding), so each input value is read from global memory about
+// once instead of (2h+1)^3 times. The taps are summed in the reference's order (x fastest).
+//   MODE 0: forward            out = sum w src / sum_valid w
+//   MODE 1: forward + SIMP     also k = (k0 - kmin) out^p + kmin and dk = dk/dout
+//   MODE 2: adjoint            out = sum_off w g(i - off) / ws(i - off)
+//   MODE 3: adjoint chain      as 2 with g = g_k * dk
+constexpr int kTX = 32, kTY = 8, kTZ = 4;
+
+template <int H>
+constexpr int tile_elems() {
+  return (kTX + 2 * H) * (kTY + 2 * H) * (kTZ + 2 * H);
+}
+
+template <int H, int MODE>
+__global__ void __launch_bounds__(256) k_conv_tiled(Dims d, const float* __restrict__ src, int src_pitch,
+                                                    const float* __restrict__ dk_in, const float* __restrict__ ws_in,
+                                                    float* __restrict__ dst, int dst_pitch,
+                                                    float* __restrict__ ws_out, int periodic, ConvWeights cw,
+                                                    float wsum_all, float p, float k0, float kmin,
+                                                    float* __restrict__ kout, float* __restrict__ dkout) {
+  constexpr int SX = kTX + 2 * H, SY = kTY + 2 * H, SZ = kTZ + 2 * H, W1 = 2 * H + 1;
+  constexpr bool kFwd = MODE < 2;
+  extern __shared__ float sm[];
+  float* val = sm;
+  float* msk = sm + SX * SY * SZ;  // only used without periodicity
+  const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY, z0 = blockIdx.z * kTZ;
+  const int tid = threadIdx.y * kTX + threadIdx.x;
+  for (int i = tid; i < SX * SY * SZ; i += 256) {
+    const int lx = i % SX, ly = (i / SX) % SY, lz = i / (SX * SY);
+    int gx = x0 + lx - H, gy = y0 + ly - H, gz = z0 + lz - H;
+    const bool in = gx >= 0 && gx < d.nx && gy >= 0 && gy < d.ny && gz >= 0 && gz < d.nz;
+    float v = 0.f, m = 0.f;
+    if (in || periodic) {
+      gx = ((gx % d.nx) + d.nx) % d.nx;
+      gy = ((gy % d.ny) + d.ny) % d.ny;
+      gz = ((gz % d.nz) + d.nz) % d.nz;
+      const size_t row = size_t(gy) + size_t(d.ny) * gz;
+      v = __ldg(src + row * src_pitch + gx);
+      if (!kFwd) {
+        const size_t q = row * d.nx + gx;
+        if (MODE == 3) v *= __ldg(dk_in + q);
+        v /= __ldg(ws_in + q);
+      }
+      m = 1.f;
     }
-    const float w = cw.w[t];
-    sum += w * __ldg(src + (size_t(py) + size_t(d.ny) * pz) * src_pitch + px);
-    ws += w;
+    val[i] = v;
+    if (!periodic) msk[i] = m;
   }
-  const float out = sum / ws;
-  const size_t o = (size_t(y) + size_t(d.ny) * z) * dst_pitch + x;
-  if (dst) dst[o] = out;
-  if (wsum) wsum[v] = ws;
-  if (kSimp) {
-    const float pw = (p == 3.f) ? out * out * out : powf(out, p);
-    kout[v] = (k0 - kmin) * pw + kmin;
-    const float dpw = (p == 3.f) ? 3.f * out * out : p * powf(out, p - 1.f);
-    dkout[v] = (k0 - kmin) * dpw;
+  __syncthreads();
+  const int gx = x0 + threadIdx.x, gy = y0 + threadIdx.y;
+  if (gx >= d.nx || gy >= d.ny) return;
+#pragma unroll 1
+  for (int tz = 0; tz < kTZ; tz++) {
+    const int gz = z0 + tz;
+    if (gz >= d.nz) break;
+    float sum = 0.f, ws = 0.f;
+    // full unrolling (compile-time weight offsets) for the common radii, loops beyond
+    constexpr int UR = H <= 3 ? W1 : 1;
+#pragma unroll UR
+    for (int oz = -H; oz <= H; oz++)
+#pragma unroll UR
+      for (int oy = -H; oy <= H; oy++)
+#pragma unroll UR
+        for (int ox = -H; ox <= H; ox++) {
+          const float w = cw.w[(oz + H) * W1 * W1 + (oy + H) * W1 + (ox + H)];
+          const int sx = kFwd ? ox : -ox, sy = kFwd ? oy : -oy, sz = kFwd ? oz : -oz;
+          const int li = (tz + H + sz) * SX * SY + (threadIdx.y + H + sy) * SX + (threadIdx.x + H + sx);
+          sum += w * val[li];
+          if (kFwd && !periodic) ws += w * msk[li];
+        }
+    const size_t row = size_t(gy) + size_t(d.ny) * gz;
+    if (kFwd) {
+      if (periodic) ws = wsum_all;
+      const float out = sum / ws;
+      if (dst) dst[row * dst_pitch + gx] = out;
+      if (ws_out) ws_out[row * d.nx + gx] = ws;
+      if (MODE == 1) {
+        const float pw = (p == 3.f) ? out * out * out : powf(out, p);
+        kout[row * d.nx + gx] = (k0 - kmin) * pw + kmin;
+        const float dpw = (p == 3.f) ? 3.f * out * out : p * powf(out, p - 1.f);
+        dkout[row * d.nx + gx] = (k0 - kmin) * dpw;
+      }
+    } else {
+      dst[row * dst_pitch + gx] = sum;
+    }
   }
 }
 
-// Adjoint: g_src(i) = sum_off w(off) g(i - off) / ws(i - off); with kChain the incoming
-// gradient is g_k * dk (chain rule through the SIMP map, unarymap_backward).
-template <bool kChain>
-__global__ void __launch_bounds__(256) k_conv_backward(Dims d, const float* __restrict__ g, int g_pitch,
-                                                       const float* __restrict__ dk, const float* __restrict__ wsum,
-                                                       float* __restrict__ out, int out_pitch, int periodic,
-                                                       ConvWeights cw) {
-  const size_t nv = d.nv();
-  const size_t v = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (v >= nv) return;
-  const int x = int(v % d.nx), y = int((v / d.nx) % d.ny), z = int(v / (size_t(d.nx) * d.ny));
-  const int h = cw.half, w1 = 2 * h + 1;
-  float sum = 0.f;
-  for (int t = 0; t < cw.taps; t++) {
-    const int ox = t % w1 - h, oy = (t / w1) % w1 - h, oz = t / (w1 * w1) - h;
-    int px = x - ox, py = y - oy, pz = z - oz;
-    const bool in = px >= 0 && px < d.nx && py >= 0 && py < d.ny && pz >= 0 && pz < d.nz;
-    if (!in) {
-      if (!periodic) continue;
-      px = ((px % d.nx) + d.nx) % d.nx;
-      py = ((py % d.ny) + d.ny) % d.ny;
-      pz = ((pz % d.nz) + d.nz) % d.nz;
-    }
-    const size_t q = (size_t(py) + size_t(d.ny) * pz) * d.nx + px;
-    float gq = __ldg(g + (size_t(py) + size_t(d.ny) * pz) * g_pitch + px);
-    if (kChain) gq *= __ldg(dk + q);
-    sum += cw.w[t] * gq / __ldg(wsum + q);
+template <int H, int MODE>
+static otm_status launch_tiled(const Dims& d, const float* src, int src_pitch, const float* dk_in,
+                               const float* ws_in, float* dst, int dst_pitch, float* ws_out, int periodic,
+                               const ConvWeights& cw, float wsum_all, float p, float k0, float kmin, float* kout,
+                               float* dkout, cudaStream_t s) {
+  const size_t smem = size_t(tile_elems<H>()) * sizeof(float) * (periodic ? 1 : 2);
+  static bool attr = false;  // the attribute is per function and process-wide
+  if (!attr) {
+    cudaFuncSetAttribute(k_conv_tiled<H, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * tile_elems<H>() * 4);
+    attr = true;
   }
-  out[(size_t(y) + size_t(d.ny) * z) * out_pitch + x] = sum;
+  dim3 grid((d.nx + kTX - 1) / kTX, (d.ny + kTY - 1) / kTY, (d.nz + kTZ - 1) / kTZ);
+  k_conv_tiled<H, MODE><<<grid, dim3(kTX, kTY), smem, s>>>(d, src, src_pitch, dk_in, ws_in, dst, dst_pitch, ws_out,
+                                                          periodic, cw, wsum_all, p, k0, kmin, kout, dkout);
+  OTM_CHECK_LAUNCH("k_conv_tiled");
+  count_launches(1);
+  return OTM_OK;
+}
+
+template <int MODE>
+static otm_status conv_dispatch(const Dims& d, const float* src, int src_pitch, const float* dk_in,
+                                const float* ws_in, float* dst, int dst_pitch, float* ws_out, int periodic,
+                                const ConvWeights& cw, float p, float k0, float kmin, float* kout, float* dkout,
+                                cudaStream_t s) {
+  // sum of the normalised weights in the reference's tap order (the in-bounds weight of a
+  // periodic filter)
+  float wsum_all = 0.f;
+  for (int t = 0; t < cw.taps; t++) wsum_all += cw.w[t];
+  switch (cw.half) {
+#define OTM_H(HH) \
+  case HH:        \
+    return launch_tiled<HH, MODE>(d, src, src_pitch, dk_in, ws_in, dst, dst_pitch, ws_out, periodic, cw, wsum_all, \
+                                  p, k0, kmin, kout, dkout, s);
+    OTM_H(0) OTM_H(1) OTM_H(2) OTM_H(3) OTM_H(4) OTM_H(5) OTM_H(6)
+#undef OTM_H
+  }
+  set_error("unsupported filter half width");
+  return OTM_ERR_UNSUPPORTED;
 }
 
 static otm_status check_reso(const int reso[3]) {
@@ -151,11 +211,8 @@ otm_status otm_filter_forward(const int reso[3], const float* src, int src_pitch
   if (src_pitchT < d.nx || dst_pitchT < d.nx) return OTM_ERR_INVALID_ARGUMENT;
   ConvWeights cw;
   OTM_TRY(make_weights(weight_type, radius, &cw));
-  k_conv_forward<false><<<ceil_div(d.nv(), 256), 256, 0, (cudaStream_t)stream>>>(
-      d, src, src_pitchT, dst, dst_pitchT, wsum, periodic, cw, 1.f, 1.f, 0.f, nullptr, nullptr);
-  OTM_CHECK_LAUNCH("k_conv_forward");
-  count_launches(1);
-  return OTM_OK;
+  return conv_dispatch<0>(d, src, src_pitchT, nullptr, nullptr, dst, dst_pitchT, wsum, periodic, cw, 1.f, 1.f, 0.f,
+                         nullptr, nullptr, (cudaStream_t)stream);
 }
 
 otm_status otm_filter_backward(const int reso[3], const float* g_dst, int g_dst_pitchT, const float* wsum,
@@ -169,11 +226,8 @@ otm_status otm_filter_backward(const int reso[3], const float* g_dst, int g_dst_
   if (g_dst_pitchT < d.nx || g_src_pitchT < d.nx) return OTM_ERR_INVALID_ARGUMENT;
   ConvWeights cw;
   OTM_TRY(make_weights(weight_type, radius, &cw));
-  k_conv_backward<false><<<ceil_div(d.nv(), 256), 256, 0, (cudaStream_t)stream>>>(
-      d, g_dst, g_dst_pitchT, nullptr, wsum, g_src, g_src_pitchT, periodic, cw);
-  OTM_CHECK_LAUNCH("k_conv_backward");
-  count_launches(1);
-  return OTM_OK;
+  return conv_dispatch<2>(d, g_dst, g_dst_pitchT, nullptr, wsum, g_src, g_src_pitchT, nullptr, periodic, cw, 1.f,
+                         1.f, 0.f, nullptr, nullptr, (cudaStream_t)stream);
 }
 
 otm_status otm_density_forward(const int reso[3], const float* rho, int rho_pitchT, float* rho_f, float* k,
@@ -186,11 +240,8 @@ otm_status otm_density_forward(const int reso[3], const float* rho, int rho_pitc
   if (rho_pitchT < d.nx) return OTM_ERR_INVALID_ARGUMENT;
   ConvWeights cw;
   OTM_TRY(make_weights(weight_type, radius, &cw));
-  k_conv_forward<true><<<ceil_div(d.nv(), 256), 256, 0, (cudaStream_t)stream>>>(
-      d, rho, rho_pitchT, rho_f, d.nx, wsum, periodic, cw, p, k0, kmin, k, dk);
-  OTM_CHECK_LAUNCH("k_conv_forward<simp>");
-  count_launches(1);
-  return OTM_OK;
+  return conv_dispatch<1>(d, rho, rho_pitchT, nullptr, nullptr, rho_f, d.nx, wsum, periodic, cw, p, k0, kmin, k, dk,
+                         (cudaStream_t)stream);
 }
 
 otm_status otm_density_backward(const int reso[3], const float* g_k, const float* dk, const float* wsum,
@@ -203,11 +254,8 @@ otm_status otm_density_backward(const int reso[3], const float* g_k, const float
   if (g_rho_pitchT < d.nx) return OTM_ERR_INVALID_ARGUMENT;
   ConvWeights cw;
   OTM_TRY(make_weights(weight_type, radius, &cw));
-  k_conv_backward<true><<<ceil_div(d.nv(), 256), 256, 0, (cudaStream_t)stream>>>(
-      d, g_k, d.nx, dk, wsum, g_rho, g_rho_pitchT, periodic, cw);
-  OTM_CHECK_LAUNCH("k_conv_backward<chain>");
-  count_launches(1);
-  return OTM_OK;
+  return conv_dispatch<3>(d, g_k, d.nx, dk, wsum, g_rho, g_rho_pitchT, nullptr, periodic, cw, 1.f, 1.f, 0.f, nullptr,
+                         nullptr, (cudaStream_t)stream);
 }
 
 }  // extern "C"

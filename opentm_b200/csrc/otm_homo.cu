@@ -59,7 +59,7 @@ static std::vector<Dims> level_dims(const int reso[3], int coarsest_max_dof) {
 
 static constexpr int kMaxCoarsest = 1024;
 
-static bool mixed_supported() { return false; }
+static bool mixed_supported() { return true; }
 
 otm_status Homo::alloc(void** p, size_t bytes) {
   cudaError_t e = cudaMalloc(p, bytes);
@@ -119,6 +119,8 @@ otm_status Homo::build(const otm_config& c) {
     return OTM_ERR_UNSUPPORTED;
   }
   op = FineOp{float(tm.c[0]), float(tm.c[1]), float(tm.c[2]), float(tm.c[3])};
+  op0 = FineOp{1.f, float(tm.c[1] / tm.c[0]), float(tm.c[2] / tm.c[0]), float(tm.c[3] / tm.c[0])};
+  mixed = cfg.precision != OTM_PRECISION_FP32;
   face = !tm.face_zero;
   for (int j = 0; j < 8; j++)
     for (int cc = 0; cc < 3; cc++) {
@@ -138,12 +140,16 @@ otm_status Homo::build(const otm_config& c) {
     Level& L = lv[l];
     L.d = dims[l];
     const size_t nv = L.d.nv();
-    OTM_TRY(alloc((void**)&L.u, 3 * nv * sizeof(float)));
+    // the mixed form keeps the fine-level correction and residual in 16-bit buffers instead
+    const bool fp32_fine = !(mixed && l == 0 && dims.size() > 1);
+    if (fp32_fine) {
+      OTM_TRY(alloc((void**)&L.u, 3 * nv * sizeof(float)));
+      OTM_TRY(alloc((void**)&L.r, 3 * nv * sizeof(float)));
+      OTM_CUDA(cudaMemsetAsync(L.u, 0, 3 * nv * sizeof(float), stream));
+      OTM_CUDA(cudaMemsetAsync(L.r, 0, 3 * nv * sizeof(float), stream));
+    }
     OTM_TRY(alloc((void**)&L.f, 3 * nv * sizeof(float)));
-    OTM_TRY(alloc((void**)&L.r, 3 * nv * sizeof(float)));
-    OTM_CUDA(cudaMemsetAsync(L.u, 0, 3 * nv * sizeof(float), stream));
     OTM_CUDA(cudaMemsetAsync(L.f, 0, 3 * nv * sizeof(float), stream));
-    OTM_CUDA(cudaMemsetAsync(L.r, 0, 3 * nv * sizeof(float), stream));
     if (l > 0 || dims.size() == 1) OTM_TRY(alloc((void**)&L.st, 27 * nv * sizeof(float)));
   }
   const size_t nv = lv[0].d.nv();
@@ -151,10 +157,23 @@ otm_status Homo::build(const otm_config& c) {
   OTM_TRY(alloc((void**)&kraw, nv * sizeof(float)));
   OTM_TRY(alloc((void**)&b, 3 * nv * sizeof(float)));
   OTM_TRY(alloc((void**)&x, 3 * nv * sizeof(float)));
-  OTM_TRY(alloc((void**)&p, 3 * nv * sizeof(float)));
-  OTM_TRY(alloc((void**)&q, 3 * nv * sizeof(float)));
   OTM_CUDA(cudaMemsetAsync(x, 0, 3 * nv * sizeof(float), stream));
-  OTM_CUDA(cudaMemsetAsync(p, 0, 3 * nv * sizeof(float), stream));
+  if (mixed) {
+    if (lv.size() == 1) {
+      set_error("mixed precision needs at least two multigrid levels");
+      return OTM_ERR_UNSUPPORTED;
+    }
+    OTM_TRY(alloc((void**)&x64, 3 * nv * sizeof(double)));
+    OTM_TRY(alloc(&k16, nv * 2));
+    OTM_TRY(alloc(&u16, 3 * nv * 2));
+    OTM_TRY(alloc(&r16, 3 * nv * 2));
+    OTM_CUDA(cudaMemsetAsync(x64, 0, 3 * nv * sizeof(double), stream));
+    OTM_CUDA(cudaMemsetAsync(u16, 0, 3 * nv * 2, stream));
+  } else {
+    OTM_TRY(alloc((void**)&p, 3 * nv * sizeof(float)));
+    OTM_TRY(alloc((void**)&q, 3 * nv * sizeof(float)));
+    OTM_CUDA(cudaMemsetAsync(p, 0, 3 * nv * sizeof(float), stream));
+  }
   nc = int(lv.back().d.nv());
   OTM_TRY(alloc((void**)&Ainv, size_t(nc) * nc * sizeof(double)));
   OTM_TRY(alloc((void**)&table, 64 * 27 * sizeof(float)));
@@ -170,6 +189,25 @@ otm_status Homo::build(const otm_config& c) {
   galerkin_level1_table(tm, tab.data());
   OTM_CUDA(cudaMemcpyAsync(table, tab.data(), tab.size() * sizeof(float), cudaMemcpyHostToDevice, stream));
   OTM_CUDA(cudaStreamSynchronize(stream));
+  // small levels (<= 16^3 unknowns) and the coarsest solve run in one single-CTA kernel
+  {
+    const int L = int(lv.size());
+    int t = -1;
+    for (int l = 1; l < L; l++)
+      if (lv[l].d.nv() <= size_t(kTailMaxNv)) {
+        t = l;
+        break;
+      }
+    if (t > 0 && t < L - 1 && L - t <= kTailMaxLevels) {
+      size_t floats = 0;
+      for (int l = t; l < L; l++) floats += 9 * lv[l].d.nv();
+      if (floats * sizeof(float) <= 200 * 1024) {
+        tail_l = t;
+        tail_smem = floats * sizeof(float);
+        OTM_CUDA(cudaFuncSetAttribute(k_vcycle_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tail_smem)));
+      }
+    }
+  }
   stats.levels = int(lv.size());
   stats.coarsest_reso[0] = lv.back().d.nx;
   stats.coarsest_reso[1] = lv.back().d.ny;
@@ -205,11 +243,23 @@ otm_status Homo::update(const float* kin, int pitchT) {
   OTM_CHECK_LAUNCH("k_import");
   launched(1);
   const int L = int(lv.size());
+  const unsigned int* kmax_bits = (const unsigned int*)(flags + 2);
+  if (mixed) {
+    OTM_CUDA(cudaMemsetAsync(flags + 2, 0, sizeof(int), stream));
+    k_kmax<<<reduce_blocks(nv), kBlock, 0, stream>>>(nv, ks, (unsigned int*)(flags + 2));
+    if (cfg.precision == OTM_PRECISION_MIXED_BF16)
+      k_to16<__nv_bfloat16><<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(nv, ks, kmax_bits, (__nv_bfloat16*)k16);
+    else
+      k_to16<__half><<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(nv, ks, kmax_bits, (__half*)k16);
+    OTM_CHECK_LAUNCH("k_to16");
+    launched(2);
+  }
   for (int l = 1; l < L; l++) {
     const bool cb = (l < L - 1);  // smoothed levels use the colour-blocked stencil order
     const size_t nvc = lv[l].d.nv();
     if (l == 1)
-      k_galerkin_fine<<<ceil_div(nvc, kBlock), kBlock, 0, stream>>>(lv[0].d, lv[1].d, ks, table, lv[1].st, cb);
+      k_galerkin_fine<<<ceil_div(nvc, kBlock), kBlock, 0, stream>>>(lv[0].d, lv[1].d, ks, table, lv[1].st, cb,
+                                                                    mixed ? kmax_bits : nullptr, op.c0);
     else
       k_galerkin_coarse<<<ceil_div(nvc, kBlock), kBlock, 0, stream>>>(lv[l - 1].d, lv[l].d, lv[l - 1].st, lv[l].st,
                                                                       cb);
@@ -221,7 +271,14 @@ otm_status Homo::update(const float* kin, int pitchT) {
     OTM_CHECK_LAUNCH("k_fine_stencil");
     launched(1);
   }
-  k_coarsest_build<<<1, 1024, 0, stream>>>(lv.back().d, lv.back().st, Ainv, flags + 1);
+  {
+    const size_t abytes = size_t(nc) * nc * sizeof(double);
+    const int use_smem = abytes <= 200 * 1024;
+    if (use_smem)
+      OTM_CUDA(cudaFuncSetAttribute(k_coarsest_build, cudaFuncAttributeMaxDynamicSharedMemorySize, int(abytes)));
+    k_coarsest_build<<<1, 1024, use_smem ? abytes : 0, stream>>>(lv.back().d, lv.back().st, Ainv, flags + 1,
+                                                                  use_smem);
+  }
   OTM_CHECK_LAUNCH("k_coarsest_build");
   launched(1);
   updated = true;
@@ -232,9 +289,49 @@ otm_status Homo::update(const float* kin, int pitchT) {
 // ---------------------------------------------------------------------------------------
 // V-cycle and iteration (MG_H::v_cycle, homogenization/MG.cpp:46-71).
 // ---------------------------------------------------------------------------------------
+// Fine-level operations of the mixed form on 16-bit storage T: what = 0 colour pass,
+// 1 residual, 2 restriction to level 1, 3 prolongation from level 1.
+template <typename T>
+void Homo::fine_ops16(int what, int color) {
+  Level& L = lv[0];
+  const size_t nv = L.d.nv();
+  const T* kk = (const T*)k16;
+  T* u = (T*)u16;
+  T* r = (T*)r16;
+  const double* fs = sc->fscale;
+  switch (what) {
+    case 0:
+      if (face)
+        k_gs_fine<true, 3, T, T><<<ceil_div(nv >> 3, kBlock), kBlock, 0, stream>>>(L.d, color, kk, op0, u, L.f, sc, fs);
+      else
+        k_gs_fine<false, 3, T, T><<<ceil_div(nv >> 3, kBlock), kBlock, 0, stream>>>(L.d, color, kk, op0, u, L.f, sc, fs);
+      break;
+    case 1:
+      if (face)
+        k_resid_fine<true, 3, T, T><<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(L.d, kk, op0, u, L.f, r, sc, fs);
+      else
+        k_resid_fine<false, 3, T, T><<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(L.d, kk, op0, u, L.f, r, sc, fs);
+      break;
+    case 2:
+      k_restrict<3, T><<<ceil_div(lv[1].d.nv(), kBlock), kBlock, 0, stream>>>(L.d, lv[1].d, r, lv[1].f, sc);
+      break;
+    default:
+      k_prolong<3, T><<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(L.d, lv[1].d, lv[1].u, u, sc);
+      break;
+  }
+  launched(1);
+}
+
 void Homo::gs(int l, int color) {
   Level& L = lv[l];
   const size_t nsub = L.d.nv() >> 3;
+  if (l == 0 && mixed) {
+    if (cfg.precision == OTM_PRECISION_MIXED_BF16)
+      fine_ops16<__nv_bfloat16>(0, color);
+    else
+      fine_ops16<__half>(0, color);
+    return;
+  }
   if (l == 0) {
     if (face)
       k_gs_fine<true, 3><<<ceil_div(nsub, kBlock), kBlock, 0, stream>>>(L.d, color, ks, op, L.u, L.f, sc);
@@ -249,13 +346,38 @@ void Homo::gs(int l, int color) {
 void Homo::vcycle(int l) {
   Level& L = lv[l];
   const size_t nv = L.d.nv();
+  if (l == tail_l) {
+    TailDesc td{};
+    td.nlev = int(lv.size()) - l;
+    td.pre = cfg.pre_smooth;
+    td.post = cfg.post_smooth;
+    td.nc = nc;
+    int off = 0;
+    for (int i = 0; i < td.nlev; i++) {
+      td.lv[i].d = lv[l + i].d;
+      td.lv[i].st = lv[l + i].st;
+      td.lv[i].off = off;
+      off += int(9 * lv[l + i].d.nv());
+    }
+    td.f_in = L.f;
+    td.u_out = L.u;
+    td.Ainv = Ainv;
+    k_vcycle_tail<<<1, kTailThreads, tail_smem, stream>>>(td, sc);
+    launched(1);
+    return;
+  }
   if (l == int(lv.size()) - 1) {
     k_coarsest_solve<<<1, std::min(1024, std::max(32, (nc + 31) / 32 * 32)), 3 * nc * sizeof(double), stream>>>(
         nc, Ainv, L.f, L.u, sc);
     launched(1);
     return;
   }
-  cudaMemsetAsync(L.u, 0, 3 * nv * sizeof(float), stream);
+  const bool m16 = (l == 0 && mixed);
+  const bool bf = cfg.precision == OTM_PRECISION_MIXED_BF16;
+  if (m16)
+    cudaMemsetAsync(u16, 0, 3 * nv * 2, stream);
+  else
+    cudaMemsetAsync(L.u, 0, 3 * nv * sizeof(float), stream);
   for (int s = 0; s < cfg.pre_smooth; s++) {
     const bool timed = cfg.profile && l == 0 && s == 0 && prof_slot >= 0;
     // inside a stream capture only an "external" event record becomes a graph node
@@ -264,20 +386,37 @@ void Homo::vcycle(int l) {
     for (int c = 0; c < 8; c++) gs(l, c);
     if (timed) cudaEventRecordWithFlags(prof_ev[1][prof_slot], stream, evflag);
   }
-  if (l == 0) {
-    if (face)
-      k_resid_fine<true, 3><<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(L.d, ks, op, L.u, L.f, L.r, sc);
-    else
-      k_resid_fine<false, 3><<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(L.d, ks, op, L.u, L.f, L.r, sc);
-  } else {
-    k_resid_coarse<3><<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(L.d, L.st, L.u, L.f, L.r, sc);
-  }
   Level& C = lv[l + 1];
-  k_restrict<3><<<ceil_div(C.d.nv(), kBlock), kBlock, 0, stream>>>(L.d, C.d, L.r, C.f, sc);
-  launched(2);  // residual + restriction
+  if (m16) {
+    if (bf) {
+      fine_ops16<__nv_bfloat16>(1, 0);
+      fine_ops16<__nv_bfloat16>(2, 0);
+    } else {
+      fine_ops16<__half>(1, 0);
+      fine_ops16<__half>(2, 0);
+    }
+  } else {
+    if (l == 0) {
+      if (face)
+        k_resid_fine<true, 3><<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(L.d, ks, op, L.u, L.f, L.r, sc);
+      else
+        k_resid_fine<false, 3><<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(L.d, ks, op, L.u, L.f, L.r, sc);
+    } else {
+      k_resid_coarse<3><<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(L.d, L.st, L.u, L.f, L.r, sc);
+    }
+    k_restrict<3><<<ceil_div(C.d.nv(), kBlock), kBlock, 0, stream>>>(L.d, C.d, L.r, C.f, sc);
+    launched(2);  // residual + restriction
+  }
   vcycle(l + 1);
-  k_prolong<3><<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(L.d, C.d, C.u, L.u, sc);
-  launched(1);
+  if (m16) {
+    if (bf)
+      fine_ops16<__nv_bfloat16>(3, 0);
+    else
+      fine_ops16<__half>(3, 0);
+  } else {
+    k_prolong<3><<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(L.d, C.d, C.u, L.u, sc);
+    launched(1);
+  }
   for (int s = 0; s < cfg.post_smooth; s++)
     for (int c = 7; c >= 0; c--) gs(l, c);
 }
@@ -289,7 +428,20 @@ void Homo::iteration(int j) {
   const int nb = reduce_blocks(nv);
   float* r = lv[0].f;  // Krylov residual is the V-cycle's level-0 right-hand side
   float* z = lv[0].u;  // and the V-cycle's level-0 result is the preconditioned residual
-  if (cfg.solver == OTM_SOLVER_PCG) {
+  if (mixed) {
+    // FP64 refinement step: residual, one 16-bit V-cycle on the scaled residual, update
+    const unsigned int* kmax_bits = (const unsigned int*)(flags + 2);
+    if (face)
+      k_resid64<true><<<nb, kBlock, 0, stream>>>(d0, ks, op, x64, b, r, partials, sc, kmax_bits, cfg.max_iter, 0);
+    else
+      k_resid64<false><<<nb, kBlock, 0, stream>>>(d0, ks, op, x64, b, r, partials, sc, kmax_bits, cfg.max_iter, 0);
+    vcycle(0);
+    if (cfg.precision == OTM_PRECISION_MIXED_BF16)
+      k_update64<__nv_bfloat16><<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(nv, x64, (const __nv_bfloat16*)u16, sc);
+    else
+      k_update64<__half><<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(nv, x64, (const __half*)u16, sc);
+    launched(2);
+  } else if (cfg.solver == OTM_SOLVER_PCG) {
     vcycle(0);
     k_dot_rz<<<nb, kBlock, 0, stream>>>(nv, r, z, partials, sc);
     k_update_p<<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(nv, z, p, sc);
@@ -367,17 +519,29 @@ otm_status Homo::solve_impl() {
     return OTM_ERR_NAN;
   }
   for (int attempt = 0; attempt < 2; attempt++) {
-    if (!cfg.warm_start || attempt > 0) OTM_CUDA(cudaMemsetAsync(x, 0, 3 * nv * sizeof(float), stream));
+    if (!cfg.warm_start || attempt > 0) {
+      OTM_CUDA(cudaMemsetAsync(x, 0, 3 * nv * sizeof(float), stream));
+      if (mixed) OTM_CUDA(cudaMemsetAsync(x64, 0, 3 * nv * sizeof(double), stream));
+    }
     k_rhs<<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(d0, ks, ef, b);
     // project RHS and initial guess off the constants
     k_sums2<<<nb, kBlock, 0, stream>>>(nv, b, x, partials, means, &sc->counter[T_MEAN]);
     k_sub_means<<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(nv, b, x, means);
     sc_host->tol = cfg.fem_rel_thres;
     OTM_CUDA(cudaMemcpyAsync(&sc->tol, &sc_host->tol, sizeof(double), cudaMemcpyHostToDevice, stream));
-    if (face)
+    if (mixed) {
+      const unsigned int* kmax_bits = (const unsigned int*)(flags + 2);
+      if (face)
+        k_resid64<true><<<nb, kBlock, 0, stream>>>(d0, ks, op, x64, b, lv[0].f, partials, sc, kmax_bits,
+                                                   cfg.max_iter, 1);
+      else
+        k_resid64<false><<<nb, kBlock, 0, stream>>>(d0, ks, op, x64, b, lv[0].f, partials, sc, kmax_bits,
+                                                    cfg.max_iter, 1);
+    } else if (face) {
       k_init_residual<true><<<nb, kBlock, 0, stream>>>(d0, ks, op, x, b, lv[0].f, partials, sc);
-    else
+    } else {
       k_init_residual<false><<<nb, kBlock, 0, stream>>>(d0, ks, op, x, b, lv[0].f, partials, sc);
+    }
     OTM_CHECK_LAUNCH("solve init");
     launched(4);
     int nlaunched = 0, iter_before = 0;
@@ -405,6 +569,7 @@ otm_status Homo::solve_impl() {
       nlaunched += chunk;
     }
     stats.iterations = sc_host->iter;
+    stats.refinements = mixed ? sc_host->iter : 0;
     for (int c = 0; c < 3; c++) stats.rel_res[c] = sc_host->relres[c];
     if (!sc_host->nan) break;
     // "numerical explode, resetting initial guess" (homogenization/MG.cpp:392-423): one
@@ -421,6 +586,11 @@ otm_status Homo::solve_impl() {
   }
   stats.status = st;
   solved = (st == OTM_OK || st == OTM_ERR_NOT_CONVERGED);
+  if (mixed) {
+    // FP32 copy of the FP64 solution for K^H, sensitivity and the solution accessors
+    k_x64_to_x<<<ceil_div(3 * nv, kBlock), kBlock, 0, stream>>>(3 * nv, x64, x);
+    launched(1);
+  }
   return st;
 }
 
@@ -639,6 +809,11 @@ otm_status otm_homo_set_solution(otm_homo* h, int lcase, const float* src_dev) {
   const size_t nv = H.lv[0].d.nv();
   OTM_TRY(H.enter());
   OTM_CUDA(cudaMemcpyAsync(H.x + lcase * nv, src_dev, nv * sizeof(float), cudaMemcpyDeviceToDevice, H.stream));
+  if (H.mixed) {
+    otm::k_x_to_x64<<<otm::ceil_div(nv, otm::kBlock), otm::kBlock, 0, H.stream>>>(nv, H.x + lcase * nv,
+                                                                                 H.x64 + lcase * nv);
+    H.launched(1);
+  }
   return H.leave();
 }
 
@@ -647,6 +822,7 @@ otm_status otm_homo_reset_displacement(otm_homo* h) {
   Homo& H = h->impl;
   OTM_TRY(H.enter());
   OTM_CUDA(cudaMemsetAsync(H.x, 0, 3 * H.lv[0].d.nv() * sizeof(float), H.stream));
+  if (H.mixed) OTM_CUDA(cudaMemsetAsync(H.x64, 0, 3 * H.lv[0].d.nv() * sizeof(double), H.stream));
   H.solved = false;
   return H.leave();
 }

@@ -7,6 +7,7 @@
 
 #include "otm_mg_kernels.cuh"
 #include "otm_solver_kernels.cuh"
+#include "otm_tail.cuh"
 #include "otm_template.h"
 
 namespace otm {
@@ -40,6 +41,13 @@ struct Homo {
   FineOp op{};
   ElemFields ef{};
   bool face = false;
+  // mixed precision: FP64 solution, 16-bit fine-level storage, normalised inner operator
+  bool mixed = false;
+  double* x64 = nullptr;
+  void* k16 = nullptr;
+  void* u16 = nullptr;
+  void* r16 = nullptr;
+  FineOp op0{};  // op / c0
   float* ks = nullptr;    // solver conductivity 1e-9 + k^p
   float* kraw = nullptr;  // conductivity as imported
   float* b = nullptr;     // right-hand sides
@@ -47,6 +55,8 @@ struct Homo {
   float* p = nullptr;
   float* q = nullptr;
   double* Ainv = nullptr;
+  int tail_l = -1;          // first level handled by the single-CTA tail kernel (-1: none)
+  size_t tail_smem = 0;     // its dynamic shared memory
   int nc = 0;
   float* table = nullptr;
   SolveScalars* sc = nullptr;
@@ -74,6 +84,8 @@ struct Homo {
   otm_status leave();
   otm_status update(const float* kin, int pitchT);
   void gs(int l, int color);
+  template <typename T>
+  void fine_ops16(int what, int color);
   void vcycle(int l);
   void iteration(int j);
   void launched(uint64_t n) {

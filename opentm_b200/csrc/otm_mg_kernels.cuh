@@ -10,6 +10,9 @@
 // Stencil offset o = (ox+1) + 3(oy+1) + 9(oz+1).
 #pragma once
 
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
 #include "otm_common.cuh"
 
 namespace otm {
@@ -38,6 +41,9 @@ struct SolveScalars {
   int nan;           // 1 if a NaN/Inf appeared
   int first;         // 1 before the first beta
   unsigned int counter[8];  // last-block tickets
+  // mixed precision: f is read as alpha_c * f by the inner cycle, x64 += xscale_c * u
+  double fscale[3];
+  double xscale[3];
 };
 
 enum Ticket { T_RZ = 0, T_PQ = 1, T_RR = 2, T_KH = 3, T_MEAN = 4, T_INIT = 5, T_RES = 6 };
@@ -104,6 +110,14 @@ __device__ __forceinline__ float fine_coef(const float (&k8)[8], const FineOp& o
   return c * ksum<ox, oy, oz>(k8);
 }
 
+// Storage conversions of the fine-level fields (FP32, BF16 or FP16 storage, FP32 arithmetic).
+__device__ __forceinline__ float ld(const float* p) { return *p; }
+__device__ __forceinline__ float ld(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+__device__ __forceinline__ float ld(const __half* p) { return __half2float(*p); }
+__device__ __forceinline__ void st(float* p, float v) { *p = v; }
+__device__ __forceinline__ void st(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
+__device__ __forceinline__ void st(__half* p, float v) { *p = __float2half_rn(v); }
+
 // Neighbour indices of (x,y,z) on a periodic grid: idx[o] for the 27 offsets.
 struct Nbr {
   int xs[3];
@@ -123,12 +137,13 @@ struct Nbr {
 };
 
 // The 8 element conductivities around vertex (x,y,z): element lower corners x-1..x etc.
-__device__ __forceinline__ void load_k8(const float* __restrict__ ks, const Nbr& nb, float (&k8)[8]) {
+template <typename KT>
+__device__ __forceinline__ void load_k8(const KT* __restrict__ ks, const Nbr& nb, float (&k8)[8]) {
 #pragma unroll
   for (int b = 0; b < 8; b++) {
     const int bx = b & 1, by = (b >> 1) & 1, bz = b >> 2;
     // element lower corner (x-1+bx, y-1+by, z-1+bz) = neighbour offset (bx-1, by-1, bz-1)
-    k8[b] = __ldg(ks + nb.rows[by + 3 * bz] + nb.xs[bx]);
+    k8[b] = ld(ks + nb.rows[by + 3 * bz] + nb.xs[bx]);
   }
 }
 
@@ -140,9 +155,9 @@ struct FineTerm {
 };
 
 // acc[c] -= sum_{o != 0} A(v, v+o) u_c[v+o] over the 3 cases; returns the diagonal.
-template <bool kFace, int NC>
+template <bool kFace, int NC, typename VT>
 __device__ __forceinline__ float fine_offdiag(const float (&k8)[8], const FineOp& op, const Nbr& nb,
-                                              const float* u, size_t nv, float (&acc)[NC]) {
+                                              const VT* u, size_t nv, float (&acc)[NC]) {
 #pragma unroll
   for (int o = 0; o < 27; o++) {
     if (o == 13) continue;
@@ -162,7 +177,7 @@ __device__ __forceinline__ float fine_offdiag(const float (&k8)[8], const FineOp
     }
     const size_t j = nb.at(o);
 #pragma unroll
-    for (int c = 0; c < NC; c++) acc[c] -= coef * u[c * nv + j];
+    for (int c = 0; c < NC; c++) acc[c] -= coef * ld(u + c * nv + j);
   }
   float ksum8 = 0.f;
 #pragma unroll
@@ -173,9 +188,12 @@ __device__ __forceinline__ float fine_offdiag(const float (&k8)[8], const FineOp
 // One Gauss-Seidel colour pass on the fine level, omega = 1, all NC load cases
 // (homogenization/grid.cu:318-471 without the periodic padding; the pinned Dirichlet vertex
 // is replaced by mean projection in the outer solver).
-template <bool kFace, int NC>
-__global__ void __launch_bounds__(kBlock) k_gs_fine(Dims d, int color, const float* __restrict__ ks, FineOp op,
-                                                     float* u, const float* __restrict__ f, const SolveScalars* sc) {
+// fscale (optional): per-case factor applied to f when it is read (scaled right-hand side of
+// the mixed-precision inner cycle).
+template <bool kFace, int NC, typename KT = float, typename VT = float>
+__global__ void __launch_bounds__(kBlock) k_gs_fine(Dims d, int color, const KT* __restrict__ ks, FineOp op,
+                                                     VT* u, const float* __restrict__ f, const SolveScalars* sc,
+                                                     const double* fscale = nullptr) {
   if (sc && solve_done(sc)) return;
   const int hx = d.nx >> 1, hy = d.ny >> 1;
   const size_t nsub = d.nv() >> 3;
@@ -191,18 +209,19 @@ __global__ void __launch_bounds__(kBlock) k_gs_fine(Dims d, int color, const flo
   const size_t v = nb.at(13);
   float acc[NC];
 #pragma unroll
-  for (int c = 0; c < NC; c++) acc[c] = __ldg(f + c * nv + v);
+  for (int c = 0; c < NC; c++) acc[c] = __ldg(f + c * nv + v) * (fscale ? float(fscale[c]) : 1.f);
   const float diag = fine_offdiag<kFace, NC>(k8, op, nb, u, nv, acc);
   const float inv = 1.0f / diag;
 #pragma unroll
-  for (int c = 0; c < NC; c++) u[c * nv + v] = acc[c] * inv;
+  for (int c = 0; c < NC; c++) st(u + c * nv + v, acc[c] * inv);
 }
 
 // r = f - A u on the fine level for every vertex.
-template <bool kFace, int NC>
-__global__ void __launch_bounds__(kBlock) k_resid_fine(Dims d, const float* __restrict__ ks, FineOp op,
-                                                        const float* __restrict__ u, const float* __restrict__ f,
-                                                        float* __restrict__ r, const SolveScalars* sc) {
+template <bool kFace, int NC, typename KT = float, typename VT = float>
+__global__ void __launch_bounds__(kBlock) k_resid_fine(Dims d, const KT* __restrict__ ks, FineOp op,
+                                                        const VT* __restrict__ u, const float* __restrict__ f,
+                                                        VT* __restrict__ r, const SolveScalars* sc,
+                                                        const double* fscale = nullptr) {
   if (sc && solve_done(sc)) return;
   const size_t nv = d.nv();
   const size_t v = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -214,10 +233,10 @@ __global__ void __launch_bounds__(kBlock) k_resid_fine(Dims d, const float* __re
   load_k8(ks, nb, k8);
   float acc[NC];
 #pragma unroll
-  for (int c = 0; c < NC; c++) acc[c] = __ldg(f + c * nv + v);
+  for (int c = 0; c < NC; c++) acc[c] = __ldg(f + c * nv + v) * (fscale ? float(fscale[c]) : 1.f);
   const float diag = fine_offdiag<kFace, NC>(k8, op, nb, u, nv, acc);
 #pragma unroll
-  for (int c = 0; c < NC; c++) r[c * nv + v] = acc[c] - diag * __ldg(u + c * nv + v);
+  for (int c = 0; c < NC; c++) st(r + c * nv + v, acc[c] - diag * ld(u + c * nv + v));
 }
 
 // ------------------------------------------------------------------------------------
@@ -288,8 +307,8 @@ __global__ void __launch_bounds__(kBlock) k_resid_coarse(Dims d, const float* __
 
 // f_c(V) = sum_d w(d) r_f(2V + d), w = prod (1 - |d|/2): full weighting = P^T
 // (homogenization/grid.cu:811-878).
-template <int NC>
-__global__ void __launch_bounds__(kBlock) k_restrict(Dims df, Dims dc, const float* __restrict__ r,
+template <int NC, typename VT = float>
+__global__ void __launch_bounds__(kBlock) k_restrict(Dims df, Dims dc, const VT* __restrict__ r,
                                                       float* __restrict__ fc, const SolveScalars* sc) {
   if (sc && solve_done(sc)) return;
   const size_t nvc = dc.nv(), nvf = df.nv();
@@ -307,15 +326,15 @@ __global__ void __launch_bounds__(kBlock) k_restrict(Dims df, Dims dc, const flo
     const float w = (ox ? 0.5f : 1.f) * (oy ? 0.5f : 1.f) * (oz ? 0.5f : 1.f);
     const size_t j = nb.at(o);
 #pragma unroll
-    for (int c = 0; c < NC; c++) acc[c] += w * __ldg(r + c * nvf + j);
+    for (int c = 0; c < NC; c++) acc[c] += w * ld(r + c * nvf + j);
   }
 #pragma unroll
   for (int c = 0; c < NC; c++) fc[c * nvc + V] = acc[c];
 }
 
 // u_f += P u_c, trilinear interpolation (homogenization/grid.cu:881-940).
-template <int NC>
-__global__ void __launch_bounds__(kBlock) k_prolong(Dims df, Dims dc, const float* __restrict__ uc, float* uf,
+template <int NC, typename VT = float>
+__global__ void __launch_bounds__(kBlock) k_prolong(Dims df, Dims dc, const float* __restrict__ uc, VT* uf,
                                                      const SolveScalars* sc) {
   if (sc && solve_done(sc)) return;
   const size_t nvc = dc.nv(), nvf = df.nv();
@@ -337,7 +356,7 @@ __global__ void __launch_bounds__(kBlock) k_prolong(Dims df, Dims dc, const floa
                            wy1 * (wx0 * __ldg(u + r10 + X0) + wx1 * __ldg(u + r10 + X1))) +
                     wz1 * (wy0 * (wx0 * __ldg(u + r01 + X0) + wx1 * __ldg(u + r01 + X1)) +
                            wy1 * (wx0 * __ldg(u + r11 + X0) + wx1 * __ldg(u + r11 + X1)));
-    uf[c * nvf + v] += a;
+    st(uf + c * nvf + v, ld(uf + c * nvf + v) + a);
   }
 }
 
@@ -349,9 +368,12 @@ __global__ void __launch_bounds__(kBlock) k_prolong(Dims df, Dims dc, const floa
 // 2V of k_e T[e][O], where T[e][O] = sum_ij P(p_i, V) KE_ij P(p_j, V+O) depends only on the
 // element's position relative to 2V (tabulated on the host, 64 x 27, scaled by the element
 // size). Element e = (ex,ey,ez) in 0..3 has its lower corner at 2V - 2 + (ex,ey,ez).
+// kmax_bits (optional): divide the stencil by c0 * kmax, the normalisation of the
+// mixed-precision inner operator (c0 is passed in c0).
 static __global__ void __launch_bounds__(kBlock) k_galerkin_fine(Dims df, Dims dc, const float* __restrict__ ks,
                                                            const float* __restrict__ table, float* __restrict__ st,
-                                                           int cb_out) {
+                                                           int cb_out, const unsigned int* kmax_bits = nullptr,
+                                                           float c0 = 1.f) {
   __shared__ float T[64 * 27];
   for (int i = threadIdx.x; i < 64 * 27; i += blockDim.x) T[i] = table[i];
   __syncthreads();
@@ -383,8 +405,9 @@ static __global__ void __launch_bounds__(kBlock) k_galerkin_fine(Dims df, Dims d
       }
     }
   const size_t out = cb_out ? cb_index(dc, X, Y, Z) : V;
+  const float sc = kmax_bits ? 1.f / (c0 * __uint_as_float(*kmax_bits)) : 1.f;
 #pragma unroll
-  for (int o = 0; o < 27; o++) st[size_t(o) * nvc + out] = acc[o];
+  for (int o = 0; o < 27; o++) st[size_t(o) * nvc + out] = acc[o] * sc;
 }
 
 // Per-axis coarse targets of a fine offset t = d + o in [-2, 2]: the coarse offsets O with

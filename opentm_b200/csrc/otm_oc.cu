@@ -63,6 +63,74 @@ __global__ void __launch_bounds__(kBlock) k_oc_maxabs(int ne, const float* __res
   }
 }
 
+// Five bisection steps per pass: the volumes of all 31 multipliers the bisection can visit
+// in its next 5 steps (the nodes of the bisection tree below [gmin, gmax], midpoints in FP32
+// as the reference computes them) are summed in one read of sens and rho; the last block
+// then walks the tree exactly as the sequential loop would (OCOptimizer.cu:69-88).
+constexpr int kTreeDepth = 5;
+constexpr int kTreeNodes = (1 << kTreeDepth) - 1;
+
+__device__ __forceinline__ void oc_tree(float gmin, float gmax, float (&g)[kTreeNodes]) {
+  float lo[kTreeNodes], hi[kTreeNodes];
+  lo[0] = gmin;
+  hi[0] = gmax;
+#pragma unroll
+  for (int i = 0; i < kTreeNodes; i++) {
+    g[i] = (hi[i] + lo[i]) / 2;
+    if (2 * i + 2 < kTreeNodes) {
+      lo[2 * i + 1] = lo[i];  // volume too small: gmax = g
+      hi[2 * i + 1] = g[i];
+      lo[2 * i + 2] = g[i];   // volume too large: gmin = g
+      hi[2 * i + 2] = hi[i];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_oc_tree_pass(int ne, const float* __restrict__ sens,
+                                                         const float* __restrict__ rho, float volratio, float min_rho,
+                                                         float step, float damp, double* partials, OcState* st) {
+  if (*((volatile int*)&st->done)) return;
+  __shared__ double smem[32 * kTreeNodes];
+  float g[kTreeNodes];
+  oc_tree(float(st->gmin), float(st->gmax), g);
+  double v[kTreeNodes];
+#pragma unroll
+  for (int t = 0; t < kTreeNodes; t++) v[t] = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ne; i += gridDim.x * blockDim.x) {
+    const float s = __ldg(sens + i), r = __ldg(rho + i);
+#pragma unroll
+    for (int t = 0; t < kTreeNodes; t++) v[t] += oc_new_rho(s, r, g[t], min_rho, step, damp);
+  }
+  block_reduce_f64<kTreeNodes>(v, smem);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int t = 0; t < kTreeNodes; t++) partials[blockIdx.x * kTreeNodes + t] = v[t];
+  if (last_block(&st->counter)) {
+    double tot[kTreeNodes];
+    reduce_partials<kTreeNodes>(partials, gridDim.x, tot, smem);
+    if (threadIdx.x == 0) {
+      int node = 0;
+      for (int depth = 0; depth < kTreeDepth && !st->done; depth++) {
+        const double vol = tot[node] / ne;
+        st->vol = vol;
+        st->g = double(g[node]);
+        st->iters += 1;
+        if (vol < volratio - 0.0001) {
+          st->gmax = double(g[node]);
+          node = 2 * node + 1;
+        } else if (vol > volratio + 0.0001) {
+          st->gmin = double(g[node]);
+          node = 2 * node + 2;
+        } else {
+          st->done = 1;
+        }
+        if (st->iters >= kOcSteps) st->done = 1;
+      }
+      st->counter = 0;
+    }
+  }
+}
+
 // One bisection step: volume of the candidate density at g = (gmax + gmin) / 2.
 __global__ void __launch_bounds__(kBlock) k_oc_pass(int ne, const float* __restrict__ sens,
                                                     const float* __restrict__ rho, float volratio, float min_rho,
@@ -185,14 +253,14 @@ otm_status otm_oc_update(int ne, const float* sens, float* rho, float volratio, 
   cudaStream_t s = (cudaStream_t)stream;
   const int nb = std::min(kMaxPartials, std::max(1, (ne + kBlock - 1) / kBlock));
   char* scratch = nullptr;
-  const size_t bytes = sizeof(OcState) + size_t(nb) * sizeof(double);
+  const size_t bytes = sizeof(OcState) + size_t(nb) * kTreeNodes * sizeof(double);
   OTM_CUDA(cudaMallocAsync((void**)&scratch, bytes, s));
   OcState* st = (OcState*)scratch;
   double* partials = (double*)(scratch + sizeof(OcState));
   cudaMemsetAsync(st, 0, sizeof(OcState), s);
   k_oc_maxabs<<<nb, kBlock, 0, s>>>(ne, sens, partials, st);
-  for (int i = 0; i < kOcSteps; i++)
-    k_oc_pass<<<nb, kBlock, 0, s>>>(ne, sens, rho, volratio, min_rho, step_limit, damp, partials, st);
+  for (int i = 0; i < (kOcSteps + kTreeDepth - 1) / kTreeDepth; i++)
+    k_oc_tree_pass<<<nb, kBlock, 0, s>>>(ne, sens, rho, volratio, min_rho, step_limit, damp, partials, st);
   k_oc_apply<<<ceil_div(size_t(ne), kBlock), kBlock, 0, s>>>(ne, sens, rho, min_rho, step_limit, damp, st);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess && iters_out) {
@@ -203,7 +271,7 @@ otm_status otm_oc_update(int ne, const float* sens, float* rho, float volratio, 
   }
   cudaFreeAsync(scratch, s);
   if (e != cudaSuccess) return cuda_fail(e, "otm_oc_update");
-  count_launches(2 + kOcSteps);
+  count_launches(2 + (kOcSteps + kTreeDepth - 1) / kTreeDepth);
   return OTM_OK;
 }
 

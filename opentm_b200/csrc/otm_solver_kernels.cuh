@@ -21,6 +21,24 @@ __host__ __device__ inline int reduce_blocks(size_t n) {
   return int(b);
 }
 
+// Largest solver conductivity (positive floats order like their bit patterns).
+static __global__ void k_kmax(size_t nv, const float* __restrict__ ks, unsigned int* kmax_bits) {
+  unsigned int m = 0;
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nv; i += size_t(gridDim.x) * blockDim.x)
+    m = max(m, __float_as_uint(fmaxf(ks[i], 0.f)));
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) m = max(m, __shfl_down_sync(0xffffffffu, m, off));
+  if ((threadIdx.x & 31) == 0) atomicMax(kmax_bits, m);
+}
+
+// 16-bit copy of the normalised conductivity k / kmax for the mixed-precision inner cycle.
+template <typename T>
+__global__ void k_to16(size_t nv, const float* __restrict__ ks, const unsigned int* kmax_bits, T* k16) {
+  const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= nv) return;
+  st(k16 + i, ks[i] / __uint_as_float(*kmax_bits));
+}
+
 // k_solver = 1e-9 + k^p from a pitched lexicographic field, k_raw keeps the input
 // (Grid_H::update + update_rho_kernel, homogenization/grid.cu:2465-2504, 2646-2662; the
 // floor is applied where the reference evaluates rho_penal, grid.cu:405).
@@ -368,14 +386,158 @@ static __global__ void __launch_bounds__(kBlock) k_fine_stencil(Dims d, const fl
 #undef OTM_ST
 }
 
+
+// ---------------------------------------------------------------------------------------
+// Mixed precision: FP64 iterative refinement around a 16-bit-storage V-cycle.
+// ---------------------------------------------------------------------------------------
+
+// r = b - A x64 with FP64 accumulation from the FP32 conductivity, written as FP32 into f;
+// reduces ||r||^2 and max|r| per case (and ||b||^2 when init != 0), then sets the relative
+// residual, the done flag and the scales of the next inner cycle:
+// fscale = 1 / max|r|, xscale = max|r| / (c0 kmax).
+template <bool kFace>
+__global__ void __launch_bounds__(kBlock) k_resid64(Dims d, const float* __restrict__ ks, FineOp op,
+                                                    const double* __restrict__ x64, const float* __restrict__ b,
+                                                    float* __restrict__ f, double* partials, SolveScalars* sc,
+                                                    const unsigned int* kmax_bits, int max_iter, int init) {
+  if (!init && solve_done(sc)) return;
+  __shared__ double smem[32 * 6];
+  const size_t nv = d.nv();
+  double v[6] = {0, 0, 0, 0, 0, 0};
+  double mx[3] = {0, 0, 0};
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nv; i += size_t(gridDim.x) * blockDim.x) {
+    const int xx = int(i % d.nx), yy = int((i / d.nx) % d.ny), zz = int(i / (size_t(d.nx) * d.ny));
+    Nbr nb;
+    nb.init(d, xx, yy, zz);
+    float k8[8];
+    load_k8(ks, nb, k8);
+    double acc[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) acc[c] = double(b[c * nv + i]);
+#pragma unroll
+    for (int o = 0; o < 27; o++) {
+      if (o == 13) continue;
+      const int nzc = (o % 3 != 1) + ((o / 3) % 3 != 1) + (o / 9 != 1);
+      if (!kFace && nzc == 1) continue;
+      float coef;
+      switch (o) {
+#define OTM_FC(OO) \
+  case OO:         \
+    coef = fine_coef<OO>(k8, op); \
+    break;
+        OTM_FC(0) OTM_FC(1) OTM_FC(2) OTM_FC(3) OTM_FC(4) OTM_FC(5) OTM_FC(6) OTM_FC(7) OTM_FC(8)
+        OTM_FC(9) OTM_FC(10) OTM_FC(11) OTM_FC(12) OTM_FC(14) OTM_FC(15) OTM_FC(16) OTM_FC(17)
+        OTM_FC(18) OTM_FC(19) OTM_FC(20) OTM_FC(21) OTM_FC(22) OTM_FC(23) OTM_FC(24) OTM_FC(25) OTM_FC(26)
+#undef OTM_FC
+        default: coef = 0.f;
+      }
+      const size_t j = nb.at(o);
+#pragma unroll
+      for (int c = 0; c < 3; c++) acc[c] -= double(coef) * x64[c * nv + j];
+    }
+    float ksum8 = 0.f;
+#pragma unroll
+    for (int q = 0; q < 8; q++) ksum8 += k8[q];
+    const double diag = double(op.c0 * ksum8);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const double rc = acc[c] - diag * x64[c * nv + i];
+      f[c * nv + i] = float(rc);
+      v[3 + c] += rc * rc;
+      mx[c] = fmax(mx[c], fabs(rc));
+      if (init) {
+        const double bc = b[c * nv + i];
+        v[c] += bc * bc;
+      }
+    }
+  }
+  block_reduce_f64<6>(v, smem);
+  // block max of the 3 max-norms (warp shuffles, then shared memory)
+  __shared__ double smx[32 * 3];
+#pragma unroll
+  for (int c = 0; c < 3; c++)
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) mx[c] = fmax(mx[c], __shfl_down_sync(0xffffffffu, mx[c], off));
+  if ((threadIdx.x & 31) == 0)
+#pragma unroll
+    for (int c = 0; c < 3; c++) smx[(threadIdx.x >> 5) * 3 + c] = mx[c];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < int(blockDim.x + 31) / 32; w++)
+      for (int c = 0; c < 3; c++) mx[c] = fmax(mx[c], smx[w * 3 + c]);
+#pragma unroll
+    for (int i = 0; i < 6; i++) partials[blockIdx.x * 9 + i] = v[i];
+#pragma unroll
+    for (int c = 0; c < 3; c++) partials[blockIdx.x * 9 + 6 + c] = mx[c];
+  }
+  if (last_block(&sc->counter[T_RES])) {
+    if (threadIdx.x == 0) {
+      double t[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      for (int bq = 0; bq < int(gridDim.x); bq++)
+        for (int i = 0; i < 9; i++) {
+          const double val = ((volatile double*)partials)[bq * 9 + i];
+          t[i] = i < 6 ? t[i] + val : fmax(t[i], val);
+        }
+      const double kmax = double(__uint_as_float(*kmax_bits));
+      bool all = true, bad = false;
+      if (init) {
+        sc->iter = 0;
+        sc->nan = 0;
+      }
+      for (int c = 0; c < 3; c++) {
+        if (init) sc->bb[c] = t[c];
+        sc->rr[c] = t[3 + c];
+        const double rel = sqrt(t[3 + c]) / (sqrt(sc->bb[c]) + 1e-10);
+        sc->relres[c] = rel;
+        if (!(rel <= sc->tol)) all = false;
+        if (!isfinite(rel) || rel > 1e10) bad = true;
+        const double rmax = t[6 + c] > 0.0 ? t[6 + c] : 1.0;
+        sc->fscale[c] = 1.0 / rmax;
+        sc->xscale[c] = rmax / (double(op.c0) * kmax);
+      }
+      if (bad) sc->nan = 1;
+      sc->done = (all || bad || sc->iter >= max_iter) ? 1 : 0;
+      sc->counter[T_RES] = 0;
+    }
+  }
+}
+
+// x64 += xscale_c * u (the inner cycle's correction, 16-bit storage); counts the step.
+template <typename VT>
+__global__ void __launch_bounds__(kBlock) k_update64(size_t nv, double* x64, const VT* __restrict__ u,
+                                                     SolveScalars* sc) {
+  if (solve_done(sc)) return;
+  const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < nv) {
+#pragma unroll
+    for (int c = 0; c < 3; c++) x64[c * nv + i] += sc->xscale[c] * double(ld(u + c * nv + i));
+  }
+  if (i == 0) sc->iter += 1;
+}
+
+static __global__ void k_x64_to_x(size_t n, const double* __restrict__ x64, float* x) {
+  const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n) x[i] = float(x64[i]);
+}
+
+static __global__ void k_x_to_x64(size_t n, const float* __restrict__ x, double* x64) {
+  const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n) x64[i] = double(x[i]);
+}
+
 // ---------------------------------------------------------------------------------------
 // Coarsest level: dense FP64 inverse of A_c + (alpha/n) 1 1^T (SPD on the periodic
 // nullspace), built once per update; each V-cycle applies it as a mat-vec. Replaces the
 // host BiCGSTAB(ILUT) + nullspace projection of Grid_H::solveHostEquation
 // (homogenization/grid.cpp:272-310).
 // ---------------------------------------------------------------------------------------
-static __global__ void k_coarsest_build(Dims d, const float* __restrict__ st, double* A, int* status) {
+// With use_smem the matrix is assembled and inverted in dynamic shared memory (n^2 doubles)
+// and copied to Aout at the end; otherwise it is worked on in place in Aout.
+static __global__ void k_coarsest_build(Dims d, const float* __restrict__ st, double* Aout, int* status,
+                                        int use_smem) {
+  extern __shared__ double smA[];
   const int n = int(d.nv());
+  double* A = use_smem ? smA : Aout;
   for (size_t i = threadIdx.x; i < size_t(n) * n; i += blockDim.x) A[i] = 0.0;
   __syncthreads();
   __shared__ double dsum;
@@ -425,6 +587,8 @@ static __global__ void k_coarsest_build(Dims d, const float* __restrict__ st, do
     if (threadIdx.x == 0) A[size_t(k) * n + k] = pinv;
     __syncthreads();
   }
+  if (use_smem)
+    for (size_t i = threadIdx.x; i < size_t(n) * n; i += blockDim.x) Aout[i] = A[i];
 }
 
 // u = Ainv (f - mean f) for the 3 cases (one block).

@@ -1,0 +1,103 @@
+// Drop-in check of the C++ wrapper: the reference's call sequence (Homogenization_H::update,
+// heatMatrix, Sensitivity; OCOptimizer::filterSens/update; MMAOptimizer::update; mmasubDevice)
+// compiled unchanged against include/otm/homogenization.hpp. Prints K^H and checksums; the
+// pytest driver compares them with the Python path.
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "otm/homogenization.hpp"
+
+static float u01(unsigned long long i) {
+  unsigned long long z = i + 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  return float((z >> 11) * (1.0 / 9007199254740992.0));
+}
+
+int main() {
+  const int n = 16, ne = n * n * n, pitchT = 32;
+  cfg::HomoConfig config;
+  config.init();
+  config.reso[0] = config.reso[1] = config.reso[2] = n;
+  config.femRelThres = 1e-6;
+  homo::SolverOptions opt;
+  opt.pre_smooth = opt.post_smooth = 2;
+  homo::Homogenization_H hom(config, opt);
+
+  std::vector<float> h(size_t(n) * n * pitchT, 0.f);
+  for (int e = 0; e < ne; e++) {
+    const float rho = 0.001f + 0.999f * u01(e);
+    h[size_t(e / n) * pitchT + e % n] = 1e-3f + rho * rho * rho * (1.f - 1e-3f);
+  }
+  float *rho_d = nullptr, *sens_d = nullptr;
+  cudaMalloc(&rho_d, h.size() * sizeof(float));
+  cudaMalloc(&sens_d, h.size() * sizeof(float));
+  cudaMemcpy(rho_d, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice);
+
+  hom.update(rho_d, pitchT);
+  double C[3][3];
+  hom.heatMatrix(C);
+  float dC[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+  hom.Sensitivity(dC, sens_d, pitchT, true);
+  std::vector<float> s(h.size());
+  cudaMemcpy(s.data(), sens_d, s.size() * sizeof(float), cudaMemcpyDeviceToHost);
+  double ssum = 0;
+  for (float v : s) ssum += v;
+  std::printf("C %.9e %.9e %.9e %.9e %.9e %.9e\n", C[0][0], C[0][1], C[0][2], C[1][1], C[1][2], C[2][2]);
+  std::printf("sens_sum %.9e\n", ssum);
+
+  // MG_H view: re-solve from zero with a tighter tolerance
+  homo::MG_H mg(hom);
+  double rr = mg.solveEquation(1e-7, false);
+  std::printf("relres %.3e\n", rr);
+
+  // OC on the unpitched sensitivity of -trace(K^H)
+  float *srho = nullptr, *ss = nullptr;
+  cudaMalloc(&srho, ne * sizeof(float));
+  cudaMalloc(&ss, ne * sizeof(float));
+  std::vector<float> r0(ne, 0.3f), g(ne);
+  for (int e = 0; e < ne; e++) g[e] = -(0.1f + u01(ne + e));
+  cudaMemcpy(srho, r0.data(), ne * sizeof(float), cudaMemcpyHostToDevice);
+  cudaMemcpy(ss, g.data(), ne * sizeof(float), cudaMemcpyHostToDevice);
+  homo::OCOptimizer oc(ne, 0.001f, 0.2f, 0.5f);
+  int reso[3] = {n, n, n};
+  oc.filterSens(ss, srho, n, reso, 2.0f);
+  oc.update(ss, srho, 0.25f);
+  cudaMemcpy(r0.data(), srho, ne * sizeof(float), cudaMemcpyDeviceToHost);
+  double vol = 0;
+  for (float v : r0) vol += v;
+  std::printf("oc_vol %.6f\n", vol / ne);
+
+  // MMA: minimise sum (x - t)^2 subject to mean(x) <= 0.3 through the float interface
+  homo::MMAOptimizer mma(1, ne, 1, 0, 1e3, 1);
+  mma.setBound(0.f, 1.f);
+  std::vector<float> x(ne, 0.5f), t(ne), df(ne), dg(ne, 1.f / (0.3f * ne));
+  for (int e = 0; e < ne; e++) t[e] = u01(3 * ne + e);
+  float *xd, *dfd, *dgd;
+  cudaMalloc(&xd, ne * sizeof(float));
+  cudaMalloc(&dfd, ne * sizeof(float));
+  cudaMalloc(&dgd, ne * sizeof(float));
+  cudaMemcpy(xd, x.data(), ne * sizeof(float), cudaMemcpyHostToDevice);
+  cudaMemcpy(dgd, dg.data(), ne * sizeof(float), cudaMemcpyHostToDevice);
+  for (int it = 1; it <= 30; it++) {
+    cudaMemcpy(x.data(), xd, ne * sizeof(float), cudaMemcpyDeviceToHost);
+    double sx = 0;
+    for (int e = 0; e < ne; e++) {
+      df[e] = 2.f * (x[e] - t[e]);
+      sx += x[e];
+    }
+    float gval = float(sx / (0.3 * ne) - 1.0);
+    cudaMemcpy(dfd, df.data(), ne * sizeof(float), cudaMemcpyHostToDevice);
+    float* rows[1] = {dgd};
+    mma.update(it, xd, dfd, &gval, rows);
+  }
+  cudaMemcpy(x.data(), xd, ne * sizeof(float), cudaMemcpyDeviceToHost);
+  double mean = 0;
+  for (float v : x) mean += v;
+  std::printf("mma_mean %.6f\n", mean / ne);
+  cudaDeviceSynchronize();
+  std::printf("ok\n");
+  return 0;
+}

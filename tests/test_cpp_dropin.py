@@ -1,0 +1,51 @@
+"""The C++ drop-in header compiles against the library (CPU test) and, on a GPU, reproduces the
+Python path's K^H (GPU test)."""
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+SRC = os.path.join(ROOT, "tests", "cpp", "dropin_main.cpp")
+CUDA = "/usr/local/cuda"
+
+
+def _build(tmp_path):
+    exe = os.path.join(str(tmp_path), "dropin")
+    gxx = shutil.which("g++")
+    cmd = [gxx, "-std=c++17", "-O2", SRC, "-o", exe, "-I", os.path.join(ROOT, "include"), "-I",
+           os.path.join(CUDA, "include"), "-L", os.path.join(ROOT, "opentm_b200"), "-lopentm_b200",
+           "-Wl,-rpath," + os.path.join(ROOT, "opentm_b200"), "-L", os.path.join(CUDA, "lib64"), "-lcudart",
+           "-Wl,-rpath," + os.path.join(CUDA, "lib64")]
+    subprocess.run(cmd, check=True)
+    return exe
+
+
+def test_dropin_header_compiles_and_links(tmp_path):
+    exe = _build(tmp_path)
+    assert os.path.exists(exe)
+
+
+@pytest.mark.gpu
+def test_dropin_program_matches_python_path(tmp_path):
+    import torch
+
+    from opentm_b200 import HomoConfig, Homogenization_H
+    from opentm_b200 import workloads as wl
+    exe = _build(tmp_path)
+    out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout
+    vals = {l.split()[0]: [float(v) for v in l.split()[1:]] for l in out.strip().splitlines() if l != "ok"}
+    n = 16
+    rho = (0.001 + 0.999 * wl.uniform(0, n ** 3)).astype(np.float32)
+    k = (1e-3 + rho * rho * rho * (1 - 1e-3)).astype(np.float32).reshape(n, n, n)
+    H = Homogenization_H(HomoConfig(reso=n, femRelThres=1e-6, pre_smooth=2, post_smooth=2))
+    H.update(torch.from_numpy(k).cuda())
+    C = H.heatMatrix()
+    got = np.array(vals["C"])
+    want = np.array([C[0, 0], C[0, 1], C[0, 2], C[1, 1], C[1, 2], C[2, 2]])
+    np.testing.assert_allclose(got, want, rtol=0, atol=1e-12 + 1e-9 * np.abs(want).max())
+    assert vals["relres"][0] <= 1e-7
+    assert abs(vals["oc_vol"][0] - 0.25) <= 1e-4 + 1e-6
+    assert abs(vals["mma_mean"][0] - 0.3) <= 2e-3

@@ -200,3 +200,31 @@ def test_profile_events_inside_graphs():
         assert pr.sweep_ms > 0 and pr.sweep_bytes == 32 ** 3 * 40
         # a following library call still works (no stale error from the event queries)
         H.heatMatrix_nosolve()
+
+
+@pytest.mark.parametrize("precision", ["bf16", "fp16"])
+@pytest.mark.parametrize("shape", [(32, 32, 32), (16, 16, 16), (24, 24, 24)])
+def test_mixed_precision_parity(precision, shape):
+    """16-bit fine-level storage with FP64 refinement meets the same K^H / sensitivity gates."""
+    k, _ = random_k(shape, seed=20 + shape[0])
+    H, C, E, sens = gpu_run(k, tol=1e-6, precision=precision)
+    check_against_oracle(k, C, E, sens)
+    st = H.stats()
+    assert st.refinements == st.iterations > 0 and max(st.rel_res) <= 1e-6
+
+
+def test_mixed_precision_warm_start_and_reset():
+    from opentm_b200 import HomoConfig, Homogenization_H
+    k, _ = random_k((32, 32, 32), seed=30)
+    H = Homogenization_H(HomoConfig(reso=32, femRelThres=1e-6, pre_smooth=2, post_smooth=2, precision="bf16"))
+    H.update(torch.from_numpy(k).cuda())
+    H.heatMatrix()
+    cold = H.stats().iterations
+    H.update(torch.from_numpy(k).cuda())
+    C = H.heatMatrix()
+    assert H.stats().iterations < cold  # the FP64 solution is reused
+    H.reset_displacement()
+    H.update(torch.from_numpy(k).cuda())
+    C2 = H.heatMatrix()
+    assert H.stats().iterations == cold
+    assert rel_c(C2, C) <= KH_TOL
