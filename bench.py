@@ -321,6 +321,92 @@ def run_reference(args, rank, world):
     return line
 
 
+# ---------------------------------------------------------------------------------------
+# Serving workload (configuration 5): Poisson arrivals of mixed-resolution requests
+# ---------------------------------------------------------------------------------------
+def serve_fields(seed=4, per_reso=4):
+    """A few seeded density fields per resolution (i.i.d. U(0.001,1) smoothed by a periodic
+    3x3x3 box mean, SIMP p = 3), reused cyclically by the request stream."""
+    from opentm_b200 import workloads as wl
+    out = {}
+    for n in wl.SERVE_RESOS:
+        fl = []
+        for j in range(per_reso):
+            rho = (0.001 + 0.999 * wl.uniform(seed * 1000 + n * 10 + j, n ** 3)).reshape(n, n, n)
+            for ax in range(3):  # separable periodic box mean
+                rho = (np.roll(rho, 1, ax) + rho + np.roll(rho, -1, ax)) / 3.0
+            fl.append(wl.simp(rho.astype(np.float32)))
+        out[n] = fl
+    return out
+
+
+def run_serve(args):
+    import torch
+
+    from opentm_b200 import HomoConfig, Homogenization_H, Server, launch_count
+    from opentm_b200 import workloads as wl
+    torch.cuda.set_device(0)
+    fields = serve_fields()
+    reqs = wl.serving_requests(args.requests, seed=4, rate=args.rate)
+    # serial plain-FP32 baseline: one handle per request, solved one after another
+    serial = []
+    for (t, n, i) in reqs[: min(len(reqs), 60)]:
+        k = fields[n][i % len(fields[n])]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        H = Homogenization_H(HomoConfig(reso=n, femRelThres=TOL, pre_smooth=2, post_smooth=2, warm_start=False))
+        H.update(torch.from_numpy(k).cuda())
+        H.heatMatrix()
+        torch.cuda.synchronize()
+        serial.append(time.perf_counter() - t0)
+        H.close()
+    srv = Server(hbm_budget_bytes=150 * 10 ** 9, max_active=args.max_active, fem_rel_thres=TOL,
+                 iters_per_step=args.iters_per_step)
+    # warm-up: a few requests of every size
+    for n in wl.SERVE_RESOS:
+        srv.submit(fields[n][0])
+    srv.run_until_idle()
+    l0 = launch_count()
+    t_start = time.perf_counter()
+    pending, arrival, done_at = list(reqs), {}, {}
+    active = []
+    while pending or active:
+        now = time.perf_counter() - t_start
+        while pending and pending[0][0] <= now:
+            t, n, i = pending.pop(0)
+            rid = srv.submit(fields[n][i % len(fields[n])])
+            arrival[rid] = t
+            active.append(rid)
+        if not active:
+            time.sleep(max(0.0, pending[0][0] - now))
+            continue
+        srv.step()
+        now = time.perf_counter() - t_start
+        still = []
+        for rid in active:
+            r = srv.poll(rid)
+            if r is None:
+                still.append(rid)
+            else:
+                done_at[rid] = now
+        active = still
+    makespan = max(done_at.values()) - min(arrival.values())
+    lat = np.array([done_at[r] - arrival[r] for r in done_at]) * 1e3
+    value = len(done_at) / makespan
+    serial_rate = 1.0 / float(np.mean(serial))
+    line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": 1, "steps": len(done_at),
+            "warmup": len(wl.SERVE_RESOS), "ms_per_step": round(1e3 / value, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"serving stream, {len(reqs)} requests, Poisson {args.rate} req/s, "
+                                   f"resolutions {wl.SERVE_RESOS} weights {wl.SERVE_WEIGHTS}",
+                       "rate": args.rate, "max_active": args.max_active, "iters_per_step": args.iters_per_step,
+                       "tol": TOL},
+            "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
+            "serial_fp32_solves_per_s": round(serial_rate, 3), "speedup_vs_serial": round(value / serial_rate, 3),
+            "gpu_launches": int(launch_count() - l0)}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -330,7 +416,15 @@ def main():
     ap.add_argument("--n", type=int, default=N_CELL)
     ap.add_argument("--mixed", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="oc", choices=["oc", "serve"])
+    ap.add_argument("--requests", type=int, default=2000)
+    ap.add_argument("--rate", type=float, default=500.0)
+    ap.add_argument("--max-active", type=int, default=64)
+    ap.add_argument("--iters-per-step", type=int, default=2)
     args = ap.parse_args()
+    if args.workload == "serve":
+        run_serve(args)
+        return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

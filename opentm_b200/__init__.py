@@ -24,7 +24,7 @@ def launch_count() -> int:
     return int(lib().otm_launch_count())
 
 
-__all__ = ["launch_count", 
+__all__ = ["launch_count", "Server", 
     "HomoConfig", "Homogenization_H", "OCOptimizer", "MMAOptimizer", "DensityFilter", "OtmError", "lib",
     "WEIGHT_SPLINE4", "WEIGHT_LINEAR", "filter_forward", "filter_backward",
 ]
@@ -301,3 +301,78 @@ class MMAOptimizer:
         rows = (ctypes.c_void_p * self.m)(*[_ptr(r) for r in dgdx])
         check(lib().otm_mma_update(self._h, int(itn), ctypes.c_void_p(_ptr(x)), ctypes.c_void_p(_ptr(dfdx)), g, rows),
               "otm_mma_update")
+
+
+class Server:
+    """Continuous-batching server of homogenization requests (include/opentm_b200_server.h).
+
+    submit(k) queues a solve of one cell (k: host numpy array of shape (nz, ny, nx)); step()
+    admits what fits the memory budget and advances every running request; poll(id) returns
+    None while the request runs, else (K^H, info).
+    """
+
+    def __init__(self, hbm_budget_bytes=150 * 10 ** 9, max_active=64, fem_rel_thres=1e-6, max_iter=200,
+                 pre_smooth=2, iters_per_step=2, power_penal=1.0, stream=None):
+        cfg = _lib.ServerConfig()
+        check(lib().otm_server_config_init(ctypes.byref(cfg)), "otm_server_config_init")
+        cfg.hbm_budget_bytes = int(hbm_budget_bytes)
+        cfg.max_active = int(max_active)
+        cfg.fem_rel_thres = float(fem_rel_thres)
+        cfg.max_iter = int(max_iter)
+        cfg.pre_smooth = int(pre_smooth)
+        cfg.iters_per_step = int(iters_per_step)
+        cfg.power_penal = float(power_penal)
+        self._h = ctypes.c_void_p()
+        check(lib().otm_server_create(ctypes.byref(cfg), ctypes.c_void_p(_stream(stream)), ctypes.byref(self._h)),
+              "otm_server_create")
+
+    def close(self):
+        if self._h:
+            lib().otm_server_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def request_bytes(reso) -> int:
+        return int(lib().otm_server_request_bytes(i3(reso)))
+
+    def bytes_in_use(self) -> int:
+        return int(lib().otm_server_bytes_in_use(self._h))
+
+    def submit(self, k) -> int:
+        k = np.ascontiguousarray(k, dtype=np.float32)
+        nz, ny, nx = k.shape
+        rid = ctypes.c_int64(0)
+        check(lib().otm_server_submit(self._h, i3((nx, ny, nz)), k.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                      ctypes.byref(rid)), "otm_server_submit")
+        return rid.value
+
+    def step(self):
+        nr, nq = ctypes.c_int(0), ctypes.c_int(0)
+        check(lib().otm_server_step(self._h, ctypes.byref(nr), ctypes.byref(nq)), "otm_server_step")
+        return nr.value, nq.value
+
+    def poll(self, rid):
+        C = (ctypes.c_double * 9)()
+        info = _lib.RequestInfo()
+        st = lib().otm_server_poll(self._h, ctypes.c_int64(rid), C, ctypes.byref(info))
+        if st == _lib.OTM_ERR_NOT_READY:
+            return None
+        if st not in (0, _lib.OTM_ERR_NOT_CONVERGED):
+            raise OtmError(st, "otm_server_poll", _lib.last_error())
+        return np.array(C[:]).reshape(3, 3), info
+
+    def cancel(self, rid):
+        check(lib().otm_server_cancel(self._h, ctypes.c_int64(rid)), "otm_server_cancel")
+
+    def run_until_idle(self, max_steps=100000):
+        for _ in range(max_steps):
+            nr, nq = self.step()
+            if nr == 0 and nq == 0:
+                return
+        raise RuntimeError("server did not drain")

@@ -68,6 +68,17 @@ class Profile(ctypes.Structure):
                 ("launches_per_sweep", ctypes.c_int)]
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_size_t), ("max_active", ctypes.c_int), ("fem_rel_thres", ctypes.c_double),
+                ("max_iter", ctypes.c_int), ("pre_smooth", ctypes.c_int), ("iters_per_step", ctypes.c_int),
+                ("power_penal", ctypes.c_float)]
+
+
+class RequestInfo(ctypes.Structure):
+    _fields_ = [("state", ctypes.c_int), ("status", ctypes.c_int), ("submit_s", ctypes.c_double),
+                ("admit_s", ctypes.c_double), ("done_s", ctypes.c_double), ("stats", SolveStats)]
+
+
 class PitchedPtr(ctypes.Structure):
     _fields_ = [("ptr", ctypes.c_void_p), ("pitch", ctypes.c_size_t), ("xsize", ctypes.c_size_t),
                 ("ysize", ctypes.c_size_t)]
@@ -124,6 +135,15 @@ SIGNATURES = {
     "otm_mmasub_device": (_S, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P, _P, _P, _P, ctypes.c_double, _P,
                                _P, PitchedPtr, _P, _P, ctypes.c_double, _P, _P, _P, ctypes.c_double, _P]),
     # serving (include/opentm_b200_server.h)
+    "otm_server_config_init": (_S, [ctypes.POINTER(ServerConfig)]),
+    "otm_server_create": (_S, [ctypes.POINTER(ServerConfig), _P, ctypes.POINTER(_P)]),
+    "otm_server_destroy": (_S, [_P]),
+    "otm_server_submit": (_S, [_P, _I3, _F, ctypes.POINTER(ctypes.c_int64)]),
+    "otm_server_step": (_S, [_P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "otm_server_poll": (_S, [_P, ctypes.c_int64, _D, ctypes.POINTER(RequestInfo)]),
+    "otm_server_cancel": (_S, [_P, ctypes.c_int64]),
+    "otm_server_request_bytes": (ctypes.c_size_t, [_I3]),
+    "otm_server_bytes_in_use": (ctypes.c_size_t, [_P]),
 }
 
 _lib = None

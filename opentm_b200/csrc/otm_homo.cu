@@ -62,7 +62,7 @@ static constexpr int kMaxCoarsest = 1024;
 static bool mixed_supported() { return true; }
 
 otm_status Homo::alloc(void** p, size_t bytes) {
-  cudaError_t e = cudaMalloc(p, bytes);
+  cudaError_t e = pool ? cudaMallocFromPoolAsync(p, bytes, pool, stream) : cudaMalloc(p, bytes);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc");
   allocations.push_back(*p);
   bytes_allocated += bytes;
@@ -72,18 +72,25 @@ otm_status Homo::alloc(void** p, size_t bytes) {
 Homo::~Homo() {
   for (auto& g : graphs)
     if (g.exec) cudaGraphExecDestroy(g.exec);
-  if (stream) cudaStreamDestroy(stream);
+  if (stream && !external) cudaStreamDestroy(stream);
   if (ev_in) cudaEventDestroy(ev_in);
   if (ev_out) cudaEventDestroy(ev_out);
   for (int a = 0; a < 2; a++)
     for (int j = 0; j < kMaxChunk; j++)
       if (prof_ev[a][j]) cudaEventDestroy(prof_ev[a][j]);
-  for (void* p : allocations) cudaFree(p);
+  for (void* p : allocations) {
+    if (pool)
+      cudaFreeAsync(p, stream);
+    else
+      cudaFree(p);
+  }
   if (sc_host) cudaFreeHost(sc_host);
 }
 
-otm_status Homo::build(const otm_config& c) {
+otm_status Homo::build(const otm_config& c, cudaStream_t ext_stream, cudaMemPool_t ext_pool, bool external_mode) {
   cfg = c;
+  external = external_mode;
+  pool = ext_pool;
   for (int i = 0; i < 3; i++) {
     if (cfg.reso[i] < 2) return invalid("resolution must be >= 2 per axis");
     if (cfg.reso[i] > 1024) {
@@ -128,9 +135,13 @@ otm_status Homo::build(const otm_config& c) {
       ef.feMu[j][cc] = float(tm.feMu[j][cc]);
     }
 
-  OTM_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-  OTM_CUDA(cudaEventCreateWithFlags(&ev_in, cudaEventDisableTiming));
-  OTM_CUDA(cudaEventCreateWithFlags(&ev_out, cudaEventDisableTiming));
+  if (external) {
+    stream = ext_stream;
+  } else {
+    OTM_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    OTM_CUDA(cudaEventCreateWithFlags(&ev_in, cudaEventDisableTiming));
+    OTM_CUDA(cudaEventCreateWithFlags(&ev_out, cudaEventDisableTiming));
+  }
   if (cfg.profile)
     for (int a = 0; a < 2; a++)
       for (int j = 0; j < kMaxChunk; j++) OTM_CUDA(cudaEventCreate(&prof_ev[a][j]));
@@ -183,12 +194,14 @@ otm_status Homo::build(const otm_config& c) {
   OTM_TRY(alloc((void**)&flags, 4 * sizeof(int)));
   OTM_CUDA(cudaMemsetAsync(sc, 0, sizeof(SolveScalars), stream));
   OTM_CUDA(cudaMemsetAsync(flags, 0, 4 * sizeof(int), stream));
-  OTM_CUDA(cudaMallocHost((void**)&sc_host, sizeof(SolveScalars)));
+  // pinned block: solve scalars, then the level-1 Galerkin table (uploaded from pinned memory
+  // so the copy never waits for the stream)
+  OTM_CUDA(cudaMallocHost((void**)&sc_host, sizeof(SolveScalars) + 64 * 27 * sizeof(float)));
   std::memset(sc_host, 0, sizeof(SolveScalars));
-  std::vector<float> tab(64 * 27);
-  galerkin_level1_table(tm, tab.data());
-  OTM_CUDA(cudaMemcpyAsync(table, tab.data(), tab.size() * sizeof(float), cudaMemcpyHostToDevice, stream));
-  OTM_CUDA(cudaStreamSynchronize(stream));
+  float* tab = (float*)(sc_host + 1);
+  galerkin_level1_table(tm, tab);
+  OTM_CUDA(cudaMemcpyAsync(table, tab, 64 * 27 * sizeof(float), cudaMemcpyHostToDevice, stream));
+  if (!external) OTM_CUDA(cudaStreamSynchronize(stream));
   // small levels (<= 16^3 unknowns) and the coarsest solve run in one single-CTA kernel
   {
     const int L = int(lv.size());
@@ -216,12 +229,14 @@ otm_status Homo::build(const otm_config& c) {
 }
 
 otm_status Homo::enter() {
+  if (external) return OTM_OK;
   OTM_CUDA(cudaEventRecord(ev_in, user_stream));
   OTM_CUDA(cudaStreamWaitEvent(stream, ev_in, 0));
   return OTM_OK;
 }
 
 otm_status Homo::leave() {
+  if (external) return OTM_OK;
   OTM_CUDA(cudaEventRecord(ev_out, stream));
   OTM_CUDA(cudaStreamWaitEvent(user_stream, ev_out, 0));
   return OTM_OK;
@@ -498,6 +513,28 @@ otm_status Homo::run_chunk(int iters) {
   OTM_CUDA(cudaGraphLaunch(g->exec, stream));
   count_launches(g->kernel_nodes);
   return OTM_OK;
+}
+
+// Right-hand sides, nullspace projection and initial residual of an FP32 solve from a zero
+// initial guess (launches only; used by the serving form).
+void Homo::launch_solve_init() {
+  const Dims d0 = lv[0].d;
+  const size_t nv = d0.nv();
+  const int nb = reduce_blocks(nv);
+  cudaMemsetAsync(x, 0, 3 * nv * sizeof(float), stream);
+  k_rhs<<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(d0, ks, ef, b);
+  k_sums2<<<nb, kBlock, 0, stream>>>(nv, b, x, partials, means, &sc->counter[T_MEAN]);
+  k_sub_means<<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(nv, b, x, means);
+  sc_host->tol = cfg.fem_rel_thres;
+  cudaMemcpyAsync(&sc->tol, &sc_host->tol, sizeof(double), cudaMemcpyHostToDevice, stream);
+  k_init_residual<false><<<nb, kBlock, 0, stream>>>(d0, ks, op, x, b, lv[0].f, partials, sc);
+  launched(4);
+}
+
+void Homo::launch_heat_matrix() {
+  const Dims d0 = lv[0].d;
+  k_heat_matrix<<<reduce_blocks(d0.nv()), kBlock, 0, stream>>>(d0, ks, x, op, ef, partials, sc);
+  launched(1);
 }
 
 // Solve the 3 load cases to the tolerance (MG_H::solveEquation, homogenization/MG.cpp:80-142;

@@ -64,6 +64,9 @@ struct Homo {
   double* partials = nullptr;
   double* means = nullptr;
   int* flags = nullptr;  // [0] bad import value, [1] coarsest not SPD
+  // server mode: work on the server's stream, allocate from its memory pool, never block
+  bool external = false;
+  cudaMemPool_t pool = nullptr;
   std::vector<void*> allocations;
   size_t bytes_allocated = 0;
   std::vector<ChunkGraph> graphs;
@@ -79,7 +82,10 @@ struct Homo {
 
   ~Homo();
   otm_status alloc(void** p, size_t bytes);
-  otm_status build(const otm_config& c);
+  otm_status build(const otm_config& c, cudaStream_t ext_stream = nullptr, cudaMemPool_t ext_pool = nullptr,
+                   bool external_mode = false);
+  void launch_solve_init();
+  void launch_heat_matrix();
   otm_status enter();
   otm_status leave();
   otm_status update(const float* kin, int pitchT);

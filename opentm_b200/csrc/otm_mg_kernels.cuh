@@ -67,6 +67,20 @@ __device__ __forceinline__ bool last_block(unsigned int* counter) {
   return is_last;
 }
 
+// As last_block for a block range of nblk blocks (batched launches: one range per request).
+__device__ __forceinline__ bool last_block_n(unsigned int* counter, unsigned int nblk) {
+  __shared__ bool is_last_n;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned int prev = atomicAdd(counter, 1u);
+    is_last_n = (prev == nblk - 1);
+  }
+  __syncthreads();
+  if (is_last_n) __threadfence();
+  return is_last_n;
+}
+
 // Fixed-order sum of NV partial columns (partials[b * NV + i], b < nb) inside one block.
 template <int NV>
 __device__ __forceinline__ void reduce_partials(const double* partials, int nb, double (&out)[NV], double* smem) {
@@ -190,14 +204,11 @@ __device__ __forceinline__ float fine_offdiag(const float (&k8)[8], const FineOp
 // is replaced by mean projection in the outer solver).
 // fscale (optional): per-case factor applied to f when it is read (scaled right-hand side of
 // the mixed-precision inner cycle).
-template <bool kFace, int NC, typename KT = float, typename VT = float>
-__global__ void __launch_bounds__(kBlock) k_gs_fine(Dims d, int color, const KT* __restrict__ ks, FineOp op,
-                                                     VT* u, const float* __restrict__ f, const SolveScalars* sc,
-                                                     const double* fscale = nullptr) {
-  if (sc && solve_done(sc)) return;
+template <bool kFace, int NC, typename KT, typename VT>
+__device__ __forceinline__ void gs_fine_body(const Dims& d, int color, const KT* __restrict__ ks, const FineOp& op,
+                                             VT* u, const float* __restrict__ f, const double* fscale, size_t t) {
   const int hx = d.nx >> 1, hy = d.ny >> 1;
   const size_t nsub = d.nv() >> 3;
-  const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (t >= nsub) return;
   const int i = int(t % hx), j = int((t / hx) % hy), kq = int(t / (size_t(hx) * hy));
   const int x = 2 * i + (color & 1), y = 2 * j + ((color >> 1) & 1), z = 2 * kq + (color >> 2);
@@ -216,15 +227,20 @@ __global__ void __launch_bounds__(kBlock) k_gs_fine(Dims d, int color, const KT*
   for (int c = 0; c < NC; c++) st(u + c * nv + v, acc[c] * inv);
 }
 
-// r = f - A u on the fine level for every vertex.
 template <bool kFace, int NC, typename KT = float, typename VT = float>
-__global__ void __launch_bounds__(kBlock) k_resid_fine(Dims d, const KT* __restrict__ ks, FineOp op,
-                                                        const VT* __restrict__ u, const float* __restrict__ f,
-                                                        VT* __restrict__ r, const SolveScalars* sc,
-                                                        const double* fscale = nullptr) {
+__global__ void __launch_bounds__(kBlock) k_gs_fine(Dims d, int color, const KT* __restrict__ ks, FineOp op,
+                                                     VT* u, const float* __restrict__ f, const SolveScalars* sc,
+                                                     const double* fscale = nullptr) {
   if (sc && solve_done(sc)) return;
+  gs_fine_body<kFace, NC, KT, VT>(d, color, ks, op, u, f, fscale, size_t(blockIdx.x) * blockDim.x + threadIdx.x);
+}
+
+// r = f - A u on the fine level for every vertex.
+template <bool kFace, int NC, typename KT, typename VT>
+__device__ __forceinline__ void resid_fine_body(const Dims& d, const KT* __restrict__ ks, const FineOp& op,
+                                                const VT* __restrict__ u, const float* __restrict__ f,
+                                                VT* __restrict__ r, const double* fscale, size_t v) {
   const size_t nv = d.nv();
-  const size_t v = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (v >= nv) return;
   const int x = int(v % d.nx), y = int((v / d.nx) % d.ny), z = int(v / (size_t(d.nx) * d.ny));
   Nbr nb;
@@ -239,6 +255,15 @@ __global__ void __launch_bounds__(kBlock) k_resid_fine(Dims d, const KT* __restr
   for (int c = 0; c < NC; c++) st(r + c * nv + v, acc[c] - diag * ld(u + c * nv + v));
 }
 
+template <bool kFace, int NC, typename KT = float, typename VT = float>
+__global__ void __launch_bounds__(kBlock) k_resid_fine(Dims d, const KT* __restrict__ ks, FineOp op,
+                                                        const VT* __restrict__ u, const float* __restrict__ f,
+                                                        VT* __restrict__ r, const SolveScalars* sc,
+                                                        const double* fscale = nullptr) {
+  if (sc && solve_done(sc)) return;
+  resid_fine_body<kFace, NC, KT, VT>(d, ks, op, u, f, r, fscale, size_t(blockIdx.x) * blockDim.x + threadIdx.x);
+}
+
 // ------------------------------------------------------------------------------------
 // Coarse levels (27-point stencils, colour-blocked).
 // ------------------------------------------------------------------------------------
@@ -249,12 +274,10 @@ __device__ __forceinline__ size_t cb_index(const Dims& d, int x, int y, int z) {
 }
 
 template <int NC>
-__global__ void __launch_bounds__(kBlock) k_gs_coarse(Dims d, int color, const float* __restrict__ st, float* u,
-                                                       const float* __restrict__ f, const SolveScalars* sc) {
-  if (sc && solve_done(sc)) return;
+__device__ __forceinline__ void gs_coarse_body(const Dims& d, int color, const float* __restrict__ st, float* u,
+                                               const float* __restrict__ f, size_t t) {
   const int hx = d.nx >> 1, hy = d.ny >> 1;
   const size_t nsub = d.nv() >> 3;
-  const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (t >= nsub) return;
   const int i = int(t % hx), j = int((t / hx) % hy), kq = int(t / (size_t(hx) * hy));
   const int x = 2 * i + (color & 1), y = 2 * j + ((color >> 1) & 1), z = 2 * kq + (color >> 2);
@@ -280,12 +303,17 @@ __global__ void __launch_bounds__(kBlock) k_gs_coarse(Dims d, int color, const f
 }
 
 template <int NC>
-__global__ void __launch_bounds__(kBlock) k_resid_coarse(Dims d, const float* __restrict__ st,
-                                                          const float* __restrict__ u, const float* __restrict__ f,
-                                                          float* __restrict__ r, const SolveScalars* sc) {
+__global__ void __launch_bounds__(kBlock) k_gs_coarse(Dims d, int color, const float* __restrict__ st, float* u,
+                                                       const float* __restrict__ f, const SolveScalars* sc) {
   if (sc && solve_done(sc)) return;
+  gs_coarse_body<NC>(d, color, st, u, f, size_t(blockIdx.x) * blockDim.x + threadIdx.x);
+}
+
+template <int NC>
+__device__ __forceinline__ void resid_coarse_body(const Dims& d, const float* __restrict__ st,
+                                                  const float* __restrict__ u, const float* __restrict__ f,
+                                                  float* __restrict__ r, size_t v) {
   const size_t nv = d.nv();
-  const size_t v = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (v >= nv) return;
   const int x = int(v % d.nx), y = int((v / d.nx) % d.ny), z = int(v / (size_t(d.nx) * d.ny));
   Nbr nb;
@@ -305,14 +333,20 @@ __global__ void __launch_bounds__(kBlock) k_resid_coarse(Dims d, const float* __
   for (int c = 0; c < NC; c++) r[c * nv + v] = acc[c];
 }
 
+template <int NC>
+__global__ void __launch_bounds__(kBlock) k_resid_coarse(Dims d, const float* __restrict__ st,
+                                                          const float* __restrict__ u, const float* __restrict__ f,
+                                                          float* __restrict__ r, const SolveScalars* sc) {
+  if (sc && solve_done(sc)) return;
+  resid_coarse_body<NC>(d, st, u, f, r, size_t(blockIdx.x) * blockDim.x + threadIdx.x);
+}
+
 // f_c(V) = sum_d w(d) r_f(2V + d), w = prod (1 - |d|/2): full weighting = P^T
 // (homogenization/grid.cu:811-878).
-template <int NC, typename VT = float>
-__global__ void __launch_bounds__(kBlock) k_restrict(Dims df, Dims dc, const VT* __restrict__ r,
-                                                      float* __restrict__ fc, const SolveScalars* sc) {
-  if (sc && solve_done(sc)) return;
+template <int NC, typename VT>
+__device__ __forceinline__ void restrict_body(const Dims& df, const Dims& dc, const VT* __restrict__ r,
+                                              float* __restrict__ fc, size_t V) {
   const size_t nvc = dc.nv(), nvf = df.nv();
-  const size_t V = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (V >= nvc) return;
   const int X = int(V % dc.nx), Y = int((V / dc.nx) % dc.ny), Z = int(V / (size_t(dc.nx) * dc.ny));
   Nbr nb;
@@ -332,13 +366,18 @@ __global__ void __launch_bounds__(kBlock) k_restrict(Dims df, Dims dc, const VT*
   for (int c = 0; c < NC; c++) fc[c * nvc + V] = acc[c];
 }
 
-// u_f += P u_c, trilinear interpolation (homogenization/grid.cu:881-940).
 template <int NC, typename VT = float>
-__global__ void __launch_bounds__(kBlock) k_prolong(Dims df, Dims dc, const float* __restrict__ uc, VT* uf,
-                                                     const SolveScalars* sc) {
+__global__ void __launch_bounds__(kBlock) k_restrict(Dims df, Dims dc, const VT* __restrict__ r,
+                                                      float* __restrict__ fc, const SolveScalars* sc) {
   if (sc && solve_done(sc)) return;
+  restrict_body<NC, VT>(df, dc, r, fc, size_t(blockIdx.x) * blockDim.x + threadIdx.x);
+}
+
+// u_f += P u_c, trilinear interpolation (homogenization/grid.cu:881-940).
+template <int NC, typename VT>
+__device__ __forceinline__ void prolong_body(const Dims& df, const Dims& dc, const float* __restrict__ uc, VT* uf,
+                                             size_t v) {
   const size_t nvc = dc.nv(), nvf = df.nv();
-  const size_t v = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (v >= nvf) return;
   const int x = int(v % df.nx), y = int((v / df.nx) % df.ny), z = int(v / (size_t(df.nx) * df.ny));
   const int X0 = x >> 1, Y0 = y >> 1, Z0 = z >> 1;
@@ -358,6 +397,13 @@ __global__ void __launch_bounds__(kBlock) k_prolong(Dims df, Dims dc, const floa
                            wy1 * (wx0 * __ldg(u + r11 + X0) + wx1 * __ldg(u + r11 + X1)));
     st(uf + c * nvf + v, ld(uf + c * nvf + v) + a);
   }
+}
+
+template <int NC, typename VT = float>
+__global__ void __launch_bounds__(kBlock) k_prolong(Dims df, Dims dc, const float* __restrict__ uc, VT* uf,
+                                                     const SolveScalars* sc) {
+  if (sc && solve_done(sc)) return;
+  prolong_body<NC, VT>(df, dc, uc, uf, size_t(blockIdx.x) * blockDim.x + threadIdx.x);
 }
 
 // ------------------------------------------------------------------------------------

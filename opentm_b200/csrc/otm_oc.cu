@@ -50,9 +50,15 @@ __global__ void __launch_bounds__(kBlock) k_oc_maxabs(int ne, const float* __res
     partials[blockIdx.x] = b;
   }
   if (last_block(&st->counter)) {
+    double b = 0.0;
+    for (int i = threadIdx.x; i < int(gridDim.x); i += blockDim.x) b = fmax(b, ((volatile double*)partials)[i]);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) b = fmax(b, __shfl_down_sync(0xffffffffu, b, off));
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) smem[threadIdx.x >> 5] = b;
+    __syncthreads();
     if (threadIdx.x == 0) {
-      double b = 0.0;
-      for (int i = 0; i < int(gridDim.x); i++) b = fmax(b, ((volatile double*)partials)[i]);
+      for (int w = 0; w < (blockDim.x + 31) / 32; w++) b = fmax(b, smem[w]);
       st->gmax = b;
       st->gmin = 0.0;
       st->g = b / 2;
@@ -70,17 +76,18 @@ __global__ void __launch_bounds__(kBlock) k_oc_maxabs(int ne, const float* __res
 constexpr int kTreeDepth = 5;
 constexpr int kTreeNodes = (1 << kTreeDepth) - 1;
 
-__device__ __forceinline__ void oc_tree(float gmin, float gmax, float (&g)[kTreeNodes]) {
+// Node i of the bisection tree below [gmin, gmax]: midpoints in FP32, children 2i+1 (volume
+// too small: gmax = g) and 2i+2 (volume too large: gmin = g).
+__device__ void oc_tree(float gmin, float gmax, float* g) {
   float lo[kTreeNodes], hi[kTreeNodes];
   lo[0] = gmin;
   hi[0] = gmax;
-#pragma unroll
   for (int i = 0; i < kTreeNodes; i++) {
     g[i] = (hi[i] + lo[i]) / 2;
     if (2 * i + 2 < kTreeNodes) {
-      lo[2 * i + 1] = lo[i];  // volume too small: gmax = g
+      lo[2 * i + 1] = lo[i];
       hi[2 * i + 1] = g[i];
-      lo[2 * i + 2] = g[i];   // volume too large: gmin = g
+      lo[2 * i + 2] = g[i];
       hi[2 * i + 2] = hi[i];
     }
   }
@@ -90,24 +97,40 @@ __global__ void __launch_bounds__(kBlock) k_oc_tree_pass(int ne, const float* __
                                                          const float* __restrict__ rho, float volratio, float min_rho,
                                                          float step, float damp, double* partials, OcState* st) {
   if (*((volatile int*)&st->done)) return;
-  __shared__ double smem[32 * kTreeNodes];
-  float g[kTreeNodes];
-  oc_tree(float(st->gmin), float(st->gmax), g);
-  double v[kTreeNodes];
+  __shared__ float g[kTreeNodes];
+  __shared__ float wsum[kBlock / 32][kTreeNodes];
+  if (threadIdx.x == 0) oc_tree(float(st->gmin), float(st->gmax), g);
+  __syncthreads();
+  // per-thread FP32 partial volumes of the 31 candidates (a few elements per thread)
+  float v[kTreeNodes];
 #pragma unroll
-  for (int t = 0; t < kTreeNodes; t++) v[t] = 0.0;
+  for (int t = 0; t < kTreeNodes; t++) v[t] = 0.f;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ne; i += gridDim.x * blockDim.x) {
     const float s = __ldg(sens + i), r = __ldg(rho + i);
 #pragma unroll
     for (int t = 0; t < kTreeNodes; t++) v[t] += oc_new_rho(s, r, g[t], min_rho, step, damp);
   }
-  block_reduce_f64<kTreeNodes>(v, smem);
-  if (threadIdx.x == 0)
 #pragma unroll
-    for (int t = 0; t < kTreeNodes; t++) partials[blockIdx.x * kTreeNodes + t] = v[t];
+  for (int t = 0; t < kTreeNodes; t++)
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v[t] += __shfl_down_sync(0xffffffffu, v[t], off);
+  if ((threadIdx.x & 31) == 0)
+#pragma unroll
+    for (int t = 0; t < kTreeNodes; t++) wsum[threadIdx.x >> 5][t] = v[t];
+  __syncthreads();
+  if (threadIdx.x < kTreeNodes) {
+    double b = 0.0;
+    for (int w = 0; w < int(blockDim.x) / 32; w++) b += double(wsum[w][threadIdx.x]);
+    partials[blockIdx.x * kTreeNodes + threadIdx.x] = b;
+  }
   if (last_block(&st->counter)) {
-    double tot[kTreeNodes];
-    reduce_partials<kTreeNodes>(partials, gridDim.x, tot, smem);
+    __shared__ double tot[kTreeNodes];
+    if (threadIdx.x < kTreeNodes) {
+      double a = 0.0;
+      for (int b = 0; b < int(gridDim.x); b++) a += ((volatile double*)partials)[b * kTreeNodes + threadIdx.x];
+      tot[threadIdx.x] = a;
+    }
+    __syncthreads();
     if (threadIdx.x == 0) {
       int node = 0;
       for (int depth = 0; depth < kTreeDepth && !st->done; depth++) {

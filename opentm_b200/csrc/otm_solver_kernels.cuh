@@ -176,12 +176,11 @@ __global__ void __launch_bounds__(kBlock) k_init_residual(Dims d, const float* _
 }
 
 // rho = r . z, zbar = mean z, rbar-correction; beta = rho / rho_old (0 on the first step).
-static __global__ void __launch_bounds__(kBlock) k_dot_rz(size_t nv, const float* __restrict__ r,
-                                                   const float* __restrict__ z, double* partials, SolveScalars* sc) {
-  if (solve_done(sc)) return;
+__device__ __forceinline__ void dot_rz_body(size_t nv, const float* __restrict__ r, const float* __restrict__ z,
+                                            double* partials, SolveScalars* sc, unsigned int blk, unsigned int nblk) {
   __shared__ double smem[32 * 9];
   double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nv; i += size_t(gridDim.x) * blockDim.x) {
+  for (size_t i = size_t(blk) * blockDim.x + threadIdx.x; i < nv; i += size_t(nblk) * blockDim.x) {
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       const double rc = r[c * nv + i], zc = z[c * nv + i];
@@ -193,10 +192,10 @@ static __global__ void __launch_bounds__(kBlock) k_dot_rz(size_t nv, const float
   block_reduce_f64<9>(v, smem);
   if (threadIdx.x == 0)
 #pragma unroll
-    for (int i = 0; i < 9; i++) partials[blockIdx.x * 9 + i] = v[i];
-  if (last_block(&sc->counter[T_RZ])) {
+    for (int i = 0; i < 9; i++) partials[blk * 9 + i] = v[i];
+  if (last_block_n(&sc->counter[T_RZ], nblk)) {
     double t[9];
-    reduce_partials<9>(partials, gridDim.x, t, smem);
+    reduce_partials<9>(partials, nblk, t, smem);
     if (threadIdx.x == 0) {
       for (int c = 0; c < 3; c++) {
         const double zbar = t[3 + c] / double(nv);
@@ -212,11 +211,15 @@ static __global__ void __launch_bounds__(kBlock) k_dot_rz(size_t nv, const float
   }
 }
 
-// p = (z - zbar) + beta p
-static __global__ void __launch_bounds__(kBlock) k_update_p(size_t nv, const float* __restrict__ z, float* p,
-                                                     const SolveScalars* sc) {
+static __global__ void __launch_bounds__(kBlock) k_dot_rz(size_t nv, const float* __restrict__ r,
+                                                   const float* __restrict__ z, double* partials, SolveScalars* sc) {
   if (solve_done(sc)) return;
-  const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  dot_rz_body(nv, r, z, partials, sc, blockIdx.x, gridDim.x);
+}
+
+// p = (z - zbar) + beta p
+__device__ __forceinline__ void update_p_body(size_t nv, const float* __restrict__ z, float* p,
+                                              const SolveScalars* sc, size_t i) {
   if (i >= nv) return;
 #pragma unroll
   for (int c = 0; c < 3; c++) {
@@ -225,16 +228,21 @@ static __global__ void __launch_bounds__(kBlock) k_update_p(size_t nv, const flo
   }
 }
 
+static __global__ void __launch_bounds__(kBlock) k_update_p(size_t nv, const float* __restrict__ z, float* p,
+                                                     const SolveScalars* sc) {
+  if (solve_done(sc)) return;
+  update_p_body(nv, z, p, sc, size_t(blockIdx.x) * blockDim.x + threadIdx.x);
+}
+
 // q = A p on the fine level and alpha = rho / (p . q).
 template <bool kFace>
-__global__ void __launch_bounds__(kBlock) k_apply_dot(Dims d, const float* __restrict__ ks, FineOp op,
-                                                      const float* __restrict__ p, float* __restrict__ q,
-                                                      double* partials, SolveScalars* sc) {
-  if (solve_done(sc)) return;
+__device__ __forceinline__ void apply_dot_body(const Dims& d, const float* __restrict__ ks, const FineOp& op,
+                                               const float* __restrict__ p, float* __restrict__ q, double* partials,
+                                               SolveScalars* sc, unsigned int blk, unsigned int nblk) {
   __shared__ double smem[32 * 3];
   const size_t nv = d.nv();
   double v[3] = {0, 0, 0};
-  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nv; i += size_t(gridDim.x) * blockDim.x) {
+  for (size_t i = size_t(blk) * blockDim.x + threadIdx.x; i < nv; i += size_t(nblk) * blockDim.x) {
     const int xx = int(i % d.nx), yy = int((i / d.nx) % d.ny), zz = int(i / (size_t(d.nx) * d.ny));
     Nbr nb;
     nb.init(d, xx, yy, zz);
@@ -253,10 +261,10 @@ __global__ void __launch_bounds__(kBlock) k_apply_dot(Dims d, const float* __res
   block_reduce_f64<3>(v, smem);
   if (threadIdx.x == 0)
 #pragma unroll
-    for (int i = 0; i < 3; i++) partials[blockIdx.x * 3 + i] = v[i];
-  if (last_block(&sc->counter[T_PQ])) {
+    for (int i = 0; i < 3; i++) partials[blk * 3 + i] = v[i];
+  if (last_block_n(&sc->counter[T_PQ], nblk)) {
     double t[3];
-    reduce_partials<3>(partials, gridDim.x, t, smem);
+    reduce_partials<3>(partials, nblk, t, smem);
     if (threadIdx.x == 0) {
       for (int c = 0; c < 3; c++) sc->alpha[c] = t[c] != 0.0 ? sc->rz[c] / t[c] : 0.0;
       sc->counter[T_PQ] = 0;
@@ -264,17 +272,24 @@ __global__ void __launch_bounds__(kBlock) k_apply_dot(Dims d, const float* __res
   }
 }
 
-// x += alpha p, r -= alpha q, ||r||^2 -> relative residual and the done flag.
-static __global__ void __launch_bounds__(kBlock) k_update_xr(size_t nv, float* x, float* r, const float* __restrict__ p,
-                                                      const float* __restrict__ q, double* partials,
-                                                      SolveScalars* sc, int max_iter) {
+template <bool kFace>
+__global__ void __launch_bounds__(kBlock) k_apply_dot(Dims d, const float* __restrict__ ks, FineOp op,
+                                                      const float* __restrict__ p, float* __restrict__ q,
+                                                      double* partials, SolveScalars* sc) {
   if (solve_done(sc)) return;
+  apply_dot_body<kFace>(d, ks, op, p, q, partials, sc, blockIdx.x, gridDim.x);
+}
+
+// x += alpha p, r -= alpha q, ||r||^2 -> relative residual and the done flag.
+__device__ __forceinline__ void update_xr_body(size_t nv, float* x, float* r, const float* __restrict__ p,
+                                               const float* __restrict__ q, double* partials, SolveScalars* sc,
+                                               int max_iter, unsigned int blk, unsigned int nblk) {
   __shared__ double smem[32 * 3];
   float al[3];
 #pragma unroll
   for (int c = 0; c < 3; c++) al[c] = float(sc->alpha[c]);
   double v[3] = {0, 0, 0};
-  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nv; i += size_t(gridDim.x) * blockDim.x) {
+  for (size_t i = size_t(blk) * blockDim.x + threadIdx.x; i < nv; i += size_t(nblk) * blockDim.x) {
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       x[c * nv + i] += al[c] * p[c * nv + i];
@@ -286,10 +301,10 @@ static __global__ void __launch_bounds__(kBlock) k_update_xr(size_t nv, float* x
   block_reduce_f64<3>(v, smem);
   if (threadIdx.x == 0)
 #pragma unroll
-    for (int i = 0; i < 3; i++) partials[blockIdx.x * 3 + i] = v[i];
-  if (last_block(&sc->counter[T_RR])) {
+    for (int i = 0; i < 3; i++) partials[blk * 3 + i] = v[i];
+  if (last_block_n(&sc->counter[T_RR], nblk)) {
     double t[3];
-    reduce_partials<3>(partials, gridDim.x, t, smem);
+    reduce_partials<3>(partials, nblk, t, smem);
     if (threadIdx.x == 0) {
       bool all = true, bad = false;
       for (int c = 0; c < 3; c++) {
@@ -305,6 +320,13 @@ static __global__ void __launch_bounds__(kBlock) k_update_xr(size_t nv, float* x
       sc->counter[T_RR] = 0;
     }
   }
+}
+
+static __global__ void __launch_bounds__(kBlock) k_update_xr(size_t nv, float* x, float* r, const float* __restrict__ p,
+                                                      const float* __restrict__ q, double* partials,
+                                                      SolveScalars* sc, int max_iter) {
+  if (solve_done(sc)) return;
+  update_xr_body(nv, x, r, p, q, partials, sc, max_iter, blockIdx.x, gridDim.x);
 }
 
 // Stationary V-cycle iteration: r = b - A x with ||r||^2 -> relres/done (MG_H::solveEquation,

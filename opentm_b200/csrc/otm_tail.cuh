@@ -164,9 +164,7 @@ __device__ __forceinline__ void tail_coarsest(const TailLevel& L, float* sm, con
   }
 }
 
-static __global__ void __launch_bounds__(kTailThreads) k_vcycle_tail(TailDesc td, const SolveScalars* sc) {
-  if (sc && solve_done(sc)) return;
-  extern __shared__ float sm[];
+__device__ __forceinline__ void vcycle_tail_body(const TailDesc& td, float* sm) {
   const int L = td.nlev;
   // load the first tail level's right-hand side
   {
@@ -208,6 +206,12 @@ static __global__ void __launch_bounds__(kTailThreads) k_vcycle_tail(TailDesc td
     const float* u = sm + td.lv[0].off;
     for (int i = threadIdx.x; i < 3 * nv; i += blockDim.x) td.u_out[i] = u[i];
   }
+}
+
+static __global__ void __launch_bounds__(kTailThreads) k_vcycle_tail(TailDesc td, const SolveScalars* sc) {
+  if (sc && solve_done(sc)) return;
+  extern __shared__ float sm[];
+  vcycle_tail_body(td, sm);
 }
 
 }  // namespace otm

