@@ -12,7 +12,8 @@ import re
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB_PATH = os.path.join(HERE, "libopentm_b200.so")
-HEADERS = [os.path.join(ROOT, "include", f) for f in ("opentm_b200.h", "opentm_b200_mma.h", "opentm_b200_server.h")]
+HEADERS = [os.path.join(ROOT, "include", f)
+           for f in ("opentm_b200.h", "opentm_b200_mma.h", "opentm_b200_server.h", "opentm_b200_noalloc.h")]
 
 OTM_OK = 0
 STATUS_NAMES = {
@@ -134,6 +135,8 @@ SIGNATURES = {
     "otm_mma_update": (_S, [_P, ctypes.c_int, _P, _P, _F, ctypes.POINTER(_P)]),
     "otm_mmasub_device": (_S, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P, _P, _P, _P, ctypes.c_double, _P,
                                _P, PitchedPtr, _P, _P, ctypes.c_double, _P, _P, _P, ctypes.c_double, _P]),
+    # allocation-free filter (include/opentm_b200_noalloc.h)
+    "otm_oc_filter_sens_noalloc": (_S, [_P, _P, ctypes.c_size_t, _I3, ctypes.c_float, _P]),
     # serving (include/opentm_b200_server.h)
     "otm_server_config_init": (_S, [ctypes.POINTER(ServerConfig)]),
     "otm_server_create": (_S, [ctypes.POINTER(ServerConfig), _P, ctypes.POINTER(_P)]),

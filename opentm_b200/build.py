@@ -26,6 +26,7 @@ SOURCES = [
     "otm_oc.cu",
     "otm_mma.cu",
     "otm_server.cu",
+    "otm_noalloc.cu",
 ]
 
 
@@ -48,7 +49,7 @@ def _compile(src: str, verbose: bool) -> str:
     obj = os.path.join(BUILD_DIR, os.path.basename(src) + ".o")
     path = os.path.join(CSRC, src)
     deps = [path] + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
-    deps.append(os.path.join(ROOT, "include", "opentm_b200.h"))
+    deps += [os.path.join(ROOT, "include", f) for f in os.listdir(os.path.join(ROOT, "include")) if f.endswith(".h")]
     if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(d) for d in deps):
         return obj
     cmd = [nvcc, *host_compiler(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
