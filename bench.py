@@ -343,26 +343,51 @@ def serve_fields(seed=4, per_reso=4):
 def run_serve(args):
     import torch
 
-    from opentm_b200 import HomoConfig, Homogenization_H, Server, launch_count
+    from opentm_b200 import HomoConfig, Homogenization_H
     from opentm_b200 import workloads as wl
     torch.cuda.set_device(0)
     fields = serve_fields()
-    reqs = wl.serving_requests(args.requests, seed=4, rate=args.rate)
-    # serial plain-FP32 baseline: one handle per request, solved one after another
-    serial = []
-    for (t, n, i) in reqs[: min(len(reqs), 60)]:
-        k = fields[n][i % len(fields[n])]
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        H = Homogenization_H(HomoConfig(reso=n, femRelThres=TOL, pre_smooth=2, post_smooth=2, warm_start=False))
-        H.update(torch.from_numpy(k).cuda())
-        H.heatMatrix()
-        torch.cuda.synchronize()
-        serial.append(time.perf_counter() - t0)
-        H.close()
+    # serial plain-FP32 baseline: one resident handle per resolution, requests solved one after
+    # another from a zero initial guess (H2D of the field, update, 3 load cases, K^H)
+    handles = {n: Homogenization_H(HomoConfig(reso=n, femRelThres=TOL, pre_smooth=2, post_smooth=2,
+                                              warm_start=False)) for n in wl.SERVE_RESOS}
+    kdev = {n: torch.empty((n, n, n), dtype=torch.float32, device="cuda") for n in wl.SERVE_RESOS}
+    for n in wl.SERVE_RESOS:  # warm-up (graph capture)
+        kdev[n].copy_(torch.from_numpy(fields[n][0]))
+        handles[n].update(kdev[n])
+        handles[n].heatMatrix()
+    reqs0 = wl.serving_requests(200, seed=4, rate=args.rate)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for (t, n, i) in reqs0:
+        kdev[n].copy_(torch.from_numpy(fields[n][i % len(fields[n])]))
+        handles[n].update(kdev[n])
+        handles[n].heatMatrix()
+    torch.cuda.synchronize()
+    serial_rate = len(reqs0) / (time.perf_counter() - t0)
+    for h in handles.values():
+        h.close()
+    rates = [args.rate] if args.rate > 0 else [50.0, 200.0, 500.0, 1000.0, 2000.0]
+    results = []
+    for rate in rates:
+        results.append(serve_once(args, fields, rate, serial_rate))
+    line = dict(results[-1])
+    if len(results) > 1:
+        line["sweep"] = [{k: r[k] for k in ("rate", "value", "p50_ms", "p99_ms")} for r in results]
+        best = max(results, key=lambda r: r["value"])
+        line.update({k: best[k] for k in ("value", "p50_ms", "p99_ms", "ms_per_step", "steps", "gpu_launches")})
+        line["config"]["rate"] = best["rate"]
+    line.pop("rate", None)
+    print(json.dumps(line), flush=True)
+
+
+def serve_once(args, fields, rate, serial_rate):
+    from opentm_b200 import Server, launch_count
+    from opentm_b200 import workloads as wl
+    reqs = wl.serving_requests(args.requests, seed=4, rate=rate)
     srv = Server(hbm_budget_bytes=150 * 10 ** 9, max_active=args.max_active, fem_rel_thres=TOL,
                  iters_per_step=args.iters_per_step)
-    # warm-up: a few requests of every size
+    # warm-up: one request of every size
     for n in wl.SERVE_RESOS:
         srv.submit(fields[n][0])
     srv.run_until_idle()
@@ -393,18 +418,18 @@ def run_serve(args):
     makespan = max(done_at.values()) - min(arrival.values())
     lat = np.array([done_at[r] - arrival[r] for r in done_at]) * 1e3
     value = len(done_at) / makespan
-    serial_rate = 1.0 / float(np.mean(serial))
-    line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": 1, "steps": len(done_at),
+    srv.close()
+    return {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": 1, "steps": len(done_at),
             "warmup": len(wl.SERVE_RESOS), "ms_per_step": round(1e3 / value, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"serving stream, {len(reqs)} requests, Poisson {args.rate} req/s, "
+            "config": {"workload": f"serving stream, {len(reqs)} requests, Poisson arrivals, "
                                    f"resolutions {wl.SERVE_RESOS} weights {wl.SERVE_WEIGHTS}",
-                       "rate": args.rate, "max_active": args.max_active, "iters_per_step": args.iters_per_step,
-                       "tol": TOL},
-            "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                       "max_active": args.max_active, "iters_per_step": args.iters_per_step, "tol": TOL,
+                       "budget_bytes": 150 * 10 ** 9},
+            "rate": rate, "p50_ms": round(float(np.percentile(lat, 50)), 3),
+            "p99_ms": round(float(np.percentile(lat, 99)), 3),
             "serial_fp32_solves_per_s": round(serial_rate, 3), "speedup_vs_serial": round(value / serial_rate, 3),
             "gpu_launches": int(launch_count() - l0)}
-    print(json.dumps(line), flush=True)
 
 
 def main():
@@ -418,7 +443,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", default="oc", choices=["oc", "serve"])
     ap.add_argument("--requests", type=int, default=2000)
-    ap.add_argument("--rate", type=float, default=500.0)
+    ap.add_argument("--rate", type=float, default=0.0, help="Poisson rate; 0 sweeps 50..2000 req/s")
     ap.add_argument("--max-active", type=int, default=64)
     ap.add_argument("--iters-per-step", type=int, default=2)
     args = ap.parse_args()

@@ -315,11 +315,11 @@ void Homo::fine_ops16(int what, int color) {
   T* r = (T*)r16;
   const double* fs = sc->fscale;
   switch (what) {
-    case 0:
+    case 0:  // color is a colour pair (0..3) unless face entries are present
       if (face)
         k_gs_fine<true, 3, T, T><<<ceil_div(nv >> 3, kBlock), kBlock, 0, stream>>>(L.d, color, kk, op0, u, L.f, sc, fs);
       else
-        k_gs_fine<false, 3, T, T><<<ceil_div(nv >> 3, kBlock), kBlock, 0, stream>>>(L.d, color, kk, op0, u, L.f, sc, fs);
+        k_gs_fine_pair<3, T, T><<<ceil_div(nv >> 3, kBlock), kBlock, 0, stream>>>(L.d, color, kk, op0, u, L.f, sc, fs);
       break;
     case 1:
       if (face)
@@ -350,8 +350,8 @@ void Homo::gs(int l, int color) {
   if (l == 0) {
     if (face)
       k_gs_fine<true, 3><<<ceil_div(nsub, kBlock), kBlock, 0, stream>>>(L.d, color, ks, op, L.u, L.f, sc);
-    else
-      k_gs_fine<false, 3><<<ceil_div(nsub, kBlock), kBlock, 0, stream>>>(L.d, color, ks, op, L.u, L.f, sc);
+    else  // color is a colour pair (0..3)
+      k_gs_fine_pair<3><<<ceil_div(nsub, kBlock), kBlock, 0, stream>>>(L.d, color, ks, op, L.u, L.f, sc);
   } else {
     k_gs_coarse<3><<<ceil_div(nsub, kBlock), kBlock, 0, stream>>>(L.d, color, L.st, L.u, L.f, sc);
   }
@@ -393,12 +393,14 @@ void Homo::vcycle(int l) {
     cudaMemsetAsync(u16, 0, 3 * nv * 2, stream);
   else
     cudaMemsetAsync(L.u, 0, 3 * nv * sizeof(float), stream);
+  // the fine level of the cube element sweeps colour pairs (4 launches), coarse levels 8 colours
+  const int passes = (l == 0 && !face) ? 4 : 8;
   for (int s = 0; s < cfg.pre_smooth; s++) {
     const bool timed = cfg.profile && l == 0 && s == 0 && prof_slot >= 0;
     // inside a stream capture only an "external" event record becomes a graph node
     const unsigned int evflag = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
     if (timed) cudaEventRecordWithFlags(prof_ev[0][prof_slot], stream, evflag);
-    for (int c = 0; c < 8; c++) gs(l, c);
+    for (int c = 0; c < passes; c++) gs(l, c);
     if (timed) cudaEventRecordWithFlags(prof_ev[1][prof_slot], stream, evflag);
   }
   Level& C = lv[l + 1];
@@ -433,7 +435,7 @@ void Homo::vcycle(int l) {
     launched(1);
   }
   for (int s = 0; s < cfg.post_smooth; s++)
-    for (int c = 7; c >= 0; c--) gs(l, c);
+    for (int c = passes - 1; c >= 0; c--) gs(l, c);
 }
 
 void Homo::iteration(int j) {
@@ -871,7 +873,7 @@ otm_status otm_homo_get_profile(otm_homo* h, otm_profile* prof, int reset) {
   prof->sweeps = H.prof_sweeps;
   prof->sweep_ms = H.prof_ms;
   prof->sweep_bytes = nv * (4.0 + 3.0 * (4.0 + 4.0 + 4.0));
-  prof->launches_per_sweep = 8;
+  prof->launches_per_sweep = H.face ? 8 : 4;
   if (reset) {
     H.prof_sweeps = 0;
     H.prof_ms = 0.0;

@@ -235,6 +235,81 @@ __global__ void __launch_bounds__(kBlock) k_gs_fine(Dims d, int color, const KT*
   gs_fine_body<kFace, NC, KT, VT>(d, color, ks, op, u, f, fscale, size_t(blockIdx.x) * blockDim.x + threadIdx.x);
 }
 
+// Colour-pair pass on the fine level. With c1 == 0 (the cube element has no coupling between
+// vertices one edge apart) colours (cx,cy,0) and (cx,cy,1) are not coupled, so both are
+// updated in one launch: exactly a Gauss-Seidel sweep in the colour order 0,4,1,5,2,6,3,7.
+// Each thread updates the vertical vertex pair (x, y, 2k) and (x, y, 2k+1), whose
+// neighbourhoods share two of their four planes.
+template <int NC, typename KT, typename VT>
+__device__ __forceinline__ void gs_fine_pair_body(const Dims& d, int pair, const KT* __restrict__ ks,
+                                                  const FineOp& op, VT* u, const float* __restrict__ f,
+                                                  const double* fscale, size_t t) {
+  const int hx = d.nx >> 1, hy = d.ny >> 1;
+  const size_t nsub = d.nv() >> 3;
+  if (t >= nsub) return;
+  const int i = int(t % hx), j = int((t / hx) % hy), kq = int(t / (size_t(hx) * hy));
+  const int x = 2 * i + (pair & 1), y = 2 * j + ((pair >> 1) & 1), z = 2 * kq;
+  const size_t nv = d.nv();
+  const int xs[3] = {wrapm(x - 1, d.nx), x, wrapm(x + 1, d.nx)};
+  const int ys[3] = {wrapm(y - 1, d.ny), y, wrapm(y + 1, d.ny)};
+  int zs[4];
+#pragma unroll
+  for (int a = 0; a < 4; a++) zs[a] = wrapm(z - 1 + a, d.nz);  // planes z-1 .. z+2
+  // conductivities of the element planes z-1, z, z+1 (lower corners), 4 per plane
+  float kk[3][4];
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+      const int bx = b & 1, by = b >> 1;
+      kk[a][b] = ld(ks + (size_t(ys[by]) + size_t(d.ny) * zs[a]) * d.nx + xs[bx]);
+    }
+#pragma unroll
+  for (int h = 0; h < 2; h++) {  // h = 0: vertex at plane z (element planes 0,1); h = 1: z+1 (planes 1,2)
+    float k8[8];
+#pragma unroll
+    for (int b = 0; b < 8; b++) k8[b] = kk[h + (b >> 2)][b & 3];
+    const size_t v = (size_t(ys[1]) + size_t(d.ny) * zs[1 + h]) * d.nx + x;
+    float acc[NC];
+#pragma unroll
+    for (int c = 0; c < NC; c++) acc[c] = __ldg(f + c * nv + v) * (fscale ? float(fscale[c]) : 1.f);
+#pragma unroll
+    for (int o = 0; o < 27; o++) {
+      const int ox = o % 3, oy = (o / 3) % 3, oz = o / 9;
+      const int nzc = (ox != 1) + (oy != 1) + (oz != 1);
+      if (nzc < 2) continue;  // self and the zero edge-neighbour entries
+      float coef;
+      switch (o) {
+#define OTM_FC(OO) \
+  case OO:         \
+    coef = fine_coef<OO>(k8, op); \
+    break;
+        OTM_FC(0) OTM_FC(2) OTM_FC(6) OTM_FC(8) OTM_FC(1) OTM_FC(3) OTM_FC(5) OTM_FC(7) OTM_FC(9) OTM_FC(11)
+        OTM_FC(15) OTM_FC(17) OTM_FC(18) OTM_FC(20) OTM_FC(24) OTM_FC(26) OTM_FC(19) OTM_FC(21) OTM_FC(23) OTM_FC(25)
+#undef OTM_FC
+        default: coef = 0.f;
+      }
+      const size_t jn = (size_t(ys[oy]) + size_t(d.ny) * zs[oz + h]) * d.nx + xs[ox];
+#pragma unroll
+      for (int c = 0; c < NC; c++) acc[c] -= coef * ld(u + c * nv + jn);
+    }
+    float ksum8 = 0.f;
+#pragma unroll
+    for (int b = 0; b < 8; b++) ksum8 += k8[b];
+    const float inv = 1.0f / (op.c0 * ksum8);
+#pragma unroll
+    for (int c = 0; c < NC; c++) st(u + c * nv + v, acc[c] * inv);
+  }
+}
+
+template <int NC, typename KT = float, typename VT = float>
+__global__ void __launch_bounds__(kBlock) k_gs_fine_pair(Dims d, int pair, const KT* __restrict__ ks, FineOp op,
+                                                          VT* u, const float* __restrict__ f, const SolveScalars* sc,
+                                                          const double* fscale = nullptr) {
+  if (sc && solve_done(sc)) return;
+  gs_fine_pair_body<NC, KT, VT>(d, pair, ks, op, u, f, fscale, size_t(blockIdx.x) * blockDim.x + threadIdx.x);
+}
+
 // r = f - A u on the fine level for every vertex.
 template <bool kFace, int NC, typename KT, typename VT>
 __device__ __forceinline__ void resid_fine_body(const Dims& d, const KT* __restrict__ ks, const FineOp& op,

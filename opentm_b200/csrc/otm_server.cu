@@ -93,8 +93,8 @@ static __global__ void __launch_bounds__(kBlock) kb_gs(const BTask* __restrict__
                                                        const ReqDesc* __restrict__ R, int color) {
   OTM_TASK_PROLOGUE
   const ReqLevel& L = D.lv[T.level];
-  if (T.level == 0)
-    gs_fine_body<false, 3, float, float>(L.d, color, D.ks, D.op, L.u, L.f, nullptr, tid);
+  if (T.level == 0)  // colour pair on the fine level
+    gs_fine_pair_body<3, float, float>(L.d, color, D.ks, D.op, L.u, L.f, nullptr, tid);
   else
     gs_coarse_body<3>(L.d, color, L.st, L.u, L.f, tid);
 }
@@ -310,6 +310,10 @@ static otm_status admit(otm_server* s, Request& r, int slot) {
       tl = l;
       break;
     }
+  if (H.face) {
+    set_error("serving needs the cube element (no edge-neighbour coupling)");
+    return OTM_ERR_UNSUPPORTED;
+  }
   if (tl < 0 || L > kSrvMaxLevels) {
     set_error("serving needs a cell with at least two multigrid levels");
     return OTM_ERR_UNSUPPORTED;
@@ -421,21 +425,23 @@ static otm_status run_batch(otm_server* s, const std::vector<int>& run_slots, in
   for (int it = 0; it < iters; it++) {
     for (int l = 0; l < Lmax; l++) {
       if (!gs[l].n) continue;
+      const int passes = l == 0 ? 4 : 8;  // colour pairs on the fine level
       kb_zero<<<zero[l].blocks, kBlock, 0, s->stream>>>(T(zero[l]), zero[l].n, R);
       for (int sw = 0; sw < pre; sw++)
-        for (int c = 0; c < 8; c++) kb_gs<<<gs[l].blocks, kBlock, 0, s->stream>>>(T(gs[l]), gs[l].n, R, c);
+        for (int c = 0; c < passes; c++) kb_gs<<<gs[l].blocks, kBlock, 0, s->stream>>>(T(gs[l]), gs[l].n, R, c);
       kb_resid<<<res[l].blocks, kBlock, 0, s->stream>>>(T(res[l]), res[l].n, R);
       kb_restrict<<<rst[l].blocks, kBlock, 0, s->stream>>>(T(rst[l]), rst[l].n, R);
-      launches += 3 + 8 * pre;
+      launches += 3 + passes * pre;
     }
     kb_tail<<<tail.blocks, kTailThreads, tail_smem, s->stream>>>(T(tail), tail.n, R);
     launches++;
     for (int l = Lmax - 1; l >= 0; l--) {
       if (!gs[l].n) continue;
+      const int passes = l == 0 ? 4 : 8;
       kb_prolong<<<pro[l].blocks, kBlock, 0, s->stream>>>(T(pro[l]), pro[l].n, R);
       for (int sw = 0; sw < post; sw++)
-        for (int c = 7; c >= 0; c--) kb_gs<<<gs[l].blocks, kBlock, 0, s->stream>>>(T(gs[l]), gs[l].n, R, c);
-      launches += 1 + 8 * post;
+        for (int c = passes - 1; c >= 0; c--) kb_gs<<<gs[l].blocks, kBlock, 0, s->stream>>>(T(gs[l]), gs[l].n, R, c);
+      launches += 1 + passes * post;
     }
     kb_dot_rz<<<red.blocks, kBlock, 0, s->stream>>>(T(red), red.n, R);
     kb_update_p<<<el0.blocks, kBlock, 0, s->stream>>>(T(el0), el0.n, R);

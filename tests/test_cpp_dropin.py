@@ -49,5 +49,11 @@ def test_dropin_program_matches_python_path(tmp_path):
     # bits, so the two solves agree to the solver tolerance, not bitwise
     assert np.abs(got - want).max() / np.abs(want).max() <= 1e-6
     assert vals["relres"][0] <= 1e-7
-    assert abs(vals["oc_vol"][0] - 0.25) <= 1e-4 + 1e-6
+    # same OC inputs through the oracle: filtered sensitivities, then the 20-step bisection
+    import oracle as ora
+    n3 = n ** 3
+    g = -(0.1 + wl.uniform(0, 2 * n3)[n3:].astype(np.float32)).reshape(n, n, n)
+    s = ora.oc_filter_sens(g, np.full((n, n, n), 0.3), 2.0)
+    want_vol = ora.oc_update(s, np.full((n, n, n), 0.3), 0.25, 0.001, 0.2, 0.5)[0].mean()
+    assert abs(vals["oc_vol"][0] - want_vol) <= 1e-5
     assert abs(vals["mma_mean"][0] - 0.3) <= 2e-3

@@ -42,7 +42,8 @@ def test_server_matches_single_request_path():
     C, _ = _solve_alone(k)
     H = Homogenization_H(HomoConfig(reso=32, femRelThres=1e-6, pre_smooth=2, post_smooth=2, warm_start=False))
     H.update(torch.from_numpy(k).cuda())
-    assert np.array_equal(C, H.heatMatrix())
+    # same algorithm, separately compiled kernels: equal to the solver tolerance
+    assert rel_c(C, H.heatMatrix()) <= 1e-7
 
 
 def test_budget_admission_and_rejection():
