@@ -71,6 +71,8 @@ typedef struct otm_config {
   int use_graphs;        /* capture the iteration loop in a CUDA graph; default 1 */
   int profile;           /* time the first fine-level smoothing sweep of every iteration with CUDA
                             events recorded inside the graph; default 0 */
+  int cluster_cycle;     /* run the levels with <= 32^3 unknowns and the coarsest solve in one
+                            thread-block-cluster launch when they fit; default 1 */
 } otm_config;
 
 typedef struct otm_solve_stats {
@@ -80,12 +82,13 @@ typedef struct otm_solve_stats {
   int status;             /* otm_status of the last solve */
   int levels;             /* multigrid levels */
   int coarsest_reso[3];   /* coarsest level cells per axis */
+  int cluster_level;      /* first level of the one-launch cluster cycle, -1 when not used */
 } otm_solve_stats;
 
 /* Event-timed fine-level smoother sweeps collected while profile != 0. */
 typedef struct otm_profile {
   int sweeps;             /* sweeps timed (iterations that ran) */
-  double sweep_ms;        /* total milliseconds of those sweeps (8 colour launches each) */
+  double sweep_ms;        /* total milliseconds of those sweeps (launches_per_sweep launches each) */
   double sweep_bytes;     /* algorithmic bytes of one sweep: nv * (4 + 3 * (4 + 4 + 4)) in FP32 */
   int launches_per_sweep; /* kernel launches per sweep */
 } otm_profile;

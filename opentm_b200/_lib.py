@@ -50,6 +50,7 @@ class Config(ctypes.Structure):
         ("check_every", ctypes.c_int),
         ("use_graphs", ctypes.c_int),
         ("profile", ctypes.c_int),
+        ("cluster_cycle", ctypes.c_int),
     ]
 
 
@@ -61,6 +62,7 @@ class SolveStats(ctypes.Structure):
         ("status", ctypes.c_int),
         ("levels", ctypes.c_int),
         ("coarsest_reso", ctypes.c_int * 3),
+        ("cluster_level", ctypes.c_int),
     ]
 
 

@@ -72,6 +72,7 @@ otm_status Homo::alloc(void** p, size_t bytes) {
 Homo::~Homo() {
   for (auto& g : graphs)
     if (g.exec) cudaGraphExecDestroy(g.exec);
+  if (loop_exec) cudaGraphExecDestroy(loop_exec);
   if (stream && !external) cudaStreamDestroy(stream);
   if (ev_in) cudaEventDestroy(ev_in);
   if (ev_out) cudaEventDestroy(ev_out);
@@ -196,9 +197,10 @@ otm_status Homo::build(const otm_config& c, cudaStream_t ext_stream, cudaMemPool
   OTM_CUDA(cudaMemsetAsync(flags, 0, 4 * sizeof(int), stream));
   // pinned block: solve scalars, then the level-1 Galerkin table (uploaded from pinned memory
   // so the copy never waits for the stream)
-  OTM_CUDA(cudaMallocHost((void**)&sc_host, sizeof(SolveScalars) + 64 * 27 * sizeof(float)));
+  OTM_CUDA(cudaMallocHost((void**)&sc_host, sizeof(SolveScalars) + 64 * 27 * sizeof(float) + 4 * sizeof(int)));
   std::memset(sc_host, 0, sizeof(SolveScalars));
   float* tab = (float*)(sc_host + 1);
+  flags_host = (int*)(tab + 64 * 27);
   galerkin_level1_table(tm, tab);
   OTM_CUDA(cudaMemcpyAsync(table, tab, 64 * 27 * sizeof(float), cudaMemcpyHostToDevice, stream));
   if (!external) OTM_CUDA(cudaStreamSynchronize(stream));
@@ -214,14 +216,53 @@ otm_status Homo::build(const otm_config& c, cudaStream_t ext_stream, cudaMemPool
     if (t > 0 && t < L - 1 && L - t <= kTailMaxLevels) {
       size_t floats = 0;
       for (int l = t; l < L; l++) floats += 9 * lv[l].d.nv();
-      if (floats * sizeof(float) <= 200 * 1024) {
+      if (floats * sizeof(float) <= size_t(kMaxDynSmem)) {
         tail_l = t;
         tail_smem = floats * sizeof(float);
-        OTM_CUDA(cudaFuncSetAttribute(k_vcycle_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tail_smem)));
+        OTM_CUDA(cudaFuncSetAttribute(k_vcycle_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
       }
     }
   }
+  // levels with <= 32^3 unknowns and the coarsest solve in one thread-block-cluster launch
+  if (cfg.cluster_cycle) {
+    const int L = int(lv.size());
+    int t = -1;
+    for (int l = 1; l < L - 1; l++)
+      if (lv[l].d.nv() <= size_t(kClMaxNv)) {
+        t = l;
+        break;
+      }
+    if (t > 0) {
+      std::vector<Dims> dims;
+      for (int l = t; l < L; l++) dims.push_back(lv[l].d);
+      ClDesc cd{};
+      const size_t bytes = cl_plan(dims.data(), int(dims.size()), &cd);
+      if (bytes > 0 &&
+          cudaFuncSetAttribute(k_vcycle_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem) ==
+              cudaSuccess) {
+        cudaLaunchConfig_t lc{};
+        lc.gridDim = dim3(kCl);
+        lc.blockDim = dim3(kClThreads);
+        lc.dynamicSmemBytes = bytes;
+        int ncl = 0;
+        if (cudaOccupancyMaxActiveClusters(&ncl, (void*)k_vcycle_cluster, &lc) == cudaSuccess && ncl >= 1) {
+          cd.pre = cfg.pre_smooth;
+          cd.post = cfg.post_smooth;
+          for (int i = 0; i < cd.nlev; i++) {
+            cd.lv[i].st = lv[t + i].st;
+            cd.lv[i].rg = lv[t + i].r;
+          }
+          cd.Ainv = Ainv;
+          cl_desc = cd;
+          cluster_l = t;
+          cluster_smem = bytes;
+        }
+      }
+      cudaGetLastError();  // a refused attribute or occupancy query leaves no error behind
+    }
+  }
   stats.levels = int(lv.size());
+  stats.cluster_level = cluster_l;
   stats.coarsest_reso[0] = lv.back().d.nx;
   stats.coarsest_reso[1] = lv.back().d.ny;
   stats.coarsest_reso[2] = lv.back().d.nz;
@@ -288,9 +329,9 @@ otm_status Homo::update(const float* kin, int pitchT) {
   }
   {
     const size_t abytes = size_t(nc) * nc * sizeof(double);
-    const int use_smem = abytes <= 200 * 1024;
+    const int use_smem = abytes <= size_t(kMaxDynSmem);
     if (use_smem)
-      OTM_CUDA(cudaFuncSetAttribute(k_coarsest_build, cudaFuncAttributeMaxDynamicSharedMemorySize, int(abytes)));
+      OTM_CUDA(cudaFuncSetAttribute(k_coarsest_build, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
     k_coarsest_build<<<1, 1024, use_smem ? abytes : 0, stream>>>(lv.back().d, lv.back().st, Ainv, flags + 1,
                                                                   use_smem);
   }
@@ -361,6 +402,14 @@ void Homo::gs(int l, int color) {
 void Homo::vcycle(int l) {
   Level& L = lv[l];
   const size_t nv = L.d.nv();
+  if (l == cluster_l) {
+    ClDesc cd = cl_desc;
+    cd.f_in = L.f;
+    cd.u_out = L.u;
+    k_vcycle_cluster<<<kCl, kClThreads, cluster_smem, stream>>>(cd, sc);
+    launched(1);
+    return;
+  }
   if (l == tail_l) {
     TailDesc td{};
     td.nlev = int(lv.size()) - l;
@@ -541,71 +590,172 @@ void Homo::launch_heat_matrix() {
 
 // Solve the 3 load cases to the tolerance (MG_H::solveEquation, homogenization/MG.cpp:80-142;
 // per-case warm start from the previous solution, homogenization/homogenization.cu:182-188).
-otm_status Homo::solve_impl() {
-  const Dims d0 = lv[0].d;
-  const size_t nv = d0.nv();
-  const int nb = reduce_blocks(nv);
-  // import / coarsest status from update()
-  int fl[2] = {0, 0};
-  OTM_CUDA(cudaMemcpyAsync(fl, flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream));
-  OTM_CUDA(cudaStreamSynchronize(stream));
-  if (fl[0]) {
+// Import / coarsest status written by update() (pinned copy in flags_host).
+otm_status Homo::check_flags() {
+  if (flags_host[0]) {
     set_error("conductivity field holds a negative, NaN or Inf value");
     return OTM_ERR_NAN;
   }
-  if (fl[1]) {
+  if (flags_host[1]) {
     set_error("coarsest-level matrix is not positive definite");
     return OTM_ERR_NAN;
+  }
+  return OTM_OK;
+}
+
+// The whole iteration loop as one graph: k_loop_start, then a conditional "while" node whose
+// body is one iteration followed by k_loop_ctrl, so a solve needs no host round trip until it
+// has finished. Built on first use (and again when the solver type changes).
+otm_status Homo::launch_loop() {
+  if (!loop_exec || loop_solver != cfg.solver) {
+    if (loop_exec) cudaGraphExecDestroy(loop_exec);
+    loop_exec = nullptr;
+    cudaGraph_t g = nullptr;
+    OTM_CUDA(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle h{};
+    cudaGraphNode_t n0{}, n1{};
+    cudaGraphNodeParams cp{};
+    cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+    if (e == cudaSuccess) {
+      void* args0[] = {&sc, &h};
+      cudaKernelNodeParams kp{};
+      kp.func = (void*)k_loop_start;
+      kp.gridDim = dim3(1);
+      kp.blockDim = dim3(1);
+      kp.sharedMemBytes = 0;
+      kp.kernelParams = args0;
+      kp.extra = nullptr;
+      e = cudaGraphAddKernelNode(&n0, g, nullptr, 0, &kp);
+    }
+    if (e == cudaSuccess) {
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = h;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      e = cudaGraphAddNode(&n1, g, &n0, 1, &cp);
+    }
+    if (e == cudaSuccess) {
+      cudaGraph_t body = cp.conditional.phGraph_out[0];
+      e = cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+      if (e == cudaSuccess) {
+        capturing = true;
+        iteration(0);
+        k_loop_ctrl<<<1, 1, 0, stream>>>(sc, h, cfg.max_iter + 1);
+        capturing = false;
+        cudaGraph_t out = nullptr;
+        e = cudaStreamEndCapture(stream, &out);
+      }
+      if (e == cudaSuccess) {
+        size_t nn = 0;
+        cudaGraphGetNodes(body, nullptr, &nn);
+        std::vector<cudaGraphNode_t> nodes(nn);
+        cudaGraphGetNodes(body, nodes.data(), &nn);
+        loop_body_kernels = 0;
+        for (auto& nd : nodes) {
+          cudaGraphNodeType t;
+          if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) loop_body_kernels++;
+        }
+      }
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&loop_exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      loop_exec = nullptr;
+      return cuda_fail(e, "building the solve-loop graph");
+    }
+    loop_solver = cfg.solver;
+  }
+  OTM_CUDA(cudaGraphLaunch(loop_exec, stream));
+  return OTM_OK;
+}
+
+// Right-hand sides, projection, initial residual (all solver forms).
+void Homo::launch_solve_start() {
+  const Dims d0 = lv[0].d;
+  const size_t nv = d0.nv();
+  const int nb = reduce_blocks(nv);
+  k_rhs<<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(d0, ks, ef, b);
+  // project RHS and initial guess off the constants
+  k_sums2<<<nb, kBlock, 0, stream>>>(nv, b, x, partials, means, &sc->counter[T_MEAN]);
+  k_sub_means<<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(nv, b, x, means);
+  sc_host->tol = cfg.fem_rel_thres;
+  cudaMemcpyAsync(&sc->tol, &sc_host->tol, sizeof(double), cudaMemcpyHostToDevice, stream);
+  if (mixed) {
+    const unsigned int* kmax_bits = (const unsigned int*)(flags + 2);
+    if (face)
+      k_resid64<true><<<nb, kBlock, 0, stream>>>(d0, ks, op, x64, b, lv[0].f, partials, sc, kmax_bits, cfg.max_iter,
+                                                 1);
+    else
+      k_resid64<false><<<nb, kBlock, 0, stream>>>(d0, ks, op, x64, b, lv[0].f, partials, sc, kmax_bits,
+                                                  cfg.max_iter, 1);
+  } else if (face) {
+    k_init_residual<true><<<nb, kBlock, 0, stream>>>(d0, ks, op, x, b, lv[0].f, partials, sc);
+  } else {
+    k_init_residual<false><<<nb, kBlock, 0, stream>>>(d0, ks, op, x, b, lv[0].f, partials, sc);
+  }
+  launched(4);
+}
+
+// Solve the 3 load cases to the tolerance (MG_H::solveEquation, homogenization/MG.cpp:80-142;
+// iterations PCG or stationary V-cycles). With graphs and without profiling the iteration loop
+// runs on the device (launch_loop) and the host waits once; with with_heat the K^H reduction
+// is queued before that wait (heat_ready tells the caller).
+otm_status Homo::solve_impl(bool with_heat) {
+  const Dims d0 = lv[0].d;
+  const size_t nv = d0.nv();
+  const bool device_loop = cfg.use_graphs && !cfg.profile;
+  heat_ready = false;
+  if (!device_loop) {
+    OTM_CUDA(cudaMemcpyAsync(flags_host, flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    OTM_CUDA(cudaStreamSynchronize(stream));
+    OTM_TRY(check_flags());
   }
   for (int attempt = 0; attempt < 2; attempt++) {
     if (!cfg.warm_start || attempt > 0) {
       OTM_CUDA(cudaMemsetAsync(x, 0, 3 * nv * sizeof(float), stream));
       if (mixed) OTM_CUDA(cudaMemsetAsync(x64, 0, 3 * nv * sizeof(double), stream));
     }
-    k_rhs<<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(d0, ks, ef, b);
-    // project RHS and initial guess off the constants
-    k_sums2<<<nb, kBlock, 0, stream>>>(nv, b, x, partials, means, &sc->counter[T_MEAN]);
-    k_sub_means<<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(nv, b, x, means);
-    sc_host->tol = cfg.fem_rel_thres;
-    OTM_CUDA(cudaMemcpyAsync(&sc->tol, &sc_host->tol, sizeof(double), cudaMemcpyHostToDevice, stream));
-    if (mixed) {
-      const unsigned int* kmax_bits = (const unsigned int*)(flags + 2);
-      if (face)
-        k_resid64<true><<<nb, kBlock, 0, stream>>>(d0, ks, op, x64, b, lv[0].f, partials, sc, kmax_bits,
-                                                   cfg.max_iter, 1);
-      else
-        k_resid64<false><<<nb, kBlock, 0, stream>>>(d0, ks, op, x64, b, lv[0].f, partials, sc, kmax_bits,
-                                                    cfg.max_iter, 1);
-    } else if (face) {
-      k_init_residual<true><<<nb, kBlock, 0, stream>>>(d0, ks, op, x, b, lv[0].f, partials, sc);
-    } else {
-      k_init_residual<false><<<nb, kBlock, 0, stream>>>(d0, ks, op, x, b, lv[0].f, partials, sc);
-    }
+    launch_solve_start();
     OTM_CHECK_LAUNCH("solve init");
-    launched(4);
-    int nlaunched = 0, iter_before = 0;
-    bool first_check = true;
-    while (true) {
+    if (device_loop) {
+      OTM_TRY(launch_loop());
+      if (mixed) {
+        k_x64_to_x<<<ceil_div(3 * nv, kBlock), kBlock, 0, stream>>>(3 * nv, x64, x);
+        launched(1);
+      }
+      if (with_heat) launch_heat_matrix();
+      OTM_CHECK_LAUNCH("solve");
+      OTM_CUDA(cudaMemcpyAsync(flags_host, flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream));
       OTM_CUDA(cudaMemcpyAsync(sc_host, sc, sizeof(SolveScalars), cudaMemcpyDeviceToHost, stream));
       OTM_CUDA(cudaStreamSynchronize(stream));
-      if (cfg.profile && !first_check) {
-        const int ran = sc_host->iter - iter_before;
-        for (int j = 0; j < ran && j < kMaxChunk; j++) {
-          float ms = 0.f;
-          if (cudaEventElapsedTime(&ms, prof_ev[0][j], prof_ev[1][j]) == cudaSuccess) {
-            prof_ms += ms;
-            prof_sweeps++;
-          } else {
-            cudaGetLastError();  // a failed query must not surface at the next launch check
+      OTM_TRY(check_flags());
+      count_launches(1 + loop_body_kernels * uint64_t(sc_host->loop));
+      heat_ready = with_heat;
+    } else {
+      int nlaunched = 0, iter_before = 0;
+      bool first_check = true;
+      while (true) {
+        OTM_CUDA(cudaMemcpyAsync(sc_host, sc, sizeof(SolveScalars), cudaMemcpyDeviceToHost, stream));
+        OTM_CUDA(cudaStreamSynchronize(stream));
+        if (cfg.profile && !first_check) {
+          const int ran = sc_host->iter - iter_before;
+          for (int j = 0; j < ran && j < kMaxChunk; j++) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, prof_ev[0][j], prof_ev[1][j]) == cudaSuccess) {
+              prof_ms += ms;
+              prof_sweeps++;
+            } else {
+              cudaGetLastError();  // a failed query must not surface at the next launch check
+            }
           }
         }
+        first_check = false;
+        iter_before = sc_host->iter;
+        if (sc_host->done || nlaunched >= cfg.max_iter) break;
+        const int chunk = std::min(cfg.check_every, cfg.max_iter - nlaunched);
+        OTM_TRY(run_chunk(chunk));
+        nlaunched += chunk;
       }
-      first_check = false;
-      iter_before = sc_host->iter;
-      if (sc_host->done || nlaunched >= cfg.max_iter) break;
-      const int chunk = std::min(cfg.check_every, cfg.max_iter - nlaunched);
-      OTM_TRY(run_chunk(chunk));
-      nlaunched += chunk;
     }
     stats.iterations = sc_host->iter;
     stats.refinements = mixed ? sc_host->iter : 0;
@@ -625,7 +775,7 @@ otm_status Homo::solve_impl() {
   }
   stats.status = st;
   solved = (st == OTM_OK || st == OTM_ERR_NOT_CONVERGED);
-  if (mixed) {
+  if (mixed && !device_loop) {
     // FP32 copy of the FP64 solution for K^H, sensitivity and the solution accessors
     k_x64_to_x<<<ceil_div(3 * nv, kBlock), kBlock, 0, stream>>>(3 * nv, x64, x);
     launched(1);
@@ -648,20 +798,29 @@ otm_status Homo::solve(otm_solve_stats* out) {
 otm_status Homo::heat_matrix(double C[9], bool do_solve) {
   if (!C) return invalid("C is NULL");
   otm_status st = OTM_OK;
-  if (do_solve) {
-    st = solve(nullptr);
-    if (st != OTM_OK && st != OTM_ERR_NOT_CONVERGED) return st;
-  } else if (!solved) {
+  if (do_solve && !updated) {
+    set_error("update() must be called before solving");
+    return OTM_ERR_STATE;
+  }
+  if (!do_solve && !solved) {
     set_error("no solution available");
     return OTM_ERR_STATE;
   }
   OTM_TRY(enter());
-  const Dims d0 = lv[0].d;
-  k_heat_matrix<<<reduce_blocks(d0.nv()), kBlock, 0, stream>>>(d0, ks, x, op, ef, partials, sc);
-  OTM_CHECK_LAUNCH("k_heat_matrix");
-  launched(1);
-  OTM_CUDA(cudaMemcpyAsync(sc_host->kh, sc->kh, 6 * sizeof(double), cudaMemcpyDeviceToHost, stream));
-  OTM_CUDA(cudaStreamSynchronize(stream));
+  heat_ready = false;
+  if (do_solve) {
+    st = solve_impl(true);
+    if (st != OTM_OK && st != OTM_ERR_NOT_CONVERGED) {
+      leave();
+      return st;
+    }
+  }
+  if (!heat_ready) {
+    launch_heat_matrix();
+    OTM_CHECK_LAUNCH("k_heat_matrix");
+    OTM_CUDA(cudaMemcpyAsync(sc_host->kh, sc->kh, 6 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    OTM_CUDA(cudaStreamSynchronize(stream));
+  }
   int cnt = 0;
   for (int a = 0; a < 3; a++)
     for (int bq = a; bq < 3; bq++) {
@@ -761,6 +920,7 @@ otm_status otm_config_init(otm_config* cfg) {
   cfg->check_every = 4;
   cfg->use_graphs = 1;
   cfg->profile = 0;
+  cfg->cluster_cycle = 1;
   return OTM_OK;
 }
 

@@ -7,6 +7,7 @@
 
 #include "otm_mg_kernels.cuh"
 #include "otm_solver_kernels.cuh"
+#include "otm_cluster.cuh"
 #include "otm_tail.cuh"
 #include "otm_template.h"
 
@@ -55,6 +56,9 @@ struct Homo {
   float* p = nullptr;
   float* q = nullptr;
   double* Ainv = nullptr;
+  int cluster_l = -1;       // first level handled by the cluster kernel (-1: none)
+  size_t cluster_smem = 0;  // its dynamic shared memory per CTA
+  ClDesc cl_desc{};         // its level layout (pointers filled per launch)
   int tail_l = -1;          // first level handled by the single-CTA tail kernel (-1: none)
   size_t tail_smem = 0;     // its dynamic shared memory
   int nc = 0;
@@ -70,6 +74,12 @@ struct Homo {
   std::vector<void*> allocations;
   size_t bytes_allocated = 0;
   std::vector<ChunkGraph> graphs;
+  // the whole iteration loop as one graph (conditional while node), used without profiling
+  cudaGraphExec_t loop_exec = nullptr;
+  int loop_solver = -1;
+  uint64_t loop_body_kernels = 0;
+  int* flags_host = nullptr;  // pinned copy of flags[0..1]
+  bool heat_ready = false;    // K^H of the last solve_impl(true) is already in sc_host->kh
   bool capturing = false;
   // profiling: events around the first fine-level sweep of iteration j of a chunk
   cudaEvent_t prof_ev[2][kMaxChunk] = {};
@@ -98,7 +108,10 @@ struct Homo {
     if (!capturing) count_launches(n);
   }
   otm_status run_chunk(int iters);
-  otm_status solve_impl();
+  otm_status launch_loop();
+  otm_status check_flags();
+  void launch_solve_start();
+  otm_status solve_impl(bool with_heat = false);
   otm_status solve(otm_solve_stats* out);
   otm_status heat_matrix(double C[9], bool do_solve);
   otm_status sensitivity(const float dC[9], float* sens, int pitchT, int lexi);

@@ -44,7 +44,13 @@ struct SolveScalars {
   // mixed precision: f is read as alpha_c * f by the inner cycle, x64 += xscale_c * u
   double fscale[3];
   double xscale[3];
+  int loop;  // bodies run by the device-side solve loop of the current solve
 };
+
+// Dynamic shared memory limit every large-shared-memory kernel is opted in to. It is one fixed
+// value (the attribute is per function, not per launch), so handles of different sizes never
+// lower each other's limit; every plan that uses dynamic shared memory stays below it.
+constexpr int kMaxDynSmem = 200 * 1024;
 
 enum Ticket { T_RZ = 0, T_PQ = 1, T_RR = 2, T_KH = 3, T_MEAN = 4, T_INIT = 5, T_RES = 6 };
 

@@ -23,15 +23,21 @@ struct OcState {
 
 constexpr int kOcSteps = 20;  // OCOptimizer.cu:69
 
-__device__ __forceinline__ float oc_new_rho(float s, float r, float g, float min_rho, float step, float damp) {
-  float B = -s / g;
-  if (B < 0.f) B = 0.01f;
-  float nr = (damp == 0.5f ? sqrtf(B) : powf(B, damp)) * r;
+// Move limit and box bounds of the OC update, in the reference's order.
+__device__ __forceinline__ float oc_clamp(float nr, float r, float min_rho, float step) {
   if (nr - r < -step) nr = r - step;
   if (nr - r > step) nr = r + step;
   if (nr < min_rho) nr = min_rho;
   if (nr > 1.f) nr = 1.f;
   return nr;
+}
+
+// rho_new = clamp(r * (-s/g)^damp) (optimization/OCOptimizer.cu:12-39), FP32 as the reference.
+__device__ __forceinline__ float oc_new_rho(float s, float r, float g, float min_rho, float step, float damp) {
+  float B = -s / g;
+  if (B < 0.f) B = 0.01f;
+  const float nr = (damp == 0.5f ? sqrtf(B) : powf(B, damp)) * r;
+  return oc_clamp(nr, r, min_rho, step);
 }
 
 __global__ void __launch_bounds__(kBlock) k_oc_maxabs(int ne, const float* __restrict__ sens, double* partials,
@@ -98,8 +104,17 @@ __global__ void __launch_bounds__(kBlock) k_oc_tree_pass(int ne, const float* __
                                                          float step, float damp, double* partials, OcState* st) {
   if (*((volatile int*)&st->done)) return;
   __shared__ float g[kTreeNodes];
+  __shared__ float cf[kTreeNodes];
   __shared__ float wsum[kBlock / 32][kTreeNodes];
   if (threadIdx.x == 0) oc_tree(float(st->gmin), float(st->gmax), g);
+  __syncthreads();
+  // (-s/g)^damp = (-s)^damp * g^-damp for s < 0: the candidate factor g^-damp is computed once
+  // per block and the element factor once per element, so a candidate costs one multiply and
+  // the clamps instead of a division and a square root. The volumes only steer the bisection;
+  // the new densities themselves (k_oc_apply) use the reference's expression.
+  if (threadIdx.x < kTreeNodes)
+    cf[threadIdx.x] = damp == 0.5f ? float(1.0 / sqrt(double(g[threadIdx.x])))
+                                    : float(pow(double(g[threadIdx.x]), -double(damp)));
   __syncthreads();
   // per-thread FP32 partial volumes of the 31 candidates (a few elements per thread)
   float v[kTreeNodes];
@@ -107,8 +122,15 @@ __global__ void __launch_bounds__(kBlock) k_oc_tree_pass(int ne, const float* __
   for (int t = 0; t < kTreeNodes; t++) v[t] = 0.f;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ne; i += gridDim.x * blockDim.x) {
     const float s = __ldg(sens + i), r = __ldg(rho + i);
+    if (s < 0.f) {
+      const float a = (damp == 0.5f ? sqrtf(-s) : powf(-s, damp)) * r;
 #pragma unroll
-    for (int t = 0; t < kTreeNodes; t++) v[t] += oc_new_rho(s, r, g[t], min_rho, step, damp);
+      for (int t = 0; t < kTreeNodes; t++) v[t] += oc_clamp(a * cf[t], r, min_rho, step);
+    } else {  // -s/g <= 0 (or NaN): the same value for every candidate
+      const float nr = oc_new_rho(s, r, g[0], min_rho, step, damp);
+#pragma unroll
+      for (int t = 0; t < kTreeNodes; t++) v[t] += nr;
+    }
   }
 #pragma unroll
   for (int t = 0; t < kTreeNodes; t++)

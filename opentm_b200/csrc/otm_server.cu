@@ -417,7 +417,7 @@ static otm_status run_batch(otm_server* s, const std::vector<int>& run_slots, in
     OTM_CUDA(cudaMallocAsync((void**)&s->d_tasks, s->task_cap * sizeof(BTask), s->stream));
   }
   OTM_CUDA(cudaMemcpyAsync(s->d_tasks, tasks.data(), tasks.size() * sizeof(BTask), cudaMemcpyHostToDevice, s->stream));
-  OTM_CUDA(cudaFuncSetAttribute(kb_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, int(tail_smem)));
+  OTM_CUDA(cudaFuncSetAttribute(kb_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
   const ReqDesc* R = s->d_desc;
   const int pre = s->cfg.pre_smooth, post = s->cfg.pre_smooth;
   auto T = [&](const Segment& sg) { return s->d_tasks + sg.off; };

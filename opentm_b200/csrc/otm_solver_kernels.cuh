@@ -548,6 +548,22 @@ static __global__ void k_x_to_x64(size_t n, const float* __restrict__ x, double*
 }
 
 // ---------------------------------------------------------------------------------------
+// Device-side solve loop: a CUDA graph "while" node runs one iteration per body until the
+// solve is done, diverged, or `cap` bodies have run (the cap bounds the loop even if no
+// kernel ever sets done).
+// ---------------------------------------------------------------------------------------
+static __global__ void k_loop_start(SolveScalars* sc, cudaGraphConditionalHandle h) {
+  sc->loop = 0;
+  cudaGraphSetConditional(h, (sc->done || sc->nan) ? 0u : 1u);
+}
+
+static __global__ void k_loop_ctrl(SolveScalars* sc, cudaGraphConditionalHandle h, int cap) {
+  const int l = sc->loop + 1;
+  sc->loop = l;
+  cudaGraphSetConditional(h, (!sc->done && !sc->nan && l < cap) ? 1u : 0u);
+}
+
+// ---------------------------------------------------------------------------------------
 // Coarsest level: dense FP64 inverse of A_c + (alpha/n) 1 1^T (SPD on the periodic
 // nullspace), built once per update; each V-cycle applies it as a mat-vec. Replaces the
 // host BiCGSTAB(ILUT) + nullspace projection of Grid_H::solveHostEquation
@@ -555,7 +571,8 @@ static __global__ void k_x_to_x64(size_t n, const float* __restrict__ x, double*
 // ---------------------------------------------------------------------------------------
 // With use_smem the matrix is assembled and inverted in dynamic shared memory (n^2 doubles)
 // and copied to Aout at the end; otherwise it is worked on in place in Aout.
-static __global__ void k_coarsest_build(Dims d, const float* __restrict__ st, double* Aout, int* status,
+constexpr int kGjRegs = 4;  // matrix elements per thread of the register-buffered elimination
+static __global__ void __launch_bounds__(1024) k_coarsest_build(Dims d, const float* __restrict__ st, double* Aout, int* status,
                                         int use_smem) {
   extern __shared__ double smA[];
   const int n = int(d.nv());
@@ -586,6 +603,48 @@ static __global__ void k_coarsest_build(Dims d, const float* __restrict__ st, do
   for (size_t i = threadIdx.x; i < size_t(n) * n; i += blockDim.x) A[i] += alpha;
   __syncthreads();
   // in-place Gauss-Jordan inversion without pivoting (SPD)
+  const int nn = n * n;  // n <= 1024
+  if (nn <= kGjRegs * int(blockDim.x)) {
+    // small systems: every element of step k is computed from the step's old values into
+    // registers, then written back (two barriers per pivot instead of four)
+    double nw[kGjRegs];
+    int ei[kGjRegs], ej[kGjRegs];  // (row, column) of the thread's elements, fixed over the pivots
+#pragma unroll
+    for (int e = 0; e < kGjRegs; e++) {
+      const int idx = int(threadIdx.x) + e * int(blockDim.x);
+      ei[e] = idx / n;
+      ej[e] = idx - ei[e] * n;
+    }
+    for (int k = 0; k < n; k++) {
+      const double pv = A[k * n + k];
+      if (threadIdx.x == 0 && !(pv > 0.0)) *status = 1;
+      const double pinv = 1.0 / pv;
+#pragma unroll
+      for (int e = 0; e < kGjRegs; e++) {
+        const int idx = int(threadIdx.x) + e * int(blockDim.x);
+        if (idx < nn) {
+          const int i = ei[e], j = ej[e];
+          const double a = A[idx];
+          if (i == k)
+            nw[e] = j == k ? pinv : a * pinv;
+          else if (j == k)
+            nw[e] = a * -pinv;
+          else
+            nw[e] = a - A[i * n + k] * (A[k * n + j] * pinv);
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int e = 0; e < kGjRegs; e++) {
+        const int idx = int(threadIdx.x) + e * int(blockDim.x);
+        if (idx < nn) A[idx] = nw[e];
+      }
+      __syncthreads();
+    }
+    if (use_smem)
+      for (int i = threadIdx.x; i < nn; i += blockDim.x) Aout[i] = A[i];
+    return;
+  }
   __shared__ double piv_inv;
   for (int k = 0; k < n; k++) {
     if (threadIdx.x == 0) {

@@ -228,3 +228,19 @@ def test_mixed_precision_warm_start_and_reset():
     C2 = H.heatMatrix()
     assert H.stats().iterations == cold
     assert rel_c(C2, C) <= KH_TOL
+
+
+@pytest.mark.parametrize("shape", [(32, 32, 32), (64, 64, 64), (48, 48, 48), (48, 32, 64)])
+def test_cluster_cycle_matches_per_level_kernels(shape):
+    """The lower levels run as one thread-block-cluster launch (distributed shared memory,
+    cluster barriers); the result equals the per-level kernels' and meets the oracle gates."""
+    nz, ny, nx = shape
+    k, _ = random_k(shape, seed=40 + nx + ny + nz)
+    H1, C1, E1, s1 = gpu_run(k, tol=1e-7, cluster_cycle=True)
+    H2, C2, E2, s2 = gpu_run(k, tol=1e-7, cluster_cycle=False)
+    assert H1.stats().cluster_level >= 1 and H2.stats().cluster_level == -1
+    assert rel_c(C1, C2) <= 1e-6
+    assert abs(H1.stats().iterations - H2.stats().iterations) <= 1
+    mx, l2 = rel_field(s1, s2)
+    assert mx <= SENS_TOL and l2 <= SENS_TOL
+    check_against_oracle(k, C1, E1, s1)
