@@ -2,14 +2,16 @@
 //
 // The levels with at most kClMaxNv unknowns, down to and including the coarsest direct solve,
 // run in kCl CTAs of one cluster. Every level is split into slabs of z-planes, one slab per
-// CTA; each CTA keeps u and f of its planes (and r and the 27-point stencils of every level
-// but the first) in its own shared memory. Values on a neighbouring CTA's planes are read
-// through distributed shared memory, and the phases (colour passes, residual, restriction,
-// coarsest solve, prolongation) are separated by cluster barriers instead of kernel
-// boundaries, so the whole lower cycle costs one launch. The first level's stencils and
-// residual stay in global memory (L2-resident). The arithmetic and its order are those of the
-// per-level kernels in otm_mg_kernels.cuh; the coarsest solve is u = Ainv (f - mean f) as in
-// k_coarsest_solve.
+// CTA; each CTA keeps u of its planes plus ghost copies of the two neighbouring planes, and f,
+// r and the 27-point stencils of its planes (the first level's stencils, right-hand side and
+// residual stay in global memory, L2-resident), in its own shared memory. A CTA that writes
+// an edge plane of u also stores the values into its neighbours' ghost copies (distributed
+// shared memory), so colour passes and residuals read only local shared memory; restriction,
+// prolongation and the coarsest gather read other CTAs' planes directly. The phases are
+// separated by cluster barriers (barrier.cluster arrive/wait, release/acquire) instead of
+// kernel boundaries, so the whole lower cycle costs one launch. The arithmetic is that of the
+// per-level kernels in otm_mg_kernels.cuh except for the summation order of the 27-point
+// products; the coarsest solve is u = Ainv (f - mean f) as in k_coarsest_solve.
 #pragma once
 
 #include <cooperative_groups.h>
@@ -24,16 +26,23 @@ constexpr int kCl = 8;             // CTAs per cluster (portable cluster size)
 constexpr int kClThreads = 512;
 constexpr int kClMaxLevels = 8;
 constexpr int kClMaxNv = 32768;    // unknowns of the first level handled by the cluster (32^3)
-constexpr int kClMaxTab = 2048;    // plane-ownership entries over all levels
+constexpr int kClMaxTab = 6144;    // plane-table entries over all levels (3 per plane)
 
 struct ClLevel {
   Dims d;
-  int cs;      // case stride in shared memory: (planes of the fullest slab) * nx * ny
+  int cs;      // case stride of f and r in shared memory: (planes of the fullest slab) * nx * ny
+  int urs;     // u row stride (nx, padded against shared-memory bank conflicts)
+  int ups;     // u plane stride (ny * urs, padded)
+  int ucs;     // u case stride: two more planes (ghost copies of the neighbouring slabs' edge planes)
   int u_off;   // float offsets in shared memory
-  int f_off;
+  int f_off;   // < 0: right-hand side read from f_in (global; first level only)
   int r_off;   // < 0: residual in rg (global, lexicographic, case-major)
-  int st_off;  // < 0: stencils read from st (global, colour-blocked)
-  int tab_off; // first plane-ownership entry of this level
+  int st_off;  // < 0: stencils read from st (global, colour-blocked); else [vertex][27]
+  int inv_off; // inverse diagonal per own vertex (with st_off >= 0)
+  int tab_off; // plane tables of this level: nz ownership entries, then 2 nz ghost-push entries
+  int tw_res;  // log2 of the lanes that share one vertex's 27 products in the residual
+  int lhx, lhy;  // log2 of nx/2, ny/2 rounded up to powers of two (colour-pass enumeration)
+  int lnx, lny;  // log2 of nx, ny rounded up (residual enumeration)
   int zstart[kCl + 1];  // CTA c holds planes [zstart[c], zstart[c+1])
   const float* st;
   float* rg;
@@ -44,121 +53,190 @@ struct ClDesc {
   int pre, post;
   int nc;          // unknowns of the coarsest level
   int gather_off;  // float offset of the coarsest right-hand-side gather buffer (3 nc floats)
-  int tab_base;    // float offset of the plane-ownership table (ints)
+  int tab_base;    // float offset of the plane tables (ints)
   ClLevel lv[kClMaxLevels];
   const float* f_in;  // right-hand side of the first level (global, case-major)
   float* u_out;       // its correction (global)
   const double* Ainv;
 };
 
-// Plane z of the vector at `off` of level L, wherever it lives in the cluster (case 0; case c
-// is at + c * L.cs). tab entries are (rank << 16) | local plane.
-__device__ __forceinline__ const float* cl_plane(const ClLevel& L, const int* tab, float* const* rb, int off,
-                                                 int z) {
+// Layout of u on a CTA that holds planes [z0, z1): local plane 0 is a copy of plane z0 - 1,
+// planes 1..z1-z0 are its own, plane z1-z0+1 a copy of plane z1 (periodic). A CTA that writes
+// an edge plane also writes the value into the copies held by its neighbours ("ghost push"),
+// so every read of a colour pass or residual is a local shared-memory load.
+
+// Plane z of f or r (in-plane stride nx) at `off` of level L, wherever it lives in the cluster
+// (case 0; case c is at + c * L.cs).
+__device__ __forceinline__ const float* cl_plane(const ClLevel& L, const int* tab, float* const* rb, int off, int z) {
   const int e = tab[L.tab_off + z];
   return rb[e >> 16] + off + (e & 0xffff) * (L.d.nx * L.d.ny);
 }
 
-// One Gauss-Seidel colour pass over this CTA's vertices of the colour (gs_coarse_body);
-// kSmemSt: the level's stencils are in shared memory (local layout [o][cs]).
-template <bool kSmemSt>
-__device__ __forceinline__ void cl_gs_t(const ClLevel& L, float* sm, const int* tab, float* const* rb, int rank,
-                                        int color) {
+// Plane z of u (row stride urs; own planes start at local plane 1; case c at + c * L.ucs).
+__device__ __forceinline__ const float* cl_uplane(const ClLevel& L, const int* tab, float* const* rb, int z) {
+  const int e = tab[L.tab_off + z];
+  return rb[e >> 16] + L.u_off + ((e & 0xffff) + 1) * L.ups;
+}
+
+// Writes value v of case c at (plane z, in-plane u index p) into every ghost copy of plane z.
+__device__ __forceinline__ void cl_push(const ClLevel& L, const int* tab, float* const* rb, int z, int p, int c,
+                                        float v) {
+#pragma unroll
+  for (int k = 0; k < 2; k++) {
+    const int e = tab[L.tab_off + L.d.nz + 2 * z + k];
+    if (e >= 0) rb[e >> 16][L.u_off + c * L.ucs + (e & 0xffff) * L.ups + p] = v;
+  }
+}
+
+// 27-point products of one vertex shared by a team of kTw lanes of one warp: lane k of the
+// team takes the offsets k, k + kTw, ... and the team sums with butterfly shuffles, so small
+// levels (a few dozen vertices per CTA) keep the latency of one vertex short. pu[0..2] are the
+// local u planes z-1, z, z+1. Returns sum_o A(v, v+o) u(v+o) over the selected offsets in
+// every lane of the team.
+template <bool kSmemSt, bool kSkipCentre, int kTw>
+__device__ __forceinline__ void cl_apply_team(const float* sp, size_t sstride, const float* const (&pu)[3], int xm,
+                                              int x, int xp, int ym, int y0, int yp, int ucs, int lane,
+                                              float (&acc)[3]) {
+  acc[0] = acc[1] = acc[2] = 0.f;
+  // fully unrolled (predicated) so that all loads of a lane are in flight together
+#pragma unroll
+  for (int k = 0; k < (27 + kTw - 1) / kTw; k++) {
+    const int o = lane + k * kTw;
+    if (o < 27 && !(kSkipCentre && o == 13)) {
+      const float s = kSmemSt ? sp[o * sstride] : __ldg(sp + o * sstride);
+      const int ox = o % 3, oy = (o / 3) % 3, oz = o / 9;
+      const int xo = ox == 0 ? xm : (ox == 1 ? x : xp);
+      const int yo = oy == 0 ? ym : (oy == 1 ? y0 : yp);
+      const float* q = (oz == 0 ? pu[0] : (oz == 1 ? pu[1] : pu[2])) + yo + xo;
+#pragma unroll
+      for (int c = 0; c < 3; c++) acc[c] += s * q[c * ucs];
+    }
+  }
+#pragma unroll
+  for (int off = kTw >> 1; off > 0; off >>= 1)
+#pragma unroll
+    for (int c = 0; c < 3; c++) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], off);
+}
+
+// One Gauss-Seidel colour pass over this CTA's vertices of the colour (gs_coarse_body, the
+// off-diagonal sum formed by a lane team); updated edge-plane values are pushed to the ghosts.
+// Vertices are enumerated over power-of-two index ranges (shifts and masks instead of
+// divisions); indices past nx/2 or ny/2 are idle.
+template <bool kSmemSt, int kTwl>
+__device__ __forceinline__ void cl_gs_t(const ClLevel& L, const float* __restrict__ f_glob, float* sm, const int* tab,
+                                        float* const* rb, int rank, int color) {
   const Dims d = L.d;
   const int nx = d.nx, ny = d.ny, hx = nx >> 1, hy = ny >> 1, plane = nx * ny;
   const int z0 = L.zstart[rank], z1 = L.zstart[rank + 1];
   const int zf = z0 + (((z0 & 1) != (color >> 2)) ? 1 : 0);  // first own plane of the colour's parity
   const int npl = zf < z1 ? (z1 - zf + 1) >> 1 : 0;
-  const int n = npl * hx * hy;
-  const int cs = L.cs;
+  const int lhx = L.lhx, lhy = L.lhy;
+  const int n = npl << (lhx + lhy);
+  if (n == 0) return;  // uniform over the CTA
+  const int cs = L.cs, ucs = L.ucs, urs = L.urs, ups = L.ups;
   const size_t nv = d.nv();
-  for (int t = threadIdx.x; t < n; t += blockDim.x) {
-    const int i = t % hx, j = (t / hx) % hy, pk = t / (hx * hy);
+  // every lane of a warp runs the same number of rounds (the team shuffles need all 32)
+  const int total = ((n << kTwl) + int(blockDim.x) - 1) / int(blockDim.x) * int(blockDim.x);
+  for (int g = threadIdx.x; g < total; g += blockDim.x) {
+    const int t0 = g >> kTwl, lane = g & ((1 << kTwl) - 1);
+    const int i0 = t0 & ((1 << lhx) - 1), j0 = (t0 >> lhx) & ((1 << lhy) - 1), pk0 = t0 >> (lhx + lhy);
+    const bool active = t0 < n && i0 < hx && j0 < hy;
+    const int i = active ? i0 : 0, j = active ? j0 : 0, pk = active ? pk0 : 0;
     const int x = 2 * i + (color & 1), y = 2 * j + ((color >> 1) & 1), z = zf + 2 * pk;
     const int xm = wrapm(x - 1, nx), xp = wrapm(x + 1, nx);
-    const int ym = wrapm(y - 1, ny) * nx, y0 = y * nx, yp = wrapm(y + 1, ny) * nx;
-    const float* pu[3] = {cl_plane(L, tab, rb, L.u_off, wrapm(z - 1, d.nz)), sm + L.u_off + (z - z0) * plane,
-                          cl_plane(L, tab, rb, L.u_off, wrapm(z + 1, d.nz))};
-    const int lidx = (z - z0) * plane + y0 + x;
-    const float* sp = kSmemSt ? sm + L.st_off + lidx : L.st + cb_index(d, x, y, z);
-    const size_t sstride = kSmemSt ? size_t(cs) : nv;
+    const int ym = wrapm(y - 1, ny) * urs, y0 = y * urs, yp = wrapm(y + 1, ny) * urs;
+    const int zl = z - z0;
+    const float* uz = sm + L.u_off + zl * ups;  // local planes zl, zl+1, zl+2 = z-1, z, z+1
+    const float* const pu[3] = {uz, uz + ups, uz + 2 * ups};
+    const int lidx = zl * plane + y * nx + x;  // own-vertex index (f, r, stencils)
+    const float* sp = kSmemSt ? sm + L.st_off + lidx * 27 : L.st + cb_index(d, x, y, z);
+    const size_t sstride = kSmemSt ? size_t(1) : nv;
     float acc[3];
+    cl_apply_team<kSmemSt, true, (1 << kTwl)>(sp, sstride, pu, xm, x, xp, ym, y0, yp, ucs, lane, acc);
+    if (active && lane == 0) {
+      const float inv = kSmemSt ? sm[L.inv_off + lidx] : 1.0f / __ldg(sp + 13 * sstride);
+      const int pu_idx = y0 + x;
 #pragma unroll
-    for (int c = 0; c < 3; c++) acc[c] = sm[L.f_off + c * cs + lidx];
-#pragma unroll
-    for (int o = 0; o < 27; o++) {
-      if (o == 13) continue;
-      const float s = kSmemSt ? sp[o * sstride] : __ldg(sp + o * sstride);
-      const int xo = o % 3 == 0 ? xm : (o % 3 == 1 ? x : xp);
-      const int yo = (o / 3) % 3 == 0 ? ym : ((o / 3) % 3 == 1 ? y0 : yp);
-      const float* q = pu[o / 9] + yo + xo;
-#pragma unroll
-      for (int c = 0; c < 3; c++) acc[c] -= s * q[c * cs];
+      for (int c = 0; c < 3; c++) {
+        const float f = L.f_off >= 0 ? sm[L.f_off + c * cs + lidx] : __ldg(f_glob + c * nv + size_t(z) * plane + y * nx + x);
+        const float v = (f - acc[c]) * inv;
+        sm[L.u_off + c * ucs + (zl + 1) * ups + pu_idx] = v;
+        cl_push(L, tab, rb, z, pu_idx, c, v);
+      }
     }
-    const float s13 = kSmemSt ? sp[13 * sstride] : __ldg(sp + 13 * sstride);
-    const float inv = 1.0f / s13;
-#pragma unroll
-    for (int c = 0; c < 3; c++) sm[L.u_off + c * cs + lidx] = acc[c] * inv;
   }
 }
 
-__device__ __forceinline__ void cl_gs(const ClLevel& L, float* sm, const int* tab, float* const* rb, int rank,
-                                      int color) {
-  if (L.st_off >= 0)
-    cl_gs_t<true>(L, sm, tab, rb, rank, color);
+// The first level (global stencils) runs one lane per vertex; the others a team of 8.
+__device__ __forceinline__ void cl_gs(const ClLevel& L, const float* f_glob, float* sm, const int* tab,
+                                      float* const* rb, int rank, int color) {
+  if (L.st_off < 0)
+    cl_gs_t<false, 0>(L, f_glob, sm, tab, rb, rank, color);
   else
-    cl_gs_t<false>(L, sm, tab, rb, rank, color);
+    cl_gs_t<true, 3>(L, f_glob, sm, tab, rb, rank, color);
 }
 
-// r = f - A u on this CTA's vertices (resid_coarse_body).
-template <bool kSmemSt>
-__device__ __forceinline__ void cl_resid_t(const ClLevel& L, float* sm, const int* tab, float* const* rb,
+// r = f - A u on this CTA's vertices (resid_coarse_body, the sum formed by a lane team).
+template <bool kSmemSt, int kTwl>
+__device__ __forceinline__ void cl_resid_t(const ClLevel& L, const float* __restrict__ f_glob, float* sm,
                                            int rank) {
   const Dims d = L.d;
   const int nx = d.nx, ny = d.ny, plane = nx * ny;
   const int z0 = L.zstart[rank], z1 = L.zstart[rank + 1];
-  const int n = (z1 - z0) * plane;
-  const int cs = L.cs;
+  const int lnx = L.lnx, lny = L.lny;
+  const int n = (z1 - z0) << (lnx + lny);
+  if (n == 0) return;  // uniform over the CTA
+  const int cs = L.cs, ucs = L.ucs, urs = L.urs, ups = L.ups;
   const size_t nv = d.nv();
-  for (int t = threadIdx.x; t < n; t += blockDim.x) {
-    const int zl = t / plane, rem = t - zl * plane, y = rem / nx, x = rem - y * nx, z = z0 + zl;
+  const int total = ((n << kTwl) + int(blockDim.x) - 1) / int(blockDim.x) * int(blockDim.x);
+  for (int g = threadIdx.x; g < total; g += blockDim.x) {
+    const int t0 = g >> kTwl, lane = g & ((1 << kTwl) - 1);
+    const int x0 = t0 & ((1 << lnx) - 1), y0i = (t0 >> lnx) & ((1 << lny) - 1), zl0 = t0 >> (lnx + lny);
+    const bool active = t0 < n && x0 < nx && y0i < ny;
+    const int x = active ? x0 : 0, y = active ? y0i : 0, zl = active ? zl0 : 0;
+    const int z = z0 + zl;
     const int xm = wrapm(x - 1, nx), xp = wrapm(x + 1, nx);
-    const int ym = wrapm(y - 1, ny) * nx, y0 = y * nx, yp = wrapm(y + 1, ny) * nx;
-    const float* pu[3] = {cl_plane(L, tab, rb, L.u_off, wrapm(z - 1, d.nz)), sm + L.u_off + zl * plane,
-                          cl_plane(L, tab, rb, L.u_off, wrapm(z + 1, d.nz))};
-    const float* sp = kSmemSt ? sm + L.st_off + t : L.st + cb_index(d, x, y, z);
-    const size_t sstride = kSmemSt ? size_t(cs) : nv;
+    const int ym = wrapm(y - 1, ny) * urs, y0 = y * urs, yp = wrapm(y + 1, ny) * urs;
+    const float* uz = sm + L.u_off + zl * ups;
+    const float* const pu[3] = {uz, uz + ups, uz + 2 * ups};
+    const int lidx = zl * plane + y * nx + x;
+    const float* sp = kSmemSt ? sm + L.st_off + lidx * 27 : L.st + cb_index(d, x, y, z);
+    const size_t sstride = kSmemSt ? size_t(1) : nv;
     float acc[3];
+    cl_apply_team<kSmemSt, false, (1 << kTwl)>(sp, sstride, pu, xm, x, xp, ym, y0, yp, ucs, lane, acc);
+    if (active && lane == 0) {
+      const size_t gi = size_t(z) * plane + y * nx + x;
 #pragma unroll
-    for (int c = 0; c < 3; c++) acc[c] = sm[L.f_off + c * cs + t];
-#pragma unroll
-    for (int o = 0; o < 27; o++) {
-      const float s = kSmemSt ? sp[o * sstride] : __ldg(sp + o * sstride);
-      const int xo = o % 3 == 0 ? xm : (o % 3 == 1 ? x : xp);
-      const int yo = (o / 3) % 3 == 0 ? ym : ((o / 3) % 3 == 1 ? y0 : yp);
-      const float* q = pu[o / 9] + yo + xo;
-#pragma unroll
-      for (int c = 0; c < 3; c++) acc[c] -= s * q[c * cs];
-    }
-    if (L.r_off >= 0) {
-#pragma unroll
-      for (int c = 0; c < 3; c++) sm[L.r_off + c * cs + t] = acc[c];
-    } else {
-      const size_t g = size_t(z) * plane + rem;
-#pragma unroll
-      for (int c = 0; c < 3; c++) L.rg[c * nv + g] = acc[c];
+      for (int c = 0; c < 3; c++) {
+        const float f = L.f_off >= 0 ? sm[L.f_off + c * cs + lidx] : __ldg(f_glob + c * nv + gi);
+        if (L.r_off >= 0)
+          sm[L.r_off + c * cs + lidx] = f - acc[c];
+        else
+          L.rg[c * nv + gi] = f - acc[c];
+      }
     }
   }
 }
 
-__device__ __forceinline__ void cl_resid(const ClLevel& L, float* sm, const int* tab, float* const* rb, int rank) {
-  if (L.st_off >= 0)
-    cl_resid_t<true>(L, sm, tab, rb, rank);
+__device__ __forceinline__ void cl_resid(const ClLevel& L, const float* f_glob, float* sm, int rank) {
+  if (L.st_off < 0)
+    cl_resid_t<false, 0>(L, f_glob, sm, rank);
+  else if (L.tw_res >= 3)
+    cl_resid_t<true, 3>(L, f_glob, sm, rank);
   else
-    cl_resid_t<false>(L, sm, tab, rb, rank);
+    cl_resid_t<true, 0>(L, f_glob, sm, rank);
 }
 
-// f_C = P^T r_F on this CTA's coarse vertices, and u_C = 0 there (restrict_body).
+// u = 0 on this CTA's planes of a level, ghost copies included.
+__device__ __forceinline__ void cl_zero_u(const ClLevel& L, float* sm, int rank) {
+  const int n = (L.zstart[rank + 1] - L.zstart[rank] + 2) * L.ups;
+  for (int idx = threadIdx.x; idx < 3 * n; idx += blockDim.x) {
+    const int c = idx / n;
+    sm[L.u_off + c * L.ucs + (idx - c * n)] = 0.f;
+  }
+}
+
+// f_C = P^T r_F on this CTA's coarse vertices (restrict_body).
 __device__ __forceinline__ void cl_restrict(const ClLevel& F, const ClLevel& C, float* sm, const int* tab,
                                             float* const* rb, int rank) {
   const Dims df = F.d, dc = C.d;
@@ -192,11 +270,9 @@ __device__ __forceinline__ void cl_restrict(const ClLevel& F, const ClLevel& C, 
       for (int c = 0; c < 3; c++) acc[c] += w * (F.r_off >= 0 ? q[c * cstride] : __ldcg(q + c * cstride));
     }
 #pragma unroll
-    for (int c = 0; c < 3; c++) {
-      sm[C.f_off + c * C.cs + t] = acc[c];
-      sm[C.u_off + c * C.cs + t] = 0.f;
-    }
+    for (int c = 0; c < 3; c++) sm[C.f_off + c * C.cs + t] = acc[c];
   }
+  cl_zero_u(C, sm, rank);
 }
 
 // u_C = Ainv (f_C - mean f_C) on this CTA's coarsest vertices (k_coarsest_solve): every CTA
@@ -239,14 +315,16 @@ __device__ __forceinline__ void cl_coarsest(const ClDesc& cd, float* sm, const i
       a2 += __shfl_xor_sync(0xffffffffu, a2, off);
     }
     if (lane == 0) {
-      sm[C.u_off + t] = float(a0);
-      sm[C.u_off + C.cs + t] = float(a1);
-      sm[C.u_off + 2 * C.cs + t] = float(a2);
+      const int zl = t / pc, rem = t - zl * pc, y = rem / C.d.nx, x = rem - y * C.d.nx;
+      float* u = sm + C.u_off + (zl + 1) * C.ups + y * C.urs + x;  // own planes start at local plane 1
+      u[0] = float(a0);
+      u[C.ucs] = float(a1);
+      u[2 * C.ucs] = float(a2);
     }
   }
 }
 
-// u_F += P u_C on this CTA's fine vertices (prolong_body).
+// u_F += P u_C on this CTA's fine vertices (prolong_body); edge-plane results pushed to ghosts.
 __device__ __forceinline__ void cl_prolong(const ClLevel& F, const ClLevel& C, float* sm, const int* tab,
                                            float* const* rb, int rank) {
   const Dims df = F.d, dc = C.d;
@@ -261,19 +339,22 @@ __device__ __forceinline__ void cl_prolong(const ClLevel& F, const ClLevel& C, f
     const int Z1 = (z & 1) ? wrapm(Z0 + 1, dc.nz) : Z0;
     const float wx1 = (x & 1) ? 0.5f : 0.f, wy1 = (y & 1) ? 0.5f : 0.f, wz1 = (z & 1) ? 0.5f : 0.f;
     const float wx0 = 1.f - wx1, wy0 = 1.f - wy1, wz0 = 1.f - wz1;
-    const float* p0 = cl_plane(C, tab, rb, C.u_off, Z0);
-    const float* p1 = cl_plane(C, tab, rb, C.u_off, Z1);
-    const int r0 = Y0 * dc.nx, r1 = Y1 * dc.nx;
+    const float* p0 = cl_uplane(C, tab, rb, Z0);
+    const float* p1 = cl_uplane(C, tab, rb, Z1);
+    const int r0 = Y0 * C.urs, r1 = Y1 * C.urs;
+    const int pu_idx = y * F.urs + x;
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-      const float* u0 = p0 + c * C.cs;
-      const float* u1 = p1 + c * C.cs;
+      const float* u0 = p0 + c * C.ucs;
+      const float* u1 = p1 + c * C.ucs;
       const float a = wz0 * (wy0 * (wx0 * u0[r0 + X0] + wx1 * u0[r0 + X1]) +
                              wy1 * (wx0 * u0[r1 + X0] + wx1 * u0[r1 + X1])) +
                       wz1 * (wy0 * (wx0 * u1[r0 + X0] + wx1 * u1[r0 + X1]) +
                              wy1 * (wx0 * u1[r1 + X0] + wx1 * u1[r1 + X1]));
-      float* uf = sm + F.u_off + c * F.cs + t;
-      *uf = *uf + a;
+      float* uf = sm + F.u_off + c * F.ucs + (zl + 1) * F.ups + pu_idx;
+      const float v = *uf + a;
+      *uf = v;
+      cl_push(F, tab, rb, z, pu_idx, c, v);
     }
   }
 }
@@ -299,29 +380,27 @@ static __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads)
   if (threadIdx.x < kCl) rb[threadIdx.x] = cluster.map_shared_rank(sm, int(threadIdx.x));
   int* tab = reinterpret_cast<int*>(sm + cd.tab_base);
   const int L = cd.nlev;
+  // plane tables: owner and local plane of every plane; the ghost copies every plane feeds
   for (int l = 0; l < L; l++) {
     const ClLevel& V = cd.lv[l];
-    for (int z = threadIdx.x; z < V.d.nz; z += blockDim.x) {
+    const int nz = V.d.nz;
+    for (int z = threadIdx.x; z < nz; z += blockDim.x) {
       int c = 0;
       while (c < kCl - 1 && z >= V.zstart[c + 1]) c++;
       tab[V.tab_off + z] = (c << 16) | (z - V.zstart[c]);
-    }
-  }
-  // own planes: right-hand side of the first level, zero correction; stencils of the others
-  {
-    const ClLevel& T = cd.lv[0];
-    const int pl = T.d.nx * T.d.ny, z0 = T.zstart[rank];
-    const int n = (T.zstart[rank + 1] - z0) * pl;
-    const size_t nv = T.d.nv();
-    for (int t = threadIdx.x; t < n; t += blockDim.x) {
-      const size_t g = size_t(z0) * pl + t;
-#pragma unroll
-      for (int c = 0; c < 3; c++) {
-        sm[T.f_off + c * T.cs + t] = __ldg(cd.f_in + c * nv + g);
-        sm[T.u_off + c * T.cs + t] = 0.f;
+      int k = 0;
+      int* push = tab + V.tab_off + nz + 2 * z;
+      push[0] = push[1] = -1;
+      for (int q = 0; q < kCl && k < 2; q++) {
+        const int a = V.zstart[q], b = V.zstart[q + 1];
+        if (b == a) continue;
+        if (wrapm(a - 1, nz) == z) push[k++] = (q << 16) | 0;          // q's lower ghost
+        if (k < 2 && wrapm(b, nz) == z) push[k++] = (q << 16) | (b - a + 1);  // q's upper ghost
       }
     }
   }
+  // first level: zero correction (ghosts included); stencils of the other smoothed levels
+  cl_zero_u(cd.lv[0], sm, rank);
   for (int l = 1; l < L - 1; l++) {
     const ClLevel& V = cd.lv[l];
     const int nx = V.d.nx, pl = nx * V.d.ny, z0 = V.zstart[rank];
@@ -330,7 +409,9 @@ static __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads)
     for (int idx = threadIdx.x; idx < 27 * n; idx += blockDim.x) {
       const int o = idx / n, t = idx - o * n;
       const int zl = t / pl, rem = t - zl * pl, y = rem / nx, x = rem - y * nx;
-      sm[V.st_off + o * V.cs + t] = __ldg(V.st + size_t(o) * nv + cb_index(V.d, x, y, z0 + zl));
+      const float a = __ldg(V.st + size_t(o) * nv + cb_index(V.d, x, y, z0 + zl));
+      sm[V.st_off + t * 27 + o] = a;
+      if (o == 13) sm[V.inv_off + t] = 1.0f / a;
     }
   }
   cluster.sync();
@@ -338,10 +419,10 @@ static __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads)
     const ClLevel& F = cd.lv[l];
     for (int s = 0; s < cd.pre; s++)
       for (int c = 0; c < 8; c++) {
-        cl_gs(F, sm, tab, rb, rank, c);
+        cl_gs(F, cd.f_in, sm, tab, rb, rank, c);
         cluster.sync();
       }
-    cl_resid(F, sm, tab, rb, rank);
+    cl_resid(F, cd.f_in, sm, rank);
     cluster.sync();
     cl_restrict(F, cd.lv[l + 1], sm, tab, rb, rank);
     cluster.sync();
@@ -354,7 +435,7 @@ static __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads)
     cluster.sync();
     for (int s = 0; s < cd.post; s++)
       for (int c = 7; c >= 0; c--) {
-        cl_gs(F, sm, tab, rb, rank, c);
+        cl_gs(F, cd.f_in, sm, tab, rb, rank, c);
         cluster.sync();
       }
   }
@@ -366,8 +447,9 @@ static __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads)
     const size_t nv = T.d.nv();
     for (int t = threadIdx.x; t < n; t += blockDim.x) {
       const size_t g = size_t(z0) * pl + t;
+      const int zl = t / pl, rem = t - zl * pl, y = rem / T.d.nx, x = rem - y * T.d.nx;
 #pragma unroll
-      for (int c = 0; c < 3; c++) cd.u_out[c * nv + g] = sm[T.u_off + c * T.cs + t];
+      for (int c = 0; c < 3; c++) cd.u_out[c * nv + g] = sm[T.u_off + c * T.ucs + (zl + 1) * T.ups + y * T.urs + x];
     }
   }
 }
@@ -375,6 +457,37 @@ static __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads)
 // Host-side layout of the cluster part for the level dimensions dims[0..n-1] (the last one is
 // the coarsest). Returns the dynamic shared memory in bytes, or 0 when the levels do not fit
 // one cluster (then the per-level kernels are used).
+// Worst number of distinct shared-memory words per bank over the lane-team reads of u (teams of
+// 8 lanes at vertices x, x+2, x+4, x+6; lane k reads offset k + 8 round) for row stride rs
+// and plane stride ps.
+inline int cl_team_conflicts(int rs, int ps) {
+  int worst = 1;
+  for (int round = 0; round < 4; round++) {
+    int addr[32], na = 0;
+    for (int j = 0; j < 4; j++)
+      for (int lane = 0; lane < 8; lane++) {
+        const int o = lane + 8 * round;
+        if (o >= 27) continue;
+        const int a = 2 * j + (o / 9) * ps + ((o / 3) % 3) * rs + o % 3;
+        bool dup = false;
+        for (int q = 0; q < na; q++) dup = dup || addr[q] == a;
+        if (!dup) addr[na++] = a;
+      }
+    for (int b = 0; b < 32; b++) {
+      int cnt = 0;
+      for (int q = 0; q < na; q++) cnt += (addr[q] % 32) == b;
+      worst = std::max(worst, cnt);
+    }
+  }
+  return worst;
+}
+
+inline int cl_log2_ceil(int v) {
+  int l = 0;
+  while ((1 << l) < v) l++;
+  return l;
+}
+
 inline size_t cl_plan(const Dims* dims, int n, ClDesc* cd) {
   if (n < 2 || n > kClMaxLevels) return 0;
   if (dims[0].nv() > size_t(kClMaxNv)) return 0;
@@ -385,25 +498,54 @@ inline size_t cl_plan(const Dims* dims, int n, ClDesc* cd) {
     V = ClLevel{};
     V.d = d;
     if (l < n - 1 && ((d.nx | d.ny | d.nz) & 1)) return 0;  // smoothed levels are colour-split
-    if (d.nz > 0xffff) return 0;
+    if (d.nz > 0x7fff) return 0;
     int maxpl = 0;
     for (int c = 0; c <= kCl; c++) V.zstart[c] = int((long long)c * d.nz / kCl);
     for (int c = 0; c < kCl; c++) maxpl = std::max(maxpl, V.zstart[c + 1] - V.zstart[c]);
-    V.cs = maxpl * d.nx * d.ny;
+    const int plane = d.nx * d.ny;
+    V.cs = maxpl * plane;
+    // u strides: padded on the lane-team levels so that a round of team reads is free of bank
+    // conflicts (smallest plane stride among the best), plain on the first level
+    V.urs = d.nx;
+    V.ups = plane;
+    if (l > 0 && l < n - 1) {
+      int best = cl_team_conflicts(V.urs, V.ups);
+      for (int px = 0; px <= 32 && best > 1; px++)
+        for (int py = 0; py < 64; py++) {
+          const int rs = d.nx + px, ps = rs * d.ny + py;
+          const int w = cl_team_conflicts(rs, ps);
+          if (w < best || (w == best && ps < V.ups)) {
+            best = w;
+            V.urs = rs;
+            V.ups = ps;
+          }
+        }
+    }
+    V.ucs = (maxpl + 2) * V.ups;
     V.u_off = off;
-    off += 3 * V.cs;
-    V.f_off = off;
-    off += 3 * V.cs;
-    V.r_off = -1;
-    V.st_off = -1;
+    off += 3 * V.ucs;
+    V.f_off = -1;  // the first level reads its right-hand side from global memory
+    if (l > 0) {
+      V.f_off = off;
+      off += 3 * V.cs;
+    }
+    V.r_off = V.st_off = V.inv_off = -1;
     if (l > 0 && l < n - 1) {
       V.r_off = off;
       off += 3 * V.cs;
       V.st_off = off;
       off += 27 * V.cs;
+      V.inv_off = off;
+      off += V.cs;
     }
     V.tab_off = tab;
-    tab += d.nz;
+    tab += 3 * d.nz;
+    V.lhx = cl_log2_ceil(std::max(1, d.nx / 2));
+    V.lhy = cl_log2_ceil(std::max(1, d.ny / 2));
+    V.lnx = cl_log2_ceil(d.nx);
+    V.lny = cl_log2_ceil(d.ny);
+    // residual: 8 lanes per vertex where that fills about one round of the CTA's threads
+    V.tw_res = (((maxpl << (V.lnx + V.lny)) << 3) <= 2 * kClThreads) ? 3 : 0;
   }
   cd->nlev = n;
   cd->nc = int(dims[n - 1].nv());

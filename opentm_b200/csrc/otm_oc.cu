@@ -143,14 +143,18 @@ __global__ void __launch_bounds__(kBlock) k_oc_tree_pass(int ne, const float* __
   if (threadIdx.x < kTreeNodes) {
     double b = 0.0;
     for (int w = 0; w < int(blockDim.x) / 32; w++) b += double(wsum[w][threadIdx.x]);
-    partials[blockIdx.x * kTreeNodes + threadIdx.x] = b;
+    partials[threadIdx.x * gridDim.x + blockIdx.x] = b;  // candidate-major
   }
   if (last_block(&st->counter)) {
+    // one warp per candidate sums the blocks' partials (coalesced, fixed order)
     __shared__ double tot[kTreeNodes];
-    if (threadIdx.x < kTreeNodes) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int t = warp; t < kTreeNodes; t += int(blockDim.x >> 5)) {
       double a = 0.0;
-      for (int b = 0; b < int(gridDim.x); b++) a += ((volatile double*)partials)[b * kTreeNodes + threadIdx.x];
-      tot[threadIdx.x] = a;
+      for (int b = lane; b < int(gridDim.x); b += 32) a += ((volatile double*)partials)[t * gridDim.x + b];
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
+      if (lane == 0) tot[t] = a;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
