@@ -221,7 +221,7 @@ def run_ours(args, rank, world, local_rank):
         traffic = None
         tp = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(tp):
-            traffic = json.load(open(tp)).get("k_gs_fine_bytes_per_launch_n128")
+            traffic = json.load(open(tp)).get(f"k_gs_fine_pair_dram_bytes_per_launch_n{n}")
         roofline = {"bound": "hbm", "kernel": "k_gs_fine_pair (one colour-pair pass, 3 load cases)",
                     "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                     "frac": round(achieved / hbm, 4), "traffic": traffic,
