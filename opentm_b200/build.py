@@ -27,6 +27,7 @@ SOURCES = [
     "otm_mma.cu",
     "otm_server.cu",
     "otm_noalloc.cu",
+    "otm_pool.cu",
 ]
 
 

@@ -24,6 +24,8 @@ void count_launches(uint64_t n);
 // Per-thread message of the last failure, returned by otm_last_error().
 void set_error(const std::string& msg);
 otm_status cuda_fail(cudaError_t e, const char* what);
+// Stream-ordered scratch from the library's per-device memory pool (freed with cudaFreeAsync).
+cudaError_t scratch_malloc(void** p, size_t bytes, cudaStream_t s);
 
 #define OTM_CUDA(call)                                  \
   do {                                                  \
@@ -48,6 +50,18 @@ struct Dims {
   int nx, ny, nz;
   __host__ __device__ size_t nv() const { return size_t(nx) * ny * nz; }
 };
+
+// (x, y, z) of lexicographic index v (x fastest) on a grid with rows of nx and planes of
+// nx * ny points. Grids hold at most 1024^3 = 2^30 points, so 32-bit division is exact and
+// several times cheaper than 64-bit.
+struct Coord3 {
+  int x, y, z;
+};
+__host__ __device__ __forceinline__ Coord3 split3(size_t v, int nx, int ny) {
+  const unsigned u = unsigned(v), unx = unsigned(nx), uny = unsigned(ny);
+  const unsigned q = u / unx;
+  return Coord3{int(u - q * unx), int(q % uny), int(q / uny)};
+}
 
 __device__ __forceinline__ int wrapm(int a, int n) {
   // a in [-n, 2n)

@@ -510,13 +510,12 @@ void Homo::iteration(int j) {
   } else if (cfg.solver == OTM_SOLVER_PCG) {
     vcycle(0);
     k_dot_rz<<<nb, kBlock, 0, stream>>>(nv, r, z, partials, sc);
-    k_update_p<<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(nv, z, p, sc);
     if (face)
-      k_apply_dot<true><<<nb, kBlock, 0, stream>>>(d0, ks, op, p, q, partials, sc);
+      k_update_p_apply_dot<true><<<nb, kBlock, 0, stream>>>(d0, ks, op, z, p, q, partials, sc);
     else
-      k_apply_dot<false><<<nb, kBlock, 0, stream>>>(d0, ks, op, p, q, partials, sc);
+      k_update_p_apply_dot<false><<<nb, kBlock, 0, stream>>>(d0, ks, op, z, p, q, partials, sc);
     k_update_xr<<<nb, kBlock, 0, stream>>>(nv, x, r, p, q, partials, sc, cfg.max_iter);
-    launched(4);
+    launched(3);
   } else {
     if (face)
       k_resid_norm<true><<<nb, kBlock, 0, stream>>>(d0, ks, op, x, b, r, partials, sc, cfg.max_iter);
@@ -573,13 +572,11 @@ void Homo::launch_solve_init() {
   const size_t nv = d0.nv();
   const int nb = reduce_blocks(nv);
   cudaMemsetAsync(x, 0, 3 * nv * sizeof(float), stream);
-  k_rhs<<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(d0, ks, ef, b);
-  k_sums2<<<nb, kBlock, 0, stream>>>(nv, b, x, partials, means, &sc->counter[T_MEAN]);
-  k_sub_means<<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(nv, b, x, means);
+  k_rhs_mean<<<nb, kBlock, 0, stream>>>(d0, ks, ef, b, partials, means, &sc->counter[T_MEAN]);
   sc_host->tol = cfg.fem_rel_thres;
   cudaMemcpyAsync(&sc->tol, &sc_host->tol, sizeof(double), cudaMemcpyHostToDevice, stream);
-  k_init_residual<false><<<nb, kBlock, 0, stream>>>(d0, ks, op, x, b, lv[0].f, partials, sc);
-  launched(4);
+  k_init_residual<false><<<nb, kBlock, 0, stream>>>(d0, ks, op, x, b, means, lv[0].f, partials, sc);
+  launched(2);
 }
 
 void Homo::launch_heat_matrix() {
@@ -674,13 +671,12 @@ void Homo::launch_solve_start() {
   const Dims d0 = lv[0].d;
   const size_t nv = d0.nv();
   const int nb = reduce_blocks(nv);
-  k_rhs<<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(d0, ks, ef, b);
-  // project RHS and initial guess off the constants
-  k_sums2<<<nb, kBlock, 0, stream>>>(nv, b, x, partials, means, &sc->counter[T_MEAN]);
-  k_sub_means<<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(nv, b, x, means);
+  // right-hand sides and their means; the initial residual kernel projects b off the constants
+  k_rhs_mean<<<nb, kBlock, 0, stream>>>(d0, ks, ef, b, partials, means, &sc->counter[T_MEAN]);
   sc_host->tol = cfg.fem_rel_thres;
   cudaMemcpyAsync(&sc->tol, &sc_host->tol, sizeof(double), cudaMemcpyHostToDevice, stream);
   if (mixed) {
+    k_sub_bmean<<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(nv, b, means);
     const unsigned int* kmax_bits = (const unsigned int*)(flags + 2);
     if (face)
       k_resid64<true><<<nb, kBlock, 0, stream>>>(d0, ks, op, x64, b, lv[0].f, partials, sc, kmax_bits, cfg.max_iter,
@@ -689,11 +685,11 @@ void Homo::launch_solve_start() {
       k_resid64<false><<<nb, kBlock, 0, stream>>>(d0, ks, op, x64, b, lv[0].f, partials, sc, kmax_bits,
                                                   cfg.max_iter, 1);
   } else if (face) {
-    k_init_residual<true><<<nb, kBlock, 0, stream>>>(d0, ks, op, x, b, lv[0].f, partials, sc);
+    k_init_residual<true><<<nb, kBlock, 0, stream>>>(d0, ks, op, x, b, means, lv[0].f, partials, sc);
   } else {
-    k_init_residual<false><<<nb, kBlock, 0, stream>>>(d0, ks, op, x, b, lv[0].f, partials, sc);
+    k_init_residual<false><<<nb, kBlock, 0, stream>>>(d0, ks, op, x, b, means, lv[0].f, partials, sc);
   }
-  launched(4);
+  launched(mixed ? 3 : 2);
 }
 
 // Solve the 3 load cases to the tolerance (MG_H::solveEquation, homogenization/MG.cpp:80-142;

@@ -216,7 +216,8 @@ __device__ __forceinline__ void gs_fine_body(const Dims& d, int color, const KT*
   const int hx = d.nx >> 1, hy = d.ny >> 1;
   const size_t nsub = d.nv() >> 3;
   if (t >= nsub) return;
-  const int i = int(t % hx), j = int((t / hx) % hy), kq = int(t / (size_t(hx) * hy));
+  const Coord3 c3_ = split3(t, hx, hy);
+    const int i = c3_.x, j = c3_.y, kq = c3_.z;
   const int x = 2 * i + (color & 1), y = 2 * j + ((color >> 1) & 1), z = 2 * kq + (color >> 2);
   Nbr nb;
   nb.init(d, x, y, z);
@@ -253,7 +254,8 @@ __device__ __forceinline__ void gs_fine_pair_body(const Dims& d, int pair, const
   const int hx = d.nx >> 1, hy = d.ny >> 1;
   const size_t nsub = d.nv() >> 3;
   if (t >= nsub) return;
-  const int i = int(t % hx), j = int((t / hx) % hy), kq = int(t / (size_t(hx) * hy));
+  const Coord3 c3_ = split3(t, hx, hy);
+    const int i = c3_.x, j = c3_.y, kq = c3_.z;
   const int x = 2 * i + (pair & 1), y = 2 * j + ((pair >> 1) & 1), z = 2 * kq;
   const size_t nv = d.nv();
   const int xs[3] = {wrapm(x - 1, d.nx), x, wrapm(x + 1, d.nx)};
@@ -323,7 +325,8 @@ __device__ __forceinline__ void resid_fine_body(const Dims& d, const KT* __restr
                                                 VT* __restrict__ r, const double* fscale, size_t v) {
   const size_t nv = d.nv();
   if (v >= nv) return;
-  const int x = int(v % d.nx), y = int((v / d.nx) % d.ny), z = int(v / (size_t(d.nx) * d.ny));
+  const Coord3 c3_ = split3(v, d.nx, d.ny);
+    const int x = c3_.x, y = c3_.y, z = c3_.z;
   Nbr nb;
   nb.init(d, x, y, z);
   float k8[8];
@@ -360,7 +363,8 @@ __device__ __forceinline__ void gs_coarse_body(const Dims& d, int color, const f
   const int hx = d.nx >> 1, hy = d.ny >> 1;
   const size_t nsub = d.nv() >> 3;
   if (t >= nsub) return;
-  const int i = int(t % hx), j = int((t / hx) % hy), kq = int(t / (size_t(hx) * hy));
+  const Coord3 c3_ = split3(t, hx, hy);
+    const int i = c3_.x, j = c3_.y, kq = c3_.z;
   const int x = 2 * i + (color & 1), y = 2 * j + ((color >> 1) & 1), z = 2 * kq + (color >> 2);
   Nbr nb;
   nb.init(d, x, y, z);
@@ -396,7 +400,8 @@ __device__ __forceinline__ void resid_coarse_body(const Dims& d, const float* __
                                                   float* __restrict__ r, size_t v) {
   const size_t nv = d.nv();
   if (v >= nv) return;
-  const int x = int(v % d.nx), y = int((v / d.nx) % d.ny), z = int(v / (size_t(d.nx) * d.ny));
+  const Coord3 c3_ = split3(v, d.nx, d.ny);
+    const int x = c3_.x, y = c3_.y, z = c3_.z;
   Nbr nb;
   nb.init(d, x, y, z);
   const size_t sb = cb_index(d, x, y, z);
@@ -429,7 +434,8 @@ __device__ __forceinline__ void restrict_body(const Dims& df, const Dims& dc, co
                                               float* __restrict__ fc, size_t V) {
   const size_t nvc = dc.nv(), nvf = df.nv();
   if (V >= nvc) return;
-  const int X = int(V % dc.nx), Y = int((V / dc.nx) % dc.ny), Z = int(V / (size_t(dc.nx) * dc.ny));
+  const Coord3 c3_ = split3(V, dc.nx, dc.ny);
+    const int X = c3_.x, Y = c3_.y, Z = c3_.z;
   Nbr nb;
   nb.init(df, 2 * X, 2 * Y, 2 * Z);
   float acc[NC];
@@ -460,7 +466,8 @@ __device__ __forceinline__ void prolong_body(const Dims& df, const Dims& dc, con
                                              size_t v) {
   const size_t nvc = dc.nv(), nvf = df.nv();
   if (v >= nvf) return;
-  const int x = int(v % df.nx), y = int((v / df.nx) % df.ny), z = int(v / (size_t(df.nx) * df.ny));
+  const Coord3 c3_ = split3(v, df.nx, df.ny);
+    const int x = c3_.x, y = c3_.y, z = c3_.z;
   const int X0 = x >> 1, Y0 = y >> 1, Z0 = z >> 1;
   const int X1 = (x & 1) ? wrapm(X0 + 1, dc.nx) : X0;
   const int Y1 = (y & 1) ? wrapm(Y0 + 1, dc.ny) : Y0;
@@ -507,7 +514,8 @@ static __global__ void __launch_bounds__(kBlock) k_galerkin_fine(Dims df, Dims d
   const size_t nvc = dc.nv();
   const size_t V = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (V >= nvc) return;
-  const int X = int(V % dc.nx), Y = int((V / dc.nx) % dc.ny), Z = int(V / (size_t(dc.nx) * dc.ny));
+  const Coord3 c3_ = split3(V, dc.nx, dc.ny);
+    const int X = c3_.x, Y = c3_.y, Z = c3_.z;
   int xs[4], ys[4], zs[4];
 #pragma unroll
   for (int a = 0; a < 4; a++) {
@@ -555,7 +563,8 @@ static __global__ void __launch_bounds__(kBlock) k_galerkin_coarse(Dims df, Dims
   const size_t nvc = dc.nv(), nvf = df.nv();
   const size_t V = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (V >= nvc) return;
-  const int X = int(V % dc.nx), Y = int((V / dc.nx) % dc.ny), Z = int(V / (size_t(dc.nx) * dc.ny));
+  const Coord3 c3_ = split3(V, dc.nx, dc.ny);
+    const int X = c3_.x, Y = c3_.y, Z = c3_.z;
   float acc[27];
 #pragma unroll
   for (int o = 0; o < 27; o++) acc[o] = 0.f;

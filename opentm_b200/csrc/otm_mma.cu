@@ -322,20 +322,20 @@ static otm_status work_alloc(MmaWork& w, int m, size_t n, cudaStream_t s, bool a
   double** arr[] = {&w.alfa, &w.beta, &w.p0, &w.q0, &w.xs, &w.xsi, &w.eta, &w.dx, &w.dxsi, &w.deta};
   for (double** a : arr) {
     if (async)
-      OTM_CUDA(cudaMallocAsync((void**)a, n * sizeof(double), s));
+      OTM_CUDA(scratch_malloc((void**)a, n * sizeof(double), s));
     else
       OTM_CUDA(cudaMalloc((void**)a, n * sizeof(double)));
   }
   for (double** a : {&w.P, &w.Q}) {
     if (async)
-      OTM_CUDA(cudaMallocAsync((void**)a, size_t(m) * n * sizeof(double), s));
+      OTM_CUDA(scratch_malloc((void**)a, size_t(m) * n * sizeof(double), s));
     else
       OTM_CUDA(cudaMalloc((void**)a, size_t(m) * n * sizeof(double)));
   }
   const size_t small = size_t(kMaxPartials) * kMmaSlots * sizeof(double) + kMmaSlots * sizeof(double) + 64;
   char* buf = nullptr;
   if (async)
-    OTM_CUDA(cudaMallocAsync((void**)&buf, small, s));
+    OTM_CUDA(scratch_malloc((void**)&buf, small, s));
   else
     OTM_CUDA(cudaMalloc((void**)&buf, small));
   w.partials = (double*)buf;

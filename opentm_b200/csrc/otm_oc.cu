@@ -231,7 +231,8 @@ __global__ void __launch_bounds__(256) k_oc_filter(Dims d, const float* __restri
   const size_t nv = d.nv();
   const size_t v = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (v >= nv) return;
-  const int x = int(v % d.nx), y = int((v / d.nx) % d.ny), z = int(v / (size_t(d.nx) * d.ny));
+  const Coord3 c3_ = split3(v, d.nx, d.ny);
+    const int x = c3_.x, y = c3_.y, z = c3_.z;
   const int h = fw.half, w1 = 2 * h + 1;
   float sum = 0.f, ws = 0.f;
   for (int t = 0; t < fw.taps; t++) {
@@ -286,7 +287,7 @@ otm_status otm_oc_filter_sens(float* sens, const float* rho, size_t pitchT, cons
   for (int t = 0; t < fw.taps; t++) fw.w[t] /= wsum;
   cudaStream_t s = (cudaStream_t)stream;
   float* tmp = nullptr;
-  OTM_CUDA(cudaMallocAsync((void**)&tmp, d.nv() * sizeof(float), s));
+  OTM_CUDA(scratch_malloc((void**)&tmp, d.nv() * sizeof(float), s));
   k_oc_filter<<<ceil_div(d.nv(), 256), 256, 0, s>>>(d, sens, rho, pitchT, tmp, fw);
   k_copy_pitched<<<ceil_div(d.nv(), 256), 256, 0, s>>>(d, tmp, sens, pitchT);
   cudaError_t e = cudaGetLastError();
@@ -303,7 +304,7 @@ otm_status otm_oc_update(int ne, const float* sens, float* rho, float volratio, 
   const int nb = std::min(kMaxPartials, std::max(1, (ne + kBlock - 1) / kBlock));
   char* scratch = nullptr;
   const size_t bytes = sizeof(OcState) + size_t(nb) * kTreeNodes * sizeof(double);
-  OTM_CUDA(cudaMallocAsync((void**)&scratch, bytes, s));
+  OTM_CUDA(scratch_malloc((void**)&scratch, bytes, s));
   OcState* st = (OcState*)scratch;
   double* partials = (double*)(scratch + sizeof(OcState));
   cudaMemsetAsync(st, 0, sizeof(OcState), s);

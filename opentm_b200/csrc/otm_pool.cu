@@ -1,0 +1,51 @@
+// otm_pool.cu -- stream-ordered scratch memory of the handle-free entry points.
+//
+// The OC update, the OC sensitivity filter, the MMA subsolver and the server's task tables need
+// temporary device buffers per call. They take them from one memory pool per device owned by
+// the library, whose release threshold keeps freed memory cached: after the first calls every
+// allocation is served from the pool without a driver call, and synchronising a stream never
+// hands the memory back to the driver (the device's default pool would, and the next call would
+// then pay for a fresh allocation).
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+
+#include "otm_common.cuh"
+
+namespace otm {
+
+namespace {
+constexpr int kPoolMaxDevices = 64;
+cudaMemPool_t g_pools[kPoolMaxDevices] = {};
+std::mutex g_pool_mu;
+}  // namespace
+
+cudaError_t scratch_malloc(void** p, size_t bytes, cudaStream_t s) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kPoolMaxDevices) return cudaErrorInvalidDevice;
+  cudaMemPool_t pool = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    if (!g_pools[dev]) {
+      cudaMemPoolProps props{};
+      props.allocType = cudaMemAllocationTypePinned;
+      props.location.type = cudaMemLocationTypeDevice;
+      props.location.id = dev;
+      e = cudaMemPoolCreate(&g_pools[dev], &props);
+      if (e != cudaSuccess) {
+        g_pools[dev] = nullptr;
+        return e;
+      }
+      uint64_t keep = UINT64_MAX;
+      e = cudaMemPoolSetAttribute(g_pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+      if (e != cudaSuccess) return e;
+    }
+    pool = g_pools[dev];
+  }
+  return cudaMallocFromPoolAsync(p, bytes, pool, s);
+}
+
+}  // namespace otm

@@ -414,7 +414,7 @@ static otm_status run_batch(otm_server* s, const std::vector<int>& run_slots, in
   if (tasks.size() > s->task_cap) {
     if (s->d_tasks) cudaFreeAsync(s->d_tasks, s->stream);
     s->task_cap = tasks.size() * 2;
-    OTM_CUDA(cudaMallocAsync((void**)&s->d_tasks, s->task_cap * sizeof(BTask), s->stream));
+    OTM_CUDA(scratch_malloc((void**)&s->d_tasks, s->task_cap * sizeof(BTask), s->stream));
   }
   OTM_CUDA(cudaMemcpyAsync(s->d_tasks, tasks.data(), tasks.size() * sizeof(BTask), cudaMemcpyHostToDevice, s->stream));
   OTM_CUDA(cudaFuncSetAttribute(kb_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));

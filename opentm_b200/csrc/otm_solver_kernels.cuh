@@ -47,8 +47,9 @@ static __global__ void k_import(Dims d, const float* __restrict__ kin, int pitch
   const size_t nv = d.nv();
   const size_t e = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (e >= nv) return;
-  const int x = int(e % d.nx);
-  const size_t yz = e / d.nx;
+  const unsigned yz32 = unsigned(e) / unsigned(d.nx);
+  const int x = int(unsigned(e) - yz32 * unsigned(d.nx));
+  const size_t yz = yz32;
   const float k = __ldg(kin + yz * size_t(pitchT) + x);
   if (!(k >= 0.f) || !isfinite(k)) atomicOr(bad, 1);
   kraw[e] = k;
@@ -62,7 +63,8 @@ static __global__ void __launch_bounds__(kBlock) k_rhs(Dims d, const float* __re
   const size_t nv = d.nv();
   const size_t v = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (v >= nv) return;
-  const int x = int(v % d.nx), y = int((v / d.nx) % d.ny), z = int(v / (size_t(d.nx) * d.ny));
+  const Coord3 c3_ = split3(v, d.nx, d.ny);
+    const int x = c3_.x, y = c3_.y, z = c3_.z;
   Nbr nb;
   nb.init(d, x, y, z);
   float k8[8];
@@ -80,71 +82,87 @@ static __global__ void __launch_bounds__(kBlock) k_rhs(Dims d, const float* __re
 // Deterministic reductions (fixed grid, fixed order, last-block finalisation).
 // ---------------------------------------------------------------------------------------
 
-// Means of the 3 case vectors of a and b -> sc->mean[] (a), and the result of
-// subtracting them is done by k_sub_means. Used to project the RHS and the initial guess
-// onto the complement of the periodic nullspace (constants).
-static __global__ void __launch_bounds__(kBlock) k_sums2(size_t nv, const float* __restrict__ a,
-                                                  const float* __restrict__ b, double* partials,
-                                                  double* out6, unsigned int* counter) {
-  __shared__ double smem[32 * 6];
-  double v[6] = {0, 0, 0, 0, 0, 0};
+// Right-hand sides (as k_rhs) and their per-case means -> bmean[0..2] (grid-stride, fixed grid).
+// The initial guess is not projected: K^H, the energies and the sensitivity do not change when
+// a constant is added to a case's solution (the element matrix annihilates constants), and
+// every Krylov update adds a mean-free direction.
+static __global__ void __launch_bounds__(kBlock) k_rhs_mean(Dims d, const float* __restrict__ ks, ElemFields ef,
+                                                            float* __restrict__ b, double* partials, double* bmean,
+                                                            unsigned int* counter) {
+  __shared__ double smem[32 * 3];
+  const size_t nv = d.nv();
+  double v[3] = {0, 0, 0};
   for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nv; i += size_t(gridDim.x) * blockDim.x) {
+    const Coord3 c3_ = split3(i, d.nx, d.ny);
+    const int x = c3_.x, y = c3_.y, z = c3_.z;
+    Nbr nb;
+    nb.init(d, x, y, z);
+    float k8[8];
+    load_k8(ks, nb, k8);
+    float acc[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int bb = 0; bb < 8; bb++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) acc[c] += k8[bb] * ef.feMu[7 - bb][c];
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-      v[c] += a[c * nv + i];
-      v[3 + c] += b[c * nv + i];
+      b[c * nv + i] = acc[c];
+      v[c] += acc[c];
     }
   }
-  block_reduce_f64<6>(v, smem);
+  block_reduce_f64<3>(v, smem);
   if (threadIdx.x == 0)
 #pragma unroll
-    for (int i = 0; i < 6; i++) partials[blockIdx.x * 6 + i] = v[i];
+    for (int i = 0; i < 3; i++) partials[blockIdx.x * 3 + i] = v[i];
   if (last_block(counter)) {
-    double r[6];
-    reduce_partials<6>(partials, gridDim.x, r, smem);
+    double r[3];
+    reduce_partials<3>(partials, gridDim.x, r, smem);
     if (threadIdx.x == 0) {
 #pragma unroll
-      for (int i = 0; i < 6; i++) out6[i] = r[i] / double(nv);
+      for (int i = 0; i < 3; i++) bmean[i] = r[i] / double(nv);
       *counter = 0;
     }
   }
 }
 
-// a -= mean_a, b -= mean_b (per case), then ||a||^2 partials -> sc->bb when a is the RHS.
-static __global__ void __launch_bounds__(kBlock) k_sub_means(size_t nv, float* a, float* b, const double* means6) {
+// b -= mean b per case (the mixed-precision start, whose residual kernel reads b).
+static __global__ void __launch_bounds__(kBlock) k_sub_bmean(size_t nv, float* b, const double* bmean) {
   const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= nv) return;
 #pragma unroll
-  for (int c = 0; c < 3; c++) {
-    a[c * nv + i] -= float(means6[c]);
-    b[c * nv + i] -= float(means6[3 + c]);
-  }
+  for (int c = 0; c < 3; c++) b[c * nv + i] -= float(bmean[c]);
 }
 
-// r = b - A x on the fine level plus ||b||^2 and ||r||^2 -> sc (start of a Krylov solve).
+// b -= mean b (per case, in place), r = b - A x on the fine level, ||b||^2 and ||r||^2 -> sc
+// (start of a Krylov solve).
 template <bool kFace>
 __global__ void __launch_bounds__(kBlock) k_init_residual(Dims d, const float* __restrict__ ks, FineOp op,
-                                                          const float* __restrict__ x, const float* __restrict__ b,
-                                                          float* __restrict__ r, double* partials,
-                                                          SolveScalars* sc) {
+                                                          const float* __restrict__ x, float* b,
+                                                          const double* __restrict__ bmean, float* __restrict__ r,
+                                                          double* partials, SolveScalars* sc) {
   __shared__ double smem[32 * 6];
   const size_t nv = d.nv();
   double v[6] = {0, 0, 0, 0, 0, 0};
   for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nv; i += size_t(gridDim.x) * blockDim.x) {
-    const int xx = int(i % d.nx), yy = int((i / d.nx) % d.ny), zz = int(i / (size_t(d.nx) * d.ny));
+    const Coord3 c3_ = split3(i, d.nx, d.ny);
+    const int xx = c3_.x, yy = c3_.y, zz = c3_.z;
     Nbr nb;
     nb.init(d, xx, yy, zz);
     float k8[8];
     load_k8(ks, nb, k8);
-    float acc[3];
+    float acc[3], bp[3];
 #pragma unroll
-    for (int c = 0; c < 3; c++) acc[c] = b[c * nv + i];
+    for (int c = 0; c < 3; c++) {
+      bp[c] = b[c * nv + i] - float(bmean[c]);
+      b[c * nv + i] = bp[c];
+      acc[c] = bp[c];
+    }
     const float diag = fine_offdiag<kFace, 3>(k8, op, nb, x, nv, acc);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       const float rc = acc[c] - diag * x[c * nv + i];
       r[c * nv + i] = rc;
-      const double bc = b[c * nv + i];
+      const double bc = bp[c];
       v[c] += bc * bc;
       v[3 + c] += double(rc) * rc;
     }
@@ -243,7 +261,8 @@ __device__ __forceinline__ void apply_dot_body(const Dims& d, const float* __res
   const size_t nv = d.nv();
   double v[3] = {0, 0, 0};
   for (size_t i = size_t(blk) * blockDim.x + threadIdx.x; i < nv; i += size_t(nblk) * blockDim.x) {
-    const int xx = int(i % d.nx), yy = int((i / d.nx) % d.ny), zz = int(i / (size_t(d.nx) * d.ny));
+    const Coord3 c3_ = split3(i, d.nx, d.ny);
+    const int xx = c3_.x, yy = c3_.y, zz = c3_.z;
     Nbr nb;
     nb.init(d, xx, yy, zz);
     float k8[8];
@@ -278,6 +297,61 @@ __global__ void __launch_bounds__(kBlock) k_apply_dot(Dims d, const float* __res
                                                       double* partials, SolveScalars* sc) {
   if (solve_done(sc)) return;
   apply_dot_body<kFace>(d, ks, op, p, q, partials, sc, blockIdx.x, gridDim.x);
+}
+
+// The search-direction update and the operator product in one pass:
+//   p = (z - zbar) + beta p,  q = A p = A z + beta q,  alpha = rho / (p . q).
+// A annihilates constants (periodic Laplacian), so A p follows from A z and the previous q
+// without a second gather. beta == 0 (first iteration) ignores the old p and q entirely.
+template <bool kFace>
+__global__ void __launch_bounds__(kBlock) k_update_p_apply_dot(Dims d, const float* __restrict__ ks, FineOp op,
+                                                               const float* __restrict__ z, float* p, float* q,
+                                                               double* partials, SolveScalars* sc) {
+  if (solve_done(sc)) return;
+  __shared__ double smem[32 * 3];
+  const size_t nv = d.nv();
+  float be[3], zb[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    be[c] = float(sc->beta[c]);
+    zb[c] = float(sc->zmean[c]);
+  }
+  double v[3] = {0, 0, 0};
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nv; i += size_t(gridDim.x) * blockDim.x) {
+    const Coord3 c3_ = split3(i, d.nx, d.ny);
+    const int xx = c3_.x, yy = c3_.y, zz = c3_.z;
+    Nbr nb;
+    nb.init(d, xx, yy, zz);
+    float k8[8];
+    load_k8(ks, nb, k8);
+    float acc[3] = {0.f, 0.f, 0.f};
+    const float diag = fine_offdiag<kFace, 3>(k8, op, nb, z, nv, acc);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const float zc = __ldg(z + c * nv + i);
+      const float az = diag * zc - acc[c];
+      float pc = zc - zb[c], qc = az;
+      if (be[c] != 0.f) {
+        pc += be[c] * p[c * nv + i];
+        qc += be[c] * q[c * nv + i];
+      }
+      p[c * nv + i] = pc;
+      q[c * nv + i] = qc;
+      v[c] += double(pc) * qc;
+    }
+  }
+  block_reduce_f64<3>(v, smem);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int i = 0; i < 3; i++) partials[blockIdx.x * 3 + i] = v[i];
+  if (last_block_n(&sc->counter[T_PQ], gridDim.x)) {
+    double t[3];
+    reduce_partials<3>(partials, gridDim.x, t, smem);
+    if (threadIdx.x == 0) {
+      for (int c = 0; c < 3; c++) sc->alpha[c] = t[c] != 0.0 ? sc->rz[c] / t[c] : 0.0;
+      sc->counter[T_PQ] = 0;
+    }
+  }
 }
 
 // x += alpha p, r -= alpha q, ||r||^2 -> relative residual and the done flag.
@@ -341,7 +415,8 @@ __global__ void __launch_bounds__(kBlock) k_resid_norm(Dims d, const float* __re
   const size_t nv = d.nv();
   double v[3] = {0, 0, 0};
   for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nv; i += size_t(gridDim.x) * blockDim.x) {
-    const int xx = int(i % d.nx), yy = int((i / d.nx) % d.ny), zz = int(i / (size_t(d.nx) * d.ny));
+    const Coord3 c3_ = split3(i, d.nx, d.ny);
+    const int xx = c3_.x, yy = c3_.y, zz = c3_.z;
     Nbr nb;
     nb.init(d, xx, yy, zz);
     float k8[8];
@@ -396,7 +471,8 @@ static __global__ void __launch_bounds__(kBlock) k_fine_stencil(Dims d, const fl
   const size_t nv = d.nv();
   const size_t v = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (v >= nv) return;
-  const int x = int(v % d.nx), y = int((v / d.nx) % d.ny), z = int(v / (size_t(d.nx) * d.ny));
+  const Coord3 c3_ = split3(v, d.nx, d.ny);
+    const int x = c3_.x, y = c3_.y, z = c3_.z;
   Nbr nb;
   nb.init(d, x, y, z);
   float k8[8];
@@ -428,7 +504,8 @@ __global__ void __launch_bounds__(kBlock) k_resid64(Dims d, const float* __restr
   double v[6] = {0, 0, 0, 0, 0, 0};
   double mx[3] = {0, 0, 0};
   for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nv; i += size_t(gridDim.x) * blockDim.x) {
-    const int xx = int(i % d.nx), yy = int((i / d.nx) % d.ny), zz = int(i / (size_t(d.nx) * d.ny));
+    const Coord3 c3_ = split3(i, d.nx, d.ny);
+    const int xx = c3_.x, yy = c3_.y, zz = c3_.z;
     Nbr nb;
     nb.init(d, xx, yy, zz);
     float k8[8];
@@ -708,7 +785,8 @@ static __global__ void k_coarsest_solve(int n, const double* __restrict__ Ainv, 
 __device__ __forceinline__ void elem_energy(const Dims& d, size_t e, const float* __restrict__ chi, const FineOp& op,
                                             const ElemFields& ef, float (&E)[6]) {
   const size_t nv = d.nv();
-  const int x = int(e % d.nx), y = int((e / d.nx) % d.ny), z = int(e / (size_t(d.nx) * d.ny));
+  const Coord3 c3_ = split3(e, d.nx, d.ny);
+    const int x = c3_.x, y = c3_.y, z = c3_.z;
   const int x1 = wrapm(x + 1, d.nx), y1 = wrapm(y + 1, d.ny), z1 = wrapm(z + 1, d.nz);
   const size_t r00 = (size_t(y) + size_t(d.ny) * z) * d.nx, r10 = (size_t(y1) + size_t(d.ny) * z) * d.nx;
   const size_t r01 = (size_t(y) + size_t(d.ny) * z1) * d.nx, r11 = (size_t(y1) + size_t(d.ny) * z1) * d.nx;
@@ -782,8 +860,9 @@ static __global__ void __launch_bounds__(kBlock) k_sensitivity(Dims d, const flo
   const size_t total = size_t(pitchT) * d.ny * d.nz;
   const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (t >= total) return;
-  const int x = int(t % pitchT);
-  const size_t yz = t / pitchT;
+  const unsigned yz32 = unsigned(t) / unsigned(pitchT);
+  const int x = int(unsigned(t) - yz32 * unsigned(pitchT));
+  const size_t yz = yz32;
   if (x >= d.nx) {
     sens[t] = 0.f;
     return;
