@@ -2,8 +2,8 @@
 // fused SIMP density chain and their adjoints (AutoDiff/TensorExpression.h:993-1185,
 // AutoDiff/TensorExpression.cuh:281-385).
 //
-// One thread per voxel; the (2h+1)^3 normalised weights travel as a kernel parameter
-// (constant bank, broadcast to the warp), so no device allocation or global state is used.
+// The nonzero normalised weights travel as a kernel parameter (constant bank, broadcast to the
+// warp), so no device allocation or global state is used.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -72,14 +72,36 @@ constexpr int tile_elems() {
   return (kTX + 2 * H) * (kTY + 2 * H) * (kTZ + 2 * H);
 }
 
+// The nonzero taps of a filter in the reference's order (x fastest), each with its offset in
+// the shared-memory tile: a radial kernel has many zero weights in its cube (27 of 125 taps are
+// nonzero for radius 2), and skipping them leaves every sum unchanged.
+struct TapList {
+  int n;
+  int doff[kMaxTaps];  // oz * SX * SY + oy * SX + ox for the forward direction (negated for the adjoint)
+  float w[kMaxTaps];
+};
+
+template <int H>
+static void make_taps(const ConvWeights& cw, TapList* tl) {
+  constexpr int SX = kTX + 2 * H, SY = kTY + 2 * H, W1 = 2 * H + 1;
+  tl->n = 0;
+  for (int t = 0; t < cw.taps; t++) {
+    if (cw.w[t] == 0.f) continue;
+    const int ox = t % W1 - H, oy = t / W1 % W1 - H, oz = t / (W1 * W1) - H;
+    tl->doff[tl->n] = oz * SX * SY + oy * SX + ox;
+    tl->w[tl->n] = cw.w[t];
+    tl->n++;
+  }
+}
+
 template <int H, int MODE>
 __global__ void __launch_bounds__(256) k_conv_tiled(Dims d, const float* __restrict__ src, int src_pitch,
                                                     const float* __restrict__ dk_in, const float* __restrict__ ws_in,
                                                     float* __restrict__ dst, int dst_pitch,
-                                                    float* __restrict__ ws_out, int periodic, ConvWeights cw,
+                                                    float* __restrict__ ws_out, int periodic, TapList tl,
                                                     float wsum_all, float p, float k0, float kmin,
                                                     float* __restrict__ kout, float* __restrict__ dkout) {
-  constexpr int SX = kTX + 2 * H, SY = kTY + 2 * H, SZ = kTZ + 2 * H, W1 = 2 * H + 1;
+  constexpr int SX = kTX + 2 * H, SY = kTY + 2 * H, SZ = kTZ + 2 * H;
   constexpr bool kFwd = MODE < 2;
   extern __shared__ float sm[];
   float* val = sm;
@@ -92,9 +114,9 @@ __global__ void __launch_bounds__(256) k_conv_tiled(Dims d, const float* __restr
     const bool in = gx >= 0 && gx < d.nx && gy >= 0 && gy < d.ny && gz >= 0 && gz < d.nz;
     float v = 0.f, m = 0.f;
     if (in || periodic) {
-      gx = ((gx % d.nx) + d.nx) % d.nx;
-      gy = ((gy % d.ny) + d.ny) % d.ny;
-      gz = ((gz % d.nz) + d.nz) % d.nz;
+      if (gx < 0 || gx >= d.nx) gx = ((gx % d.nx) + d.nx) % d.nx;
+      if (gy < 0 || gy >= d.ny) gy = ((gy % d.ny) + d.ny) % d.ny;
+      if (gz < 0 || gz >= d.nz) gz = ((gz % d.nz) + d.nz) % d.nz;
       const size_t row = size_t(gy) + size_t(d.ny) * gz;
       v = __ldg(src + row * src_pitch + gx);
       if (!kFwd) {
@@ -115,20 +137,14 @@ __global__ void __launch_bounds__(256) k_conv_tiled(Dims d, const float* __restr
     const int gz = z0 + tz;
     if (gz >= d.nz) break;
     float sum = 0.f, ws = 0.f;
-    // full unrolling (compile-time weight offsets) for the common radii, loops beyond
-    constexpr int UR = H <= 3 ? W1 : 1;
-#pragma unroll UR
-    for (int oz = -H; oz <= H; oz++)
-#pragma unroll UR
-      for (int oy = -H; oy <= H; oy++)
-#pragma unroll UR
-        for (int ox = -H; ox <= H; ox++) {
-          const float w = cw.w[(oz + H) * W1 * W1 + (oy + H) * W1 + (ox + H)];
-          const int sx = kFwd ? ox : -ox, sy = kFwd ? oy : -oy, sz = kFwd ? oz : -oz;
-          const int li = (tz + H + sz) * SX * SY + (threadIdx.y + H + sy) * SX + (threadIdx.x + H + sx);
-          sum += w * val[li];
-          if (kFwd && !periodic) ws += w * msk[li];
-        }
+    const int base = (tz + H) * SX * SY + (threadIdx.y + H) * SX + (threadIdx.x + H);
+#pragma unroll 4
+    for (int t = 0; t < tl.n; t++) {
+      const float w = tl.w[t];
+      const int li = base + (kFwd ? tl.doff[t] : -tl.doff[t]);
+      sum += w * val[li];
+      if (kFwd && !periodic) ws += w * msk[li];
+    }
     const size_t row = size_t(gy) + size_t(d.ny) * gz;
     if (kFwd) {
       if (periodic) ws = wsum_all;
@@ -159,8 +175,10 @@ static otm_status launch_tiled(const Dims& d, const float* src, int src_pitch, c
     attr = true;
   }
   dim3 grid((d.nx + kTX - 1) / kTX, (d.ny + kTY - 1) / kTY, (d.nz + kTZ - 1) / kTZ);
+  TapList tl;
+  make_taps<H>(cw, &tl);
   k_conv_tiled<H, MODE><<<grid, dim3(kTX, kTY), smem, s>>>(d, src, src_pitch, dk_in, ws_in, dst, dst_pitch, ws_out,
-                                                          periodic, cw, wsum_all, p, k0, kmin, kout, dkout);
+                                                          periodic, tl, wsum_all, p, k0, kmin, kout, dkout);
   OTM_CHECK_LAUNCH("k_conv_tiled");
   count_launches(1);
   return OTM_OK;

@@ -305,8 +305,9 @@ __global__ void __launch_bounds__(kBlock) k_apply_dot(Dims d, const float* __res
 // without a second gather. beta == 0 (first iteration) ignores the old p and q entirely.
 template <bool kFace>
 __global__ void __launch_bounds__(kBlock) k_update_p_apply_dot(Dims d, const float* __restrict__ ks, FineOp op,
-                                                               const float* __restrict__ z, float* p, float* q,
-                                                               double* partials, SolveScalars* sc) {
+                                                               const float* __restrict__ z, float* __restrict__ p,
+                                                               float* __restrict__ q, double* partials,
+                                                               SolveScalars* sc) {
   if (solve_done(sc)) return;
   __shared__ double smem[32 * 3];
   const size_t nv = d.nv();
@@ -326,14 +327,20 @@ __global__ void __launch_bounds__(kBlock) k_update_p_apply_dot(Dims d, const flo
     load_k8(ks, nb, k8);
     float acc[3] = {0.f, 0.f, 0.f};
     const float diag = fine_offdiag<kFace, 3>(k8, op, nb, z, nv, acc);
+    float po[3], qo[3];  // all loads of the vertex before its stores
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      po[c] = be[c] != 0.f ? p[c * nv + i] : 0.f;
+      qo[c] = be[c] != 0.f ? q[c * nv + i] : 0.f;
+    }
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       const float zc = __ldg(z + c * nv + i);
       const float az = diag * zc - acc[c];
       float pc = zc - zb[c], qc = az;
       if (be[c] != 0.f) {
-        pc += be[c] * p[c * nv + i];
-        qc += be[c] * q[c * nv + i];
+        pc += be[c] * po[c];
+        qc += be[c] * qo[c];
       }
       p[c * nv + i] = pc;
       q[c * nv + i] = qc;
@@ -355,7 +362,8 @@ __global__ void __launch_bounds__(kBlock) k_update_p_apply_dot(Dims d, const flo
 }
 
 // x += alpha p, r -= alpha q, ||r||^2 -> relative residual and the done flag.
-__device__ __forceinline__ void update_xr_body(size_t nv, float* x, float* r, const float* __restrict__ p,
+__device__ __forceinline__ void update_xr_body(size_t nv, float* __restrict__ x, float* __restrict__ r,
+                                               const float* __restrict__ p,
                                                const float* __restrict__ q, double* partials, SolveScalars* sc,
                                                int max_iter, unsigned int blk, unsigned int nblk) {
   __shared__ double smem[32 * 3];
