@@ -79,14 +79,20 @@ __device__ __forceinline__ void reduce_to_result(double (&s)[NS], double (&mx)[N
     for (int i = 0; i < NM; i++) partials[blockIdx.x * W + NS + i] = mx[i];
   }
   if (last_block(counter)) {
-    if (threadIdx.x < W) {
-      const int i = threadIdx.x;
+    // one warp per value: lanes stride over the blocks, then a shuffle reduction (fixed order)
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int i = warp; i < W; i += int(blockDim.x >> 5)) {
       double acc = i < NS ? 0.0 : -1e300;
-      for (int b = 0; b < int(gridDim.x); b++) {
+      for (int b = lane; b < int(gridDim.x); b += 32) {
         const double v = ((volatile double*)partials)[b * W + i];
         acc = i < NS ? acc + v : fmax(acc, v);
       }
-      result[i] = acc;
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const double o = __shfl_xor_sync(0xffffffffu, acc, off);
+        acc = i < NS ? acc + o : fmax(acc, o);
+      }
+      if (lane == 0) result[i] = acc;
     }
     __syncthreads();
     if (threadIdx.x == 0) *counter = 0;

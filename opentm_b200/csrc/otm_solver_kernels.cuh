@@ -578,13 +578,32 @@ __global__ void __launch_bounds__(kBlock) k_resid64(Dims d, const float* __restr
     for (int c = 0; c < 3; c++) partials[blockIdx.x * 9 + 6 + c] = mx[c];
   }
   if (last_block(&sc->counter[T_RES])) {
+    // parallel fixed-order finalisation: 6 sums and 3 maxima over the blocks' partials
+    double t[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int bq = threadIdx.x; bq < int(gridDim.x); bq += blockDim.x)
+#pragma unroll
+      for (int i = 0; i < 9; i++) {
+        const double val = ((volatile double*)partials)[bq * 9 + i];
+        t[i] = i < 6 ? t[i] + val : fmax(t[i], val);
+      }
+    double ts[6];
+#pragma unroll
+    for (int i = 0; i < 6; i++) ts[i] = t[i];
+    block_reduce_f64<6>(ts, smem);  // result in thread 0
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) t[6 + c] = fmax(t[6 + c], __shfl_down_sync(0xffffffffu, t[6 + c], off));
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0)
+#pragma unroll
+      for (int c = 0; c < 3; c++) smx[(threadIdx.x >> 5) * 3 + c] = t[6 + c];
+    __syncthreads();
     if (threadIdx.x == 0) {
-      double t[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-      for (int bq = 0; bq < int(gridDim.x); bq++)
-        for (int i = 0; i < 9; i++) {
-          const double val = ((volatile double*)partials)[bq * 9 + i];
-          t[i] = i < 6 ? t[i] + val : fmax(t[i], val);
-        }
+      for (int w = 1; w < int(blockDim.x + 31) / 32; w++)
+        for (int c = 0; c < 3; c++) t[6 + c] = fmax(t[6 + c], smx[w * 3 + c]);
+#pragma unroll
+      for (int i = 0; i < 6; i++) t[i] = ts[i];
       const double kmax = double(__uint_as_float(*kmax_bits));
       bool all = true, bad = false;
       if (init) {
