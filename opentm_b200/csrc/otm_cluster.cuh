@@ -361,6 +361,7 @@ __device__ __forceinline__ void cl_prolong(const ClLevel& F, const ClLevel& C, f
 
 static __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads)
     k_vcycle_cluster(ClDesc cdp, const SolveScalars* sc) {
+  pdl_wait();
   // every CTA reads the same flag (written by earlier kernels), so the whole cluster leaves
   // together before any distributed shared memory access
   if (sc && solve_done(sc)) return;

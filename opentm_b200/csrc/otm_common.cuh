@@ -51,6 +51,12 @@ struct Dims {
   __host__ __device__ size_t nv() const { return size_t(nx) * ny * nz; }
 };
 
+// Programmatic dependent launch: waits until the grids this launch depends on have completed
+// and their memory is visible. A kernel launched with the programmatic-serialization attribute
+// may start while its predecessor drains, so this must come before any read of data that the
+// predecessor writes; for a launch without the attribute it returns at once.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // (x, y, z) of lexicographic index v (x fastest) on a grid with rows of nx and planes of
 // nx * ny points. Grids hold at most 1024^3 = 2^30 points, so 32-bit division is exact and
 // several times cheaper than 64-bit.

@@ -57,6 +57,24 @@ static std::vector<Dims> level_dims(const int reso[3], int coarsest_max_dof) {
   return out;
 }
 
+// Launch with programmatic stream serialization: the kernel may be scheduled while its
+// predecessor drains and waits for it in pdl_wait() (every kernel launched this way starts with
+// it). Inside a stream capture the dependency becomes a programmatic graph edge.
+template <typename... KArgs, typename... Args>
+static void launch_pdl(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t lc{};
+  lc.gridDim = grid;
+  lc.blockDim = block;
+  lc.dynamicSmemBytes = smem;
+  lc.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  lc.attrs = at;
+  lc.numAttrs = 1;
+  cudaLaunchKernelEx(&lc, k, static_cast<KArgs>(args)...);
+}
+
 static constexpr int kMaxCoarsest = 1024;
 
 static bool mixed_supported() { return true; }
@@ -390,11 +408,13 @@ void Homo::gs(int l, int color) {
   }
   if (l == 0) {
     if (face)
-      k_gs_fine<true, 3><<<ceil_div(nsub, kBlock), kBlock, 0, stream>>>(L.d, color, ks, op, L.u, L.f, sc);
+      launch_pdl(k_gs_fine<true, 3>, dim3(ceil_div(nsub, kBlock)), dim3(kBlock), 0, stream, L.d, color, ks, op, L.u, L.f,
+                 sc, nullptr);
     else  // color is a colour pair (0..3)
-      k_gs_fine_pair<3><<<ceil_div(nsub, kBlock), kBlock, 0, stream>>>(L.d, color, ks, op, L.u, L.f, sc);
+      launch_pdl(k_gs_fine_pair<3>, dim3(ceil_div(nsub, kBlock)), dim3(kBlock), 0, stream, L.d, color, ks, op, L.u,
+                 L.f, sc, nullptr);
   } else {
-    k_gs_coarse<3><<<ceil_div(nsub, kBlock), kBlock, 0, stream>>>(L.d, color, L.st, L.u, L.f, sc);
+    launch_pdl(k_gs_coarse<3>, dim3(ceil_div(nsub, kBlock)), dim3(kBlock), 0, stream, L.d, color, L.st, L.u, L.f, sc);
   }
   launched(1);
 }
@@ -406,7 +426,7 @@ void Homo::vcycle(int l) {
     ClDesc cd = cl_desc;
     cd.f_in = L.f;
     cd.u_out = L.u;
-    k_vcycle_cluster<<<kCl, kClThreads, cluster_smem, stream>>>(cd, sc);
+    launch_pdl(k_vcycle_cluster, dim3(kCl), dim3(kClThreads), cluster_smem, stream, cd, sc);
     launched(1);
     return;
   }
@@ -426,12 +446,12 @@ void Homo::vcycle(int l) {
     td.f_in = L.f;
     td.u_out = L.u;
     td.Ainv = Ainv;
-    k_vcycle_tail<<<1, kTailThreads, tail_smem, stream>>>(td, sc);
+    launch_pdl(k_vcycle_tail, dim3(1), dim3(kTailThreads), tail_smem, stream, td, sc);
     launched(1);
     return;
   }
   if (l == int(lv.size()) - 1) {
-    k_coarsest_solve<<<1, std::min(1024, std::max(32, (nc + 31) / 32 * 32)), 3 * nc * sizeof(double), stream>>>(
+    launch_pdl(k_coarsest_solve, dim3(1), dim3(std::min(1024, std::max(32, (nc + 31) / 32 * 32))), 3 * nc * sizeof(double), stream, 
         nc, Ainv, L.f, L.u, sc);
     launched(1);
     return;
@@ -464,13 +484,15 @@ void Homo::vcycle(int l) {
   } else {
     if (l == 0) {
       if (face)
-        k_resid_fine<true, 3><<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(L.d, ks, op, L.u, L.f, L.r, sc);
+        launch_pdl(k_resid_fine<true, 3>, dim3(ceil_div(nv, kBlock)), dim3(kBlock), 0, stream, L.d, ks, op, L.u, L.f,
+                   L.r, sc, nullptr);
       else
-        k_resid_fine<false, 3><<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(L.d, ks, op, L.u, L.f, L.r, sc);
+        launch_pdl(k_resid_fine<false, 3>, dim3(ceil_div(nv, kBlock)), dim3(kBlock), 0, stream, L.d, ks, op, L.u, L.f,
+                   L.r, sc, nullptr);
     } else {
-      k_resid_coarse<3><<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(L.d, L.st, L.u, L.f, L.r, sc);
+      launch_pdl(k_resid_coarse<3>, dim3(ceil_div(nv, kBlock)), dim3(kBlock), 0, stream, L.d, L.st, L.u, L.f, L.r, sc);
     }
-    k_restrict<3><<<ceil_div(C.d.nv(), kBlock), kBlock, 0, stream>>>(L.d, C.d, L.r, C.f, sc);
+    launch_pdl(k_restrict<3>, dim3(ceil_div(C.d.nv(), kBlock)), dim3(kBlock), 0, stream, L.d, C.d, L.r, C.f, sc);
     launched(2);  // residual + restriction
   }
   vcycle(l + 1);
@@ -480,7 +502,7 @@ void Homo::vcycle(int l) {
     else
       fine_ops16<__half>(3, 0);
   } else {
-    k_prolong<3><<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(L.d, C.d, C.u, L.u, sc);
+    launch_pdl(k_prolong<3>, dim3(ceil_div(nv, kBlock)), dim3(kBlock), 0, stream, L.d, C.d, C.u, L.u, sc);
     launched(1);
   }
   for (int s = 0; s < cfg.post_smooth; s++)
@@ -498,31 +520,31 @@ void Homo::iteration(int j) {
     // FP64 refinement step: residual, one 16-bit V-cycle on the scaled residual, update
     const unsigned int* kmax_bits = (const unsigned int*)(flags + 2);
     if (face)
-      k_resid64<true><<<nb, kBlock, 0, stream>>>(d0, ks, op, x64, b, r, partials, sc, kmax_bits, cfg.max_iter, 0);
+      launch_pdl(k_resid64<true>, dim3(nb), dim3(kBlock), 0, stream, d0, ks, op, x64, b, r, partials, sc, kmax_bits, cfg.max_iter, 0);
     else
-      k_resid64<false><<<nb, kBlock, 0, stream>>>(d0, ks, op, x64, b, r, partials, sc, kmax_bits, cfg.max_iter, 0);
+      launch_pdl(k_resid64<false>, dim3(nb), dim3(kBlock), 0, stream, d0, ks, op, x64, b, r, partials, sc, kmax_bits, cfg.max_iter, 0);
     vcycle(0);
     if (cfg.precision == OTM_PRECISION_MIXED_BF16)
-      k_update64<__nv_bfloat16><<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(nv, x64, (const __nv_bfloat16*)u16, sc);
+      launch_pdl(k_update64<__nv_bfloat16>, dim3(ceil_div(nv, kBlock)), dim3(kBlock), 0, stream, nv, x64, (const __nv_bfloat16*)u16, sc);
     else
-      k_update64<__half><<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(nv, x64, (const __half*)u16, sc);
+      launch_pdl(k_update64<__half>, dim3(ceil_div(nv, kBlock)), dim3(kBlock), 0, stream, nv, x64, (const __half*)u16, sc);
     launched(2);
   } else if (cfg.solver == OTM_SOLVER_PCG) {
     vcycle(0);
-    k_dot_rz<<<nb, kBlock, 0, stream>>>(nv, r, z, partials, sc);
+    launch_pdl(k_dot_rz, dim3(nb), dim3(kBlock), 0, stream, nv, r, z, partials, sc);
     if (face)
-      k_update_p_apply_dot<true><<<nb, kBlock, 0, stream>>>(d0, ks, op, z, p, q, partials, sc);
+      launch_pdl(k_update_p_apply_dot<true>, dim3(nb), dim3(kBlock), 0, stream, d0, ks, op, z, p, q, partials, sc);
     else
-      k_update_p_apply_dot<false><<<nb, kBlock, 0, stream>>>(d0, ks, op, z, p, q, partials, sc);
-    k_update_xr<<<nb, kBlock, 0, stream>>>(nv, x, r, p, q, partials, sc, cfg.max_iter);
+      launch_pdl(k_update_p_apply_dot<false>, dim3(nb), dim3(kBlock), 0, stream, d0, ks, op, z, p, q, partials, sc);
+    launch_pdl(k_update_xr, dim3(nb), dim3(kBlock), 0, stream, nv, x, r, p, q, partials, sc, cfg.max_iter);
     launched(3);
   } else {
     if (face)
-      k_resid_norm<true><<<nb, kBlock, 0, stream>>>(d0, ks, op, x, b, r, partials, sc, cfg.max_iter);
+      launch_pdl(k_resid_norm<true>, dim3(nb), dim3(kBlock), 0, stream, d0, ks, op, x, b, r, partials, sc, cfg.max_iter);
     else
-      k_resid_norm<false><<<nb, kBlock, 0, stream>>>(d0, ks, op, x, b, r, partials, sc, cfg.max_iter);
+      launch_pdl(k_resid_norm<false>, dim3(nb), dim3(kBlock), 0, stream, d0, ks, op, x, b, r, partials, sc, cfg.max_iter);
     vcycle(0);
-    k_axpy_x<<<ceil_div(3 * nv, kBlock), kBlock, 0, stream>>>(nv, x, z, sc);
+    launch_pdl(k_axpy_x, dim3(ceil_div(3 * nv, kBlock)), dim3(kBlock), 0, stream, nv, x, z, sc);
     launched(2);
   }
 }
@@ -637,7 +659,7 @@ otm_status Homo::launch_loop() {
       if (e == cudaSuccess) {
         capturing = true;
         iteration(0);
-        k_loop_ctrl<<<1, 1, 0, stream>>>(sc, h, cfg.max_iter + 1);
+        launch_pdl(k_loop_ctrl, dim3(1), dim3(1), 0, stream, sc, h, cfg.max_iter + 1);
         capturing = false;
         cudaGraph_t out = nullptr;
         e = cudaStreamEndCapture(stream, &out);

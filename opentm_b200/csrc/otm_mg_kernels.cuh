@@ -238,6 +238,7 @@ template <bool kFace, int NC, typename KT = float, typename VT = float>
 __global__ void __launch_bounds__(kBlock) k_gs_fine(Dims d, int color, const KT* __restrict__ ks, FineOp op,
                                                      VT* u, const float* __restrict__ f, const SolveScalars* sc,
                                                      const double* fscale = nullptr) {
+  pdl_wait();
   if (sc && solve_done(sc)) return;
   gs_fine_body<kFace, NC, KT, VT>(d, color, ks, op, u, f, fscale, size_t(blockIdx.x) * blockDim.x + threadIdx.x);
 }
@@ -314,6 +315,7 @@ template <int NC, typename KT = float, typename VT = float>
 __global__ void __launch_bounds__(kBlock) k_gs_fine_pair(Dims d, int pair, const KT* __restrict__ ks, FineOp op,
                                                           VT* u, const float* __restrict__ f, const SolveScalars* sc,
                                                           const double* fscale = nullptr) {
+  pdl_wait();
   if (sc && solve_done(sc)) return;
   gs_fine_pair_body<NC, KT, VT>(d, pair, ks, op, u, f, fscale, size_t(blockIdx.x) * blockDim.x + threadIdx.x);
 }
@@ -344,6 +346,7 @@ __global__ void __launch_bounds__(kBlock) k_resid_fine(Dims d, const KT* __restr
                                                         const VT* __restrict__ u, const float* __restrict__ f,
                                                         VT* __restrict__ r, const SolveScalars* sc,
                                                         const double* fscale = nullptr) {
+  pdl_wait();
   if (sc && solve_done(sc)) return;
   resid_fine_body<kFace, NC, KT, VT>(d, ks, op, u, f, r, fscale, size_t(blockIdx.x) * blockDim.x + threadIdx.x);
 }
@@ -390,6 +393,7 @@ __device__ __forceinline__ void gs_coarse_body(const Dims& d, int color, const f
 template <int NC>
 __global__ void __launch_bounds__(kBlock) k_gs_coarse(Dims d, int color, const float* __restrict__ st, float* u,
                                                        const float* __restrict__ f, const SolveScalars* sc) {
+  pdl_wait();
   if (sc && solve_done(sc)) return;
   gs_coarse_body<NC>(d, color, st, u, f, size_t(blockIdx.x) * blockDim.x + threadIdx.x);
 }
@@ -423,6 +427,7 @@ template <int NC>
 __global__ void __launch_bounds__(kBlock) k_resid_coarse(Dims d, const float* __restrict__ st,
                                                           const float* __restrict__ u, const float* __restrict__ f,
                                                           float* __restrict__ r, const SolveScalars* sc) {
+  pdl_wait();
   if (sc && solve_done(sc)) return;
   resid_coarse_body<NC>(d, st, u, f, r, size_t(blockIdx.x) * blockDim.x + threadIdx.x);
 }
@@ -456,6 +461,7 @@ __device__ __forceinline__ void restrict_body(const Dims& df, const Dims& dc, co
 template <int NC, typename VT = float>
 __global__ void __launch_bounds__(kBlock) k_restrict(Dims df, Dims dc, const VT* __restrict__ r,
                                                       float* __restrict__ fc, const SolveScalars* sc) {
+  pdl_wait();
   if (sc && solve_done(sc)) return;
   restrict_body<NC, VT>(df, dc, r, fc, size_t(blockIdx.x) * blockDim.x + threadIdx.x);
 }
@@ -490,6 +496,7 @@ __device__ __forceinline__ void prolong_body(const Dims& df, const Dims& dc, con
 template <int NC, typename VT = float>
 __global__ void __launch_bounds__(kBlock) k_prolong(Dims df, Dims dc, const float* __restrict__ uc, VT* uf,
                                                      const SolveScalars* sc) {
+  pdl_wait();
   if (sc && solve_done(sc)) return;
   prolong_body<NC, VT>(df, dc, uc, uf, size_t(blockIdx.x) * blockDim.x + threadIdx.x);
 }

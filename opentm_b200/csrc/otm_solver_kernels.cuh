@@ -231,6 +231,7 @@ __device__ __forceinline__ void dot_rz_body(size_t nv, const float* __restrict__
 
 static __global__ void __launch_bounds__(kBlock) k_dot_rz(size_t nv, const float* __restrict__ r,
                                                    const float* __restrict__ z, double* partials, SolveScalars* sc) {
+  pdl_wait();
   if (solve_done(sc)) return;
   dot_rz_body(nv, r, z, partials, sc, blockIdx.x, gridDim.x);
 }
@@ -248,6 +249,7 @@ __device__ __forceinline__ void update_p_body(size_t nv, const float* __restrict
 
 static __global__ void __launch_bounds__(kBlock) k_update_p(size_t nv, const float* __restrict__ z, float* p,
                                                      const SolveScalars* sc) {
+  pdl_wait();
   if (solve_done(sc)) return;
   update_p_body(nv, z, p, sc, size_t(blockIdx.x) * blockDim.x + threadIdx.x);
 }
@@ -295,6 +297,7 @@ template <bool kFace>
 __global__ void __launch_bounds__(kBlock) k_apply_dot(Dims d, const float* __restrict__ ks, FineOp op,
                                                       const float* __restrict__ p, float* __restrict__ q,
                                                       double* partials, SolveScalars* sc) {
+  pdl_wait();
   if (solve_done(sc)) return;
   apply_dot_body<kFace>(d, ks, op, p, q, partials, sc, blockIdx.x, gridDim.x);
 }
@@ -308,6 +311,7 @@ __global__ void __launch_bounds__(kBlock) k_update_p_apply_dot(Dims d, const flo
                                                                const float* __restrict__ z, float* __restrict__ p,
                                                                float* __restrict__ q, double* partials,
                                                                SolveScalars* sc) {
+  pdl_wait();
   if (solve_done(sc)) return;
   __shared__ double smem[32 * 3];
   const size_t nv = d.nv();
@@ -407,6 +411,7 @@ __device__ __forceinline__ void update_xr_body(size_t nv, float* __restrict__ x,
 static __global__ void __launch_bounds__(kBlock) k_update_xr(size_t nv, float* x, float* r, const float* __restrict__ p,
                                                       const float* __restrict__ q, double* partials,
                                                       SolveScalars* sc, int max_iter) {
+  pdl_wait();
   if (solve_done(sc)) return;
   update_xr_body(nv, x, r, p, q, partials, sc, max_iter, blockIdx.x, gridDim.x);
 }
@@ -418,6 +423,7 @@ __global__ void __launch_bounds__(kBlock) k_resid_norm(Dims d, const float* __re
                                                        const float* __restrict__ x, const float* __restrict__ b,
                                                        float* __restrict__ r, double* partials, SolveScalars* sc,
                                                        int max_iter) {
+  pdl_wait();
   if (solve_done(sc)) return;
   __shared__ double smem[32 * 3];
   const size_t nv = d.nv();
@@ -465,6 +471,7 @@ __global__ void __launch_bounds__(kBlock) k_resid_norm(Dims d, const float* __re
 
 static __global__ void __launch_bounds__(kBlock) k_axpy_x(size_t nv, float* x, const float* __restrict__ z,
                                                    SolveScalars* sc) {
+  pdl_wait();
   if (solve_done(sc)) return;
   const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i < 3 * nv) x[i] += z[i];
@@ -506,6 +513,7 @@ __global__ void __launch_bounds__(kBlock) k_resid64(Dims d, const float* __restr
                                                     const double* __restrict__ x64, const float* __restrict__ b,
                                                     float* __restrict__ f, double* partials, SolveScalars* sc,
                                                     const unsigned int* kmax_bits, int max_iter, int init) {
+  pdl_wait();
   if (!init && solve_done(sc)) return;
   __shared__ double smem[32 * 6];
   const size_t nv = d.nv();
@@ -632,6 +640,7 @@ __global__ void __launch_bounds__(kBlock) k_resid64(Dims d, const float* __restr
 template <typename VT>
 __global__ void __launch_bounds__(kBlock) k_update64(size_t nv, double* x64, const VT* __restrict__ u,
                                                      SolveScalars* sc) {
+  pdl_wait();
   if (solve_done(sc)) return;
   const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i < nv) {
@@ -662,6 +671,7 @@ static __global__ void k_loop_start(SolveScalars* sc, cudaGraphConditionalHandle
 }
 
 static __global__ void k_loop_ctrl(SolveScalars* sc, cudaGraphConditionalHandle h, int cap) {
+  pdl_wait();
   const int l = sc->loop + 1;
   sc->loop = l;
   cudaGraphSetConditional(h, (!sc->done && !sc->nan && l < cap) ? 1u : 0u);
@@ -779,6 +789,7 @@ static __global__ void __launch_bounds__(1024) k_coarsest_build(Dims d, const fl
 // u = Ainv (f - mean f) for the 3 cases (one block).
 static __global__ void k_coarsest_solve(int n, const double* __restrict__ Ainv, const float* __restrict__ f, float* u,
                                  const SolveScalars* sc) {
+  pdl_wait();
   if (sc && solve_done(sc)) return;
   extern __shared__ double bsh[];  // 3 * n
   __shared__ double mean[3];

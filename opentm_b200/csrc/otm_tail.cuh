@@ -209,6 +209,7 @@ __device__ __forceinline__ void vcycle_tail_body(const TailDesc& td, float* sm) 
 }
 
 static __global__ void __launch_bounds__(kTailThreads) k_vcycle_tail(TailDesc td, const SolveScalars* sc) {
+  pdl_wait();
   if (sc && solve_done(sc)) return;
   extern __shared__ float sm[];
   vcycle_tail_body(td, sm);
