@@ -402,8 +402,9 @@ static __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads)
   }
   // first level: zero correction (ghosts included); stencils of the other smoothed levels
   cl_zero_u(cd.lv[0], sm, rank);
-  for (int l = 1; l < L - 1; l++) {
+  for (int l = 0; l < L - 1; l++) {
     const ClLevel& V = cd.lv[l];
+    if (V.st_off < 0) continue;
     const int nx = V.d.nx, pl = nx * V.d.ny, z0 = V.zstart[rank];
     const int n = (V.zstart[rank + 1] - z0) * pl;
     const size_t nv = V.d.nv();
@@ -489,7 +490,8 @@ inline int cl_log2_ceil(int v) {
   return l;
 }
 
-inline size_t cl_plan(const Dims* dims, int n, ClDesc* cd) {
+// first_smem: the first level's stencils and residual also live in shared memory.
+inline size_t cl_plan_try(const Dims* dims, int n, ClDesc* cd, bool first_smem) {
   if (n < 2 || n > kClMaxLevels) return 0;
   if (dims[0].nv() > size_t(kClMaxNv)) return 0;
   int off = 0, tab = 0;
@@ -507,9 +509,10 @@ inline size_t cl_plan(const Dims* dims, int n, ClDesc* cd) {
     V.cs = maxpl * plane;
     // u strides: padded on the lane-team levels so that a round of team reads is free of bank
     // conflicts (smallest plane stride among the best), plain on the first level
+    const bool smem_st = l < n - 1 && (l > 0 || first_smem);
     V.urs = d.nx;
     V.ups = plane;
-    if (l > 0 && l < n - 1) {
+    if (smem_st) {
       int best = cl_team_conflicts(V.urs, V.ups);
       for (int px = 0; px <= 32 && best > 1; px++)
         for (int py = 0; py < 64; py++) {
@@ -531,7 +534,7 @@ inline size_t cl_plan(const Dims* dims, int n, ClDesc* cd) {
       off += 3 * V.cs;
     }
     V.r_off = V.st_off = V.inv_off = -1;
-    if (l > 0 && l < n - 1) {
+    if (smem_st) {
       V.r_off = off;
       off += 3 * V.cs;
       V.st_off = off;
@@ -558,6 +561,13 @@ inline size_t cl_plan(const Dims* dims, int n, ClDesc* cd) {
   const size_t bytes = size_t(off) * sizeof(float);
   if (bytes > size_t(kMaxDynSmem)) return 0;
   return bytes;
+}
+
+// Host-side layout of the cluster part (see cl_plan_try): the first level's stencils in shared
+// memory when everything fits, else in global memory.
+inline size_t cl_plan(const Dims* dims, int n, ClDesc* cd) {
+  const size_t b = cl_plan_try(dims, n, cd, true);
+  return b ? b : cl_plan_try(dims, n, cd, false);
 }
 
 }  // namespace otm
