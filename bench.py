@@ -439,6 +439,121 @@ def serve_once(args, fields, rate, serial_rate):
             "gpu_launches": int(launch_count() - l0)}
 
 
+# ---------------------------------------------------------------------------------------
+# Configuration 3: one 256^3 solve in FP32 and in the two 16-bit forms, against the FP64 oracle
+# ---------------------------------------------------------------------------------------
+def run_solve256(args):
+    import torch
+
+    import oracle as ora
+    from opentm_b200 import HomoConfig, Homogenization_H
+    from opentm_b200 import workloads as wl
+
+    torch.cuda.set_device(0)
+    n = 256 if args.n == N_CELL else args.n
+    k = wl.simp(wl.config3_density(n, seed=2))
+    kd = torch.from_numpy(k).cuda()
+    dC = -np.eye(3)
+    res = {}
+    for prec in ("fp32", "bf16", "fp16"):
+        H = Homogenization_H(HomoConfig(reso=n, femRelThres=TOL, pre_smooth=2, post_smooth=2, precision=prec,
+                                        warm_start=False, max_iter=200))
+        sens = torch.empty_like(kd)
+        H.update(kd)
+        H.heatMatrix()  # builds the solve graph
+        lat = []
+        for _ in range(max(1, args.steps)):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            H.update(kd)
+            C = H.heatMatrix()
+            H.Sensitivity(dC, sens)
+            e1.record()
+            e1.synchronize()
+            lat.append(e0.elapsed_time(e1))
+        st = H.stats()
+        res[prec] = {"ms": float(np.median(lat)), "C": C, "sens": sens.cpu().numpy(), "iterations": st.iterations,
+                     "rel_res": max(st.rel_res)}
+        del H
+    ora.build()
+    t = time.perf_counter()
+    ref = ora.homogenize(k.astype(np.float64), tol=1e-10, want_energy=True)
+    s_ref = ora.sensitivity(ref["energy"], k.astype(np.float64), dC)
+    t_ora = time.perf_counter() - t
+    out = {}
+    for prec, r in res.items():
+        kh = float(np.abs(r["C"] - ref["C"]).max() / np.abs(ref["C"]).max())
+        se = float(np.abs(r["sens"] - s_ref).max() / np.abs(s_ref).max())
+        out[prec] = {"solve_ms": round(r["ms"], 3), "solves_per_s": round(1e3 / r["ms"], 3), "kh_err": kh,
+                     "sens_err": se, "iterations": r["iterations"], "rel_res": r["rel_res"]}
+    line = {"metric": "256^3 solve: ms per solve (update + 3 load cases + K^H + sensitivity), error vs FP64 oracle",
+            "value": out["bf16"]["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "steps": args.steps,
+            "higher_is_better": True, "dtype": "bf16+f64 refinement", "data": "synthetic",
+            "config": {"workload": f"configuration 3: {n}^3 thresholded smoothed Gaussian field (seed 2), SIMP p=3, "
+                                   f"cold solve to rel.res {TOL}, V(2,2), coarsest FP64 direct", "reso": n},
+            "forms": out, "oracle_seconds": round(t_ora, 1)}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------
+# Configuration 4: MMA loop on a 384^3 cell (16-bit fine levels, FP64 MMA on the device)
+# ---------------------------------------------------------------------------------------
+def run_mma384(args):
+    import torch
+
+    from opentm_b200 import DensityFilter, HomoConfig, Homogenization_H, MMAOptimizer
+    from opentm_b200 import workloads as wl
+
+    torch.cuda.set_device(0)
+    n = 384 if args.n == N_CELL else args.n
+    ne = n ** 3
+    rho = torch.from_numpy(wl.config4_density(n, seed=3)).cuda()
+    H = Homogenization_H(HomoConfig(reso=n, femRelThres=TOL, pre_smooth=2, post_smooth=2, precision="bf16"))
+    df = DensityFilter((n, n, n), FILTER_R, 1, True, P_SIMP, K0, KMIN)
+    mma = MMAOptimizer(2, ne, 1.0, 0.0, 1000.0, 0.0)
+    mma.setBound(0.001, 1.0)
+    g_k = torch.empty_like(rho)
+    dfdx, dg0, dg1 = torch.empty_like(rho), torch.full_like(rho, 1.0 / (0.25 * ne)), torch.empty_like(rho)
+    e = [np.zeros((3, 3)) for _ in range(3)]
+    for i in range(3):
+        e[i][i, i] = 1.0
+    iso_eps = 1e-3
+    lat, C = [], None
+    iters = max(args.steps, 1)
+    for it in range(args.warmup + iters):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        k = df.forward(rho)
+        H.update(k)
+        C = H.heatMatrix()
+        H.Sensitivity(-e[0], g_k)  # objective -K_xx
+        df.backward(g_k, dfdx)
+        a, b = C[0, 0] - C[1, 1], C[1, 1] - C[2, 2]
+        dC = (np.sign(a) * (e[0] - e[1]) + np.sign(b) * (e[1] - e[2])) / iso_eps
+        H.Sensitivity(dC, g_k)
+        df.backward(g_k, dg1)
+        g = [float(rho.mean().item()) / 0.25 - 1.0, (abs(a) + abs(b)) / iso_eps - 1.0]
+        mma.update(it + 1, rho, dfdx, g, [dg0, dg1])
+        e1.record()
+        e1.synchronize()
+        if it >= args.warmup:
+            lat.append(e0.elapsed_time(e1))
+    ms = float(np.mean(lat))
+    line = {"metric": "384^3 MMA loop: iterations/s (filter, bf16 solve of 3 load cases, K^H, 2 sensitivities, "
+                      "filter adjoints, FP64 MMA update)",
+            "value": round(1e3 / ms, 4), "unit": "iterations/s", "n_gpus": 1, "steps": iters, "warmup": args.warmup,
+            "ms_per_step": round(ms, 3), "p50_ms": round(float(np.percentile(lat, 50)), 3),
+            "p99_ms": round(float(np.percentile(lat, 99)), 3), "higher_is_better": True, "dtype": "bf16+f64",
+            "data": "synthetic",
+            "config": {"workload": f"configuration 4: {n}^3, max K_xx s.t. volume 0.25 and isotropy "
+                                   f"|Kxx-Kyy|+|Kyy-Kzz| <= {iso_eps}, rho0 = 0.25 + 0.02 U(-1,1) seed 3", "reso": n},
+            "final_KH_diag": [float(C[i, i]) for i in range(3)], "final_volume": float(rho.mean().item()),
+            "solve_iterations_last": H.stats().iterations}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -448,7 +563,7 @@ def main():
     ap.add_argument("--n", type=int, default=N_CELL)
     ap.add_argument("--mixed", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="oc", choices=["oc", "serve"])
+    ap.add_argument("--workload", default="oc", choices=["oc", "serve", "solve256", "mma384"])
     ap.add_argument("--requests", type=int, default=2000)
     ap.add_argument("--rate", type=float, default=0.0, help="Poisson rate; 0 sweeps 50..2000 req/s")
     ap.add_argument("--max-active", type=int, default=64)
@@ -456,6 +571,12 @@ def main():
     args = ap.parse_args()
     if args.workload == "serve":
         run_serve(args)
+        return
+    if args.workload == "solve256":
+        run_solve256(args)
+        return
+    if args.workload == "mma384":
+        run_mma384(args)
         return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -199,11 +199,10 @@ otm_status Homo::build(const otm_config& c, cudaStream_t ext_stream, cudaMemPool
     OTM_TRY(alloc(&r16, 3 * nv * 2));
     OTM_CUDA(cudaMemsetAsync(x64, 0, 3 * nv * sizeof(double), stream));
     OTM_CUDA(cudaMemsetAsync(u16, 0, 3 * nv * 2, stream));
-  } else {
-    OTM_TRY(alloc((void**)&p, 3 * nv * sizeof(float)));
-    OTM_TRY(alloc((void**)&q, 3 * nv * sizeof(float)));
-    OTM_CUDA(cudaMemsetAsync(p, 0, 3 * nv * sizeof(float), stream));
   }
+  OTM_TRY(alloc((void**)&p, 3 * nv * sizeof(float)));
+  OTM_TRY(alloc((void**)&q, 3 * nv * sizeof(float)));
+  OTM_CUDA(cudaMemsetAsync(p, 0, 3 * nv * sizeof(float), stream));
   nc = int(lv.back().d.nv());
   OTM_TRY(alloc((void**)&Ainv, size_t(nc) * nc * sizeof(double)));
   OTM_TRY(alloc((void**)&table, 64 * 27 * sizeof(float)));
@@ -516,7 +515,32 @@ void Homo::iteration(int j) {
   const int nb = reduce_blocks(nv);
   float* r = lv[0].f;  // Krylov residual is the V-cycle's level-0 right-hand side
   float* z = lv[0].u;  // and the V-cycle's level-0 result is the preconditioned residual
-  if (mixed) {
+  if (mixed && cfg.solver == OTM_SOLVER_PCG) {
+    // PCG with the 16-bit V-cycle as preconditioner, the solution in FP64 and exact FP64
+    // residual replacements (k_update_x64r requests them, k_resid64 mode 2 performs them)
+    const unsigned int* kmax_bits = (const unsigned int*)(flags + 2);
+    vcycle(0);
+    float* zf = x;  // the FP32 solution buffer holds z during a mixed solve
+    if (cfg.precision == OTM_PRECISION_MIXED_BF16)
+      launch_pdl(k_z16<__nv_bfloat16>, dim3(ceil_div(nv, kBlock)), dim3(kBlock), 0, stream, nv,
+                 (const __nv_bfloat16*)u16, zf, sc);
+    else
+      launch_pdl(k_z16<__half>, dim3(ceil_div(nv, kBlock)), dim3(kBlock), 0, stream, nv, (const __half*)u16, zf, sc);
+    launch_pdl(k_dot_rz, dim3(nb), dim3(kBlock), 0, stream, nv, r, zf, partials, sc);
+    if (face)
+      launch_pdl(k_update_p_apply_dot<true>, dim3(nb), dim3(kBlock), 0, stream, d0, ks, op, zf, p, q, partials, sc);
+    else
+      launch_pdl(k_update_p_apply_dot<false>, dim3(nb), dim3(kBlock), 0, stream, d0, ks, op, zf, p, q, partials, sc);
+    launch_pdl(k_update_x64r, dim3(nb), dim3(kBlock), 0, stream, nv, x64, r, p, q, partials, sc, kmax_bits, op.c0,
+               cfg.max_iter);
+    if (face)
+      launch_pdl(k_resid64<true>, dim3(nb), dim3(kBlock), 0, stream, d0, ks, op, x64, b, r, partials, sc, kmax_bits,
+                 cfg.max_iter, 2);
+    else
+      launch_pdl(k_resid64<false>, dim3(nb), dim3(kBlock), 0, stream, d0, ks, op, x64, b, r, partials, sc, kmax_bits,
+                 cfg.max_iter, 2);
+    launched(5);
+  } else if (mixed) {
     // FP64 refinement step: residual, one 16-bit V-cycle on the scaled residual, update
     const unsigned int* kmax_bits = (const unsigned int*)(flags + 2);
     if (face)
@@ -776,7 +800,7 @@ otm_status Homo::solve_impl(bool with_heat) {
       }
     }
     stats.iterations = sc_host->iter;
-    stats.refinements = mixed ? sc_host->iter : 0;
+    stats.refinements = mixed ? (cfg.solver == OTM_SOLVER_PCG ? sc_host->nrepl : sc_host->iter) : 0;
     for (int c = 0; c < 3; c++) stats.rel_res[c] = sc_host->relres[c];
     if (!sc_host->nan) break;
     // "numerical explode, resetting initial guess" (homogenization/MG.cpp:392-423): one

@@ -45,6 +45,10 @@ struct SolveScalars {
   double fscale[3];
   double xscale[3];
   int loop;  // bodies run by the device-side solve loop of the current solve
+  // mixed-precision PCG: exact FP64 residual replacements
+  double rr_repl[3];  // ||r||^2 at the last replacement
+  int repl;           // 1: the next replacement kernel recomputes r = b - A x64
+  int nrepl;          // replacements (FP64 residuals) of the current solve
 };
 
 // Dynamic shared memory limit every large-shared-memory kernel is opted in to. It is one fixed
