@@ -45,8 +45,9 @@ typedef enum otm_status {
 
 typedef enum otm_precision {
   OTM_PRECISION_FP32 = 0,       /* plain FP32 multigrid: the drop-in */
-  OTM_PRECISION_MIXED_BF16 = 1, /* BF16 fine-level storage, FP32 smoothing, FP64 refinement */
-  OTM_PRECISION_MIXED_FP16 = 2  /* FP16 fine-level storage, FP32 smoothing, FP64 refinement */
+  OTM_PRECISION_MIXED_BF16 = 1, /* BF16 fine-level storage in the V-cycle, FP32 smoothing arithmetic,
+                                   FP64 solution and exact FP64 residuals */
+  OTM_PRECISION_MIXED_FP16 = 2  /* the same with FP16 storage (residual scaled to max 1) */
 } otm_precision;
 
 typedef enum otm_solver {
@@ -77,7 +78,9 @@ typedef struct otm_config {
 
 typedef struct otm_solve_stats {
   int iterations;         /* PCG iterations or V-cycles of the last solve (all 3 cases together) */
-  int refinements;        /* outer FP64 refinement steps (mixed precision), else 0 */
+  int refinements;        /* mixed precision: FP64 residual evaluations r = b - A x64 (with the PCG
+                             solver the start and every exact residual replacement; with the
+                             V-cycle solver one per refinement step), else 0 */
   double rel_res[3];      /* final ||r|| / (||f|| + 1e-10) per load case */
   int status;             /* otm_status of the last solve */
   int levels;             /* multigrid levels */
