@@ -104,6 +104,16 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def job_seconds(lat_ms, world, device):
+    """Seconds of this rank's device-timed steps, max-reduced over the ranks: the job takes as
+    long as its slowest replica."""
+    import torch
+    t = torch.tensor([sum(lat_ms) / 1e3], dtype=torch.float64, device=device)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
 # ---------------------------------------------------------------------------------------
 # Our arm
 # ---------------------------------------------------------------------------------------
@@ -197,10 +207,7 @@ def run_ours(args, rank, world, local_rank):
             mixed = {"error": str(ex)}
 
     def total_s(res):
-        t = torch.tensor([sum(res["lat_ms"]) / 1e3], dtype=torch.float64, device=dev)
-        if world > 1:
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+        return job_seconds(res["lat_ms"], world, dev)
 
     t_main = total_s(main)
     t_e2e = total_s(e2e)
