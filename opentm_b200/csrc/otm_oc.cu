@@ -116,16 +116,22 @@ __global__ void __launch_bounds__(kBlock) k_oc_tree_pass(int ne, const float* __
     cf[threadIdx.x] = damp == 0.5f ? float(1.0 / sqrt(double(g[threadIdx.x])))
                                     : float(pow(double(g[threadIdx.x]), -double(damp)));
   __syncthreads();
-  // per-thread FP32 partial volumes of the 31 candidates (a few elements per thread)
-  float v[kTreeNodes];
+  // per-thread FP32 partial volumes of the 31 candidates (a few elements per thread); the
+  // candidate factors live in registers, and the move limit and box bounds are one interval
+  // [max(r - step, min_rho), min(r + step, 1)] (the same clamp for min_rho <= r <= 1)
+  float v[kTreeNodes], cfr[kTreeNodes];
 #pragma unroll
-  for (int t = 0; t < kTreeNodes; t++) v[t] = 0.f;
+  for (int t = 0; t < kTreeNodes; t++) {
+    v[t] = 0.f;
+    cfr[t] = cf[t];
+  }
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ne; i += gridDim.x * blockDim.x) {
     const float s = __ldg(sens + i), r = __ldg(rho + i);
     if (s < 0.f) {
       const float a = (damp == 0.5f ? sqrtf(-s) : powf(-s, damp)) * r;
+      const float lo = fmaxf(r - step, min_rho), hi = fminf(r + step, 1.f);
 #pragma unroll
-      for (int t = 0; t < kTreeNodes; t++) v[t] += oc_clamp(a * cf[t], r, min_rho, step);
+      for (int t = 0; t < kTreeNodes; t++) v[t] += fminf(fmaxf(a * cfr[t], lo), hi);
     } else {  // -s/g <= 0 (or NaN): the same value for every candidate
       const float nr = oc_new_rho(s, r, g[0], min_rho, step, damp);
 #pragma unroll
