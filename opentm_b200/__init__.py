@@ -12,6 +12,7 @@ shape (nz, ny, nx) (or (nz, ny, pitchT) for pitched fields).
 from __future__ import annotations
 
 import ctypes
+import time
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -305,15 +306,19 @@ class MMAOptimizer:
 
 
 class Server:
-    """Continuous-batching server of homogenization requests (include/opentm_b200_server.h).
+    """Server of independent homogenization requests (include/opentm_b200_server.h).
 
     submit(k) queues a solve of one cell (k: host numpy array of shape (nz, ny, nx)); step()
-    admits what fits the memory budget and advances every running request; poll(id) returns
-    None while the request runs, else (K^H, info).
+    retires finished requests and admits what fits the memory budget (the batched form also
+    advances every running request); poll(id) returns None while the request is queued or
+    running, else (K^H, info). batched=False (default) runs up to `streams` requests at once as
+    resident solver handles on their own streams; batched=True advances all running requests
+    with shared kernel launches.
     """
 
     def __init__(self, hbm_budget_bytes=150 * 10 ** 9, max_active=64, fem_rel_thres=1e-6, max_iter=200,
-                 pre_smooth=2, iters_per_step=2, power_penal=1.0, stream=None):
+                 pre_smooth=2, iters_per_step=2, power_penal=1.0, stream=None, batched=False, streams=8,
+                 host_stage_bytes=1 << 30):
         cfg = _lib.ServerConfig()
         check(lib().otm_server_config_init(ctypes.byref(cfg)), "otm_server_config_init")
         cfg.hbm_budget_bytes = int(hbm_budget_bytes)
@@ -323,6 +328,9 @@ class Server:
         cfg.pre_smooth = int(pre_smooth)
         cfg.iters_per_step = int(iters_per_step)
         cfg.power_penal = float(power_penal)
+        cfg.batched = int(bool(batched))
+        cfg.streams = int(streams)
+        cfg.host_stage_bytes = int(host_stage_bytes)
         self._h = ctypes.c_void_p()
         check(lib().otm_server_create(ctypes.byref(cfg), ctypes.c_void_p(_stream(stream)), ctypes.byref(self._h)),
               "otm_server_create")
@@ -344,6 +352,9 @@ class Server:
 
     def bytes_in_use(self) -> int:
         return int(lib().otm_server_bytes_in_use(self._h))
+
+    def bytes_resident(self) -> int:
+        return int(lib().otm_server_bytes_resident(self._h))
 
     def submit(self, k) -> int:
         k = np.ascontiguousarray(k, dtype=np.float32)
@@ -368,12 +379,21 @@ class Server:
             raise OtmError(st, "otm_server_poll", _lib.last_error())
         return np.array(C[:]).reshape(3, 3), info
 
+    def state(self, rid) -> int:
+        """0 queued, 1 running, 2 done, 3 cancelled, 4 failed."""
+        info = _lib.RequestInfo()
+        lib().otm_server_poll(self._h, ctypes.c_int64(rid), None, ctypes.byref(info))
+        return int(info.state)
+
     def cancel(self, rid):
         check(lib().otm_server_cancel(self._h, ctypes.c_int64(rid)), "otm_server_cancel")
 
-    def run_until_idle(self, max_steps=100000):
-        for _ in range(max_steps):
+    def run_until_idle(self, timeout_s=600.0):
+        t_end = time.monotonic() + timeout_s
+        while time.monotonic() < t_end:
             nr, nq = self.step()
             if nr == 0 and nq == 0:
                 return
+            if nq == 0:
+                time.sleep(20e-6)  # only running requests left: poll, do not spin
         raise RuntimeError("server did not drain")

@@ -74,7 +74,8 @@ class Profile(ctypes.Structure):
 class ServerConfig(ctypes.Structure):
     _fields_ = [("hbm_budget_bytes", ctypes.c_size_t), ("max_active", ctypes.c_int), ("fem_rel_thres", ctypes.c_double),
                 ("max_iter", ctypes.c_int), ("pre_smooth", ctypes.c_int), ("iters_per_step", ctypes.c_int),
-                ("power_penal", ctypes.c_float)]
+                ("power_penal", ctypes.c_float), ("batched", ctypes.c_int), ("streams", ctypes.c_int),
+                ("host_stage_bytes", ctypes.c_size_t)]
 
 
 class RequestInfo(ctypes.Structure):
@@ -149,6 +150,7 @@ SIGNATURES = {
     "otm_server_cancel": (_S, [_P, ctypes.c_int64]),
     "otm_server_request_bytes": (ctypes.c_size_t, [_I3]),
     "otm_server_bytes_in_use": (ctypes.c_size_t, [_P]),
+    "otm_server_bytes_resident": (ctypes.c_size_t, [_P]),
 }
 
 _lib = None

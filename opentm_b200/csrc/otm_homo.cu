@@ -312,6 +312,7 @@ otm_status Homo::update(const float* kin, int pitchT) {
   if (pitchT < d0.nx) return invalid("pitchT smaller than the x resolution");
   OTM_TRY(enter());
   const size_t nv = d0.nv();
+  OTM_CUDA(cudaMemsetAsync(flags, 0, 2 * sizeof(int), stream));  // import / coarsest status of this field
   k_import<<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(d0, kin, pitchT, cfg.power_penal, ks, kraw, flags);
   OTM_CHECK_LAUNCH("k_import");
   launched(1);
@@ -738,6 +739,26 @@ void Homo::launch_solve_start() {
   launched(mixed ? 3 : 2);
 }
 
+// One solve from the current x with the iteration loop on the device: start kernels, the loop
+// graph, the FP32 copy of a mixed solution, optionally the K^H reduction, then the flags and
+// solve scalars to pinned memory. Launches only; the caller waits on the stream and then reads
+// flags_host / sc_host.
+otm_status Homo::launch_device_solve(bool with_heat) {
+  const size_t nv = lv[0].d.nv();
+  launch_solve_start();
+  OTM_CHECK_LAUNCH("solve init");
+  OTM_TRY(launch_loop());
+  if (mixed) {
+    k_x64_to_x<<<ceil_div(3 * nv, kBlock), kBlock, 0, stream>>>(3 * nv, x64, x);
+    launched(1);
+  }
+  if (with_heat) launch_heat_matrix();
+  OTM_CHECK_LAUNCH("solve");
+  OTM_CUDA(cudaMemcpyAsync(flags_host, flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream));
+  OTM_CUDA(cudaMemcpyAsync(sc_host, sc, sizeof(SolveScalars), cudaMemcpyDeviceToHost, stream));
+  return OTM_OK;
+}
+
 // Solve the 3 load cases to the tolerance (MG_H::solveEquation, homogenization/MG.cpp:80-142;
 // iterations PCG or stationary V-cycles). With graphs and without profiling the iteration loop
 // runs on the device (launch_loop) and the host waits once; with with_heat the K^H reduction
@@ -757,23 +778,15 @@ otm_status Homo::solve_impl(bool with_heat) {
       OTM_CUDA(cudaMemsetAsync(x, 0, 3 * nv * sizeof(float), stream));
       if (mixed) OTM_CUDA(cudaMemsetAsync(x64, 0, 3 * nv * sizeof(double), stream));
     }
-    launch_solve_start();
-    OTM_CHECK_LAUNCH("solve init");
     if (device_loop) {
-      OTM_TRY(launch_loop());
-      if (mixed) {
-        k_x64_to_x<<<ceil_div(3 * nv, kBlock), kBlock, 0, stream>>>(3 * nv, x64, x);
-        launched(1);
-      }
-      if (with_heat) launch_heat_matrix();
-      OTM_CHECK_LAUNCH("solve");
-      OTM_CUDA(cudaMemcpyAsync(flags_host, flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream));
-      OTM_CUDA(cudaMemcpyAsync(sc_host, sc, sizeof(SolveScalars), cudaMemcpyDeviceToHost, stream));
+      OTM_TRY(launch_device_solve(with_heat));
       OTM_CUDA(cudaStreamSynchronize(stream));
       OTM_TRY(check_flags());
       count_launches(1 + loop_body_kernels * uint64_t(sc_host->loop));
       heat_ready = with_heat;
     } else {
+      launch_solve_start();
+      OTM_CHECK_LAUNCH("solve init");
       int nlaunched = 0, iter_before = 0;
       bool first_check = true;
       while (true) {

@@ -111,6 +111,7 @@ struct Homo {
   otm_status launch_loop();
   otm_status check_flags();
   void launch_solve_start();
+  otm_status launch_device_solve(bool with_heat);
   otm_status solve_impl(bool with_heat = false);
   otm_status solve(otm_solve_stats* out);
   otm_status heat_matrix(double C[9], bool do_solve);

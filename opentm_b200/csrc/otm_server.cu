@@ -1,15 +1,26 @@
-// otm_server.cu -- continuous batching of homogenization requests on one GPU.
+// otm_server.cu -- serving of independent homogenization requests on one GPU, in two forms.
 //
-// Each admitted request owns a resident multigrid hierarchy (an otm::Homo in server mode:
-// the server's stream, buffers from the server's memory pool). Its device pointers are
-// collected in a ReqDesc that lives in a device-side slot table; a batched launch carries a
-// small task list (slot, level, first block, block count) and every block finds its task by
-// binary search, then runs the same device body as the single-request kernel. One scheduling
-// step advances all running requests by a few preconditioned-CG iterations: per multigrid
-// level one launch per colour pass / residual / restriction / prolongation over every request
-// that has that level, one launch of the single-CTA tails (one block per request) and one
-// launch per Krylov update. Requests finish, release their memory and are replaced by queued
-// ones at step boundaries.
+// Handle form (default): the server keeps a few streams ("lanes"). An admitted request runs on
+// an idle lane as one resident solver handle (otm::Homo, the same object otm_homo_* drives):
+// the field goes up from the lane's pinned staging buffer, update() builds the coarse
+// operators, and the whole preconditioned-CG loop runs on the device as one conditional-graph
+// launch, followed by the K^H reduction and a copy of the solve scalars to pinned memory and an
+// event. Scheduling never waits for a lane except when the queue is blocked; lanes overlap on
+// the GPU, so the small kernels of one request fill the gaps of another. Handles stay resident
+// per lane and size after their request finishes and are reused by the next request of that
+// size (a handle is built, and its solve graph captured, once); idle handles are destroyed,
+// least recently used first, when a new one would not fit the memory budget.
+//
+// Batched form: each admitted request owns a resident multigrid hierarchy (an otm::Homo in
+// server mode: the server's stream, buffers from the server's memory pool). Its device
+// pointers are collected in a ReqDesc that lives in a device-side slot table; a batched launch
+// carries a small task list (slot, level, first block, block count) and every block finds its
+// task by binary search, then runs the same device body as the single-request kernel. One
+// scheduling step advances all running requests by a few preconditioned-CG iterations: per
+// multigrid level one launch per colour pass / residual / restriction / prolongation over every
+// request that has that level, one launch of the single-CTA tails (one block per request) and
+// one launch per Krylov update. Requests finish, release their memory and are replaced by
+// queued ones at step boundaries.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -18,15 +29,18 @@
 #include <deque>
 #include <map>
 #include <memory>
+#include <thread>
 #include <vector>
 
 #include "opentm_b200_server.h"
 #include "otm_homo_impl.h"
+#include "otm_host_ring.h"
 
 namespace otm {
 
 constexpr int kSrvMaxLevels = 12;
 constexpr int kSrvMaxActive = 256;
+constexpr int kSrvMaxStreams = 64;
 
 struct ReqLevel {
   Dims d;
@@ -180,10 +194,43 @@ static double now_s() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
+// Pinned host memory for submitted fields (offsets kept by RingOffsets). A full ring leaves the
+// field in pageable memory.
+class HostRing {
+ public:
+  ~HostRing() {
+    if (base_) cudaFreeHost(base_);
+  }
+  cudaError_t init(size_t bytes) {
+    const size_t n = bytes / sizeof(float);
+    if (n == 0) return cudaSuccess;
+    const cudaError_t e = cudaMallocHost((void**)&base_, n * sizeof(float));
+    if (e != cudaSuccess) {
+      base_ = nullptr;
+      return e;
+    }
+    off_ = RingOffsets(n, 64);  // 256-byte starts
+    return cudaSuccess;
+  }
+  float* alloc(size_t n, int64_t* seq) {
+    size_t o = 0;
+    if (!base_ || !off_.alloc(n, &o, seq)) return nullptr;
+    return base_ + o;
+  }
+  void release(int64_t seq) { off_.release(seq); }
+
+ private:
+  float* base_ = nullptr;
+  RingOffsets off_;
+};
+
 struct Request {
   int64_t id = 0;
   int reso[3] = {0, 0, 0};
-  std::vector<float> k;
+  std::vector<float> k;      // the field, when the pinned ring had no room
+  float* pinned = nullptr;   // the field in the pinned ring
+  int64_t ring_seq = -1;
+  const float* field() const { return pinned ? pinned : k.data(); }
   int state = 0;  // 0 queued, 1 running, 2 done, 3 cancelled, 4 failed
   int status = OTM_ERR_NOT_READY;
   bool cancel = false;
@@ -236,8 +283,36 @@ static size_t request_bytes(const int reso[3]) {
 
 using namespace otm;
 
+namespace otm {
+
+// A resident handle of one cell size on a lane.
+struct CachedHandle {
+  int reso[3] = {0, 0, 0};
+  std::unique_ptr<Homo> h;
+  size_t bytes = 0;
+  uint64_t last_use = 0;
+};
+
+// One stream of the handle form: at most one running request, handles kept per cell size.
+struct Lane {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;  // recorded after the running request's last copy
+  int64_t req = -1;            // running request (-1: idle)
+  Homo* run = nullptr;         // its handle
+  std::vector<CachedHandle> cache;
+  float* stage = nullptr;  // pinned copy of the running request's field
+  size_t stage_cap = 0;    // floats
+};
+
+}  // namespace otm
+
 struct otm_server {
   otm_server_config cfg{};
+  bool handles = false;  // handle form
+  std::vector<otm::Lane> lanes;
+  size_t bytes_resident = 0;  // all handles of the handle form, running or idle
+  uint64_t use_clock = 0;
+  otm::HostRing ring;
   cudaStream_t stream = nullptr;
   cudaMemPool_t pool = nullptr;
   std::map<int64_t, Request> reqs;
@@ -256,6 +331,16 @@ struct otm_server {
   size_t stage_cap = 0, stage_used = 0;
   cudaEvent_t stage_ev = nullptr;
   ~otm_server() {
+    for (auto& ln : lanes) {
+      if (ln.stream) cudaStreamSynchronize(ln.stream);
+      ln.cache.clear();  // buffers go back to the pool on the lane's stream
+      if (ln.stream) {
+        cudaStreamSynchronize(ln.stream);
+        cudaStreamDestroy(ln.stream);
+      }
+      if (ln.done) cudaEventDestroy(ln.done);
+      if (ln.stage) cudaFreeHost(ln.stage);
+    }
     if (stream) cudaStreamSynchronize(stream);
     reqs.clear();
     if (stream) cudaStreamSynchronize(stream);
@@ -271,6 +356,15 @@ struct otm_server {
 };
 
 namespace otm {
+
+// The request's host copy of its field is no longer needed (uploaded, or never will be).
+static void release_field(otm_server* s, Request& r) {
+  if (r.pinned) s->ring.release(r.ring_seq);
+  r.pinned = nullptr;
+  r.ring_seq = -1;
+  r.k.clear();
+  r.k.shrink_to_fit();
+}
 
 // A request leaves the device: its buffers go back to the pool (stream-ordered).
 static void release(otm_server* s, Request& r) {
@@ -294,7 +388,8 @@ static otm_status admit(otm_server* s, Request& r, int slot) {
   if (s->stage_used + nv > s->stage_cap) return OTM_ERR_STATE;  // sized by the caller
   float* stg = s->h_stage + s->stage_used;
   s->stage_used += nv;
-  std::memcpy(stg, r.k.data(), nv * sizeof(float));
+  std::memcpy(stg, r.field(), nv * sizeof(float));
+  release_field(s, r);
   OTM_CUDA(cudaMemcpyAsync(kdev, stg, nv * sizeof(float), cudaMemcpyHostToDevice, s->stream));
   otm_status st = H.update(kdev, d0.nx);
   cudaFreeAsync(kdev, s->stream);
@@ -465,6 +560,226 @@ static otm_status gather(otm_server* s, const std::vector<int>& sl) {
   return OTM_OK;
 }
 
+// ---------------------------------------------------------------------------------------
+// Handle form
+// ---------------------------------------------------------------------------------------
+static bool same_reso(const int a[3], const int b[3]) { return a[0] == b[0] && a[1] == b[1] && a[2] == b[2]; }
+
+static void finish_request(otm_server* s, Request& r, otm_status st, bool have_result, const double kh[6]) {
+  if (r.cancel) {
+    r.state = 3;
+    r.status = OTM_ERR_CANCELLED;
+  } else {
+    if (have_result) {
+      int cnt = 0;
+      for (int a = 0; a < 3; a++)
+        for (int b = a; b < 3; b++) {
+          r.C[a * 3 + b] = kh[cnt];
+          r.C[b * 3 + a] = kh[cnt];
+          cnt++;
+        }
+    }
+    r.status = st;
+    r.state = (have_result && (st == OTM_OK || st == OTM_ERR_NOT_CONVERGED)) ? 2 : 4;
+  }
+  r.info.stats.status = st;
+  r.info.done_s = now_s();
+  s->bytes_in_use -= std::min(s->bytes_in_use, r.bytes);
+  release_field(s, r);
+}
+
+// The lane's request has passed its event: status, statistics and K^H from pinned memory.
+static void retire_lane(otm_server* s, Lane& ln) {
+  Request& r = s->reqs[ln.req];
+  Homo& H = *ln.run;
+  const SolveScalars& S = *H.sc_host;
+  otm_status st = H.check_flags();
+  count_launches(1 + H.loop_body_kernels * uint64_t(S.loop));
+  r.info.stats.iterations = S.iter;
+  for (int c = 0; c < 3; c++) r.info.stats.rel_res[c] = S.relres[c];
+  r.info.stats.levels = int(H.lv.size());
+  r.info.stats.cluster_level = H.cluster_l;
+  for (int i = 0; i < 3; i++) r.info.stats.coarsest_reso[i] = H.stats.coarsest_reso[i];
+  if (st == OTM_OK) {
+    if (S.nan)
+      st = OTM_ERR_DIVERGED;
+    else
+      for (int c = 0; c < 3; c++)
+        if (!(S.relres[c] <= s->cfg.fem_rel_thres)) st = OTM_ERR_NOT_CONVERGED;
+  }
+  finish_request(s, r, st, st == OTM_OK || st == OTM_ERR_NOT_CONVERGED, S.kh);
+  ln.req = -1;
+  ln.run = nullptr;
+}
+
+static otm_status retire_finished(otm_server* s, bool* any) {
+  for (Lane& ln : s->lanes) {
+    if (ln.req < 0) continue;
+    const cudaError_t e = cudaEventQuery(ln.done);
+    if (e == cudaErrorNotReady) continue;
+    if (e != cudaSuccess) return cuda_fail(e, "serving lane");
+    retire_lane(s, ln);
+    *any = true;
+  }
+  return OTM_OK;
+}
+
+static void drop_handle(otm_server* s, Lane& ln, size_t i) {
+  s->bytes_resident -= std::min(s->bytes_resident, ln.cache[i].bytes);
+  ln.cache.erase(ln.cache.begin() + i);
+}
+
+// Make room for `need` more resident bytes by destroying idle handles, least recently used
+// first. Returns false (destroying nothing) when even all idle handles would not be enough.
+static bool make_room(otm_server* s, size_t need) {
+  const size_t budget = s->cfg.hbm_budget_bytes;
+  if (s->bytes_resident + need <= budget) return true;
+  size_t idle = 0;
+  for (Lane& ln : s->lanes)
+    for (auto& c : ln.cache)
+      if (c.h.get() != ln.run) idle += c.bytes;
+  if (s->bytes_resident - std::min(s->bytes_resident, idle) + need > budget) return false;
+  while (s->bytes_resident + need > budget) {
+    Lane* best_lane = nullptr;
+    size_t best = 0;
+    uint64_t oldest = UINT64_MAX;
+    for (Lane& ln : s->lanes)
+      for (size_t i = 0; i < ln.cache.size(); i++)
+        if (ln.cache[i].h.get() != ln.run && ln.cache[i].last_use < oldest) {
+          oldest = ln.cache[i].last_use;
+          best_lane = &ln;
+          best = i;
+        }
+    if (!best_lane) return false;
+    drop_handle(s, *best_lane, best);
+  }
+  return true;
+}
+
+static void handle_config(const otm_server_config& sc, const int reso[3], otm_config* c) {
+  homo_config(sc, reso, c);
+  c->use_graphs = 1;  // the iteration loop as one device-side graph launch
+  c->warm_start = 0;  // every request from a zero initial guess
+}
+
+// Queue the whole request on the lane: field upload, operator setup, solve, K^H, scalars back.
+static otm_status launch_on_lane(otm_server* s, Request& r, Lane& ln, size_t ci) {
+  CachedHandle& ch = ln.cache[ci];
+  Homo& H = *ch.h;
+  const size_t nv = size_t(r.reso[0]) * r.reso[1] * r.reso[2];
+  if (!r.pinned && nv > ln.stage_cap) {
+    if (ln.stage) cudaFreeHost(ln.stage);
+    ln.stage = nullptr;
+    ln.stage_cap = 0;
+    OTM_CUDA(cudaMallocHost((void**)&ln.stage, nv * sizeof(float)));
+    ln.stage_cap = nv;
+  }
+  const float* src = r.pinned;  // uploaded straight from the ring, released at retirement
+  if (!src) {
+    std::memcpy(ln.stage, r.k.data(), nv * sizeof(float));  // the lane is idle: its last copy is done
+    src = ln.stage;
+  }
+  // the right-hand-side buffer holds the field until the solve start overwrites it
+  OTM_CUDA(cudaMemcpyAsync(H.b, src, nv * sizeof(float), cudaMemcpyHostToDevice, ln.stream));
+  OTM_TRY(H.update(H.b, r.reso[0]));
+  OTM_CUDA(cudaMemsetAsync(H.x, 0, 3 * nv * sizeof(float), ln.stream));
+  OTM_TRY(H.launch_device_solve(true));
+  OTM_CUDA(cudaEventRecord(ln.done, ln.stream));
+  ln.req = r.id;
+  ln.run = &H;
+  ch.last_use = ++s->use_clock;
+  return OTM_OK;
+}
+
+// Admit queued requests, first come first served, onto idle lanes while the budget allows.
+static otm_status admit_handles(otm_server* s, bool* any) {
+  while (!s->queue.empty()) {
+    const int64_t id = s->queue.front();
+    Request& r = s->reqs[id];
+    if (r.cancel) {
+      s->queue.pop_front();
+      r.state = 3;
+      r.status = OTM_ERR_CANCELLED;
+      r.info.done_s = now_s();
+      release_field(s, r);
+      *any = true;
+      continue;
+    }
+    // an idle lane that already holds a handle of this size, else the idle lane holding the
+    // fewest handles
+    Lane* lane = nullptr;
+    int ci = -1;
+    for (Lane& ln : s->lanes) {
+      if (ln.req >= 0) continue;
+      for (size_t i = 0; i < ln.cache.size(); i++)
+        if (same_reso(ln.cache[i].reso, r.reso)) {
+          lane = &ln;
+          ci = int(i);
+          break;
+        }
+      if (lane) break;
+    }
+    if (!lane)
+      for (Lane& ln : s->lanes)
+        if (ln.req < 0 && (!lane || ln.cache.size() < lane->cache.size())) lane = &ln;
+    if (!lane) break;  // every lane is busy
+    if (ci < 0 && !make_room(s, r.bytes)) break;  // the head of the queue waits for memory
+    s->queue.pop_front();
+    *any = true;
+    s->bytes_in_use += r.bytes;
+    r.state = 1;
+    r.info.admit_s = now_s();
+    if (ci < 0) {
+      CachedHandle ch;
+      for (int i = 0; i < 3; i++) ch.reso[i] = r.reso[i];
+      ch.bytes = r.bytes;
+      ch.h.reset(new (std::nothrow) Homo());
+      otm_status bst = OTM_ERR_OUT_OF_MEMORY;
+      if (ch.h) {
+        otm_config c;
+        handle_config(s->cfg, r.reso, &c);
+        bst = ch.h->build(c, lane->stream, s->pool, true);
+      }
+      if (bst != OTM_OK) {
+        finish_request(s, r, bst, false, nullptr);
+        continue;
+      }
+      lane->cache.push_back(std::move(ch));
+      s->bytes_resident += r.bytes;
+      ci = int(lane->cache.size()) - 1;
+    }
+    const otm_status st = launch_on_lane(s, r, *lane, size_t(ci));
+    if (st != OTM_OK) {
+      // nothing of the request may still run when its handle goes: wait for the lane
+      cudaStreamSynchronize(lane->stream);
+      lane->req = -1;
+      lane->run = nullptr;
+      drop_handle(s, *lane, size_t(ci));
+      finish_request(s, r, st, false, nullptr);
+      if (st == OTM_ERR_CUDA) return st;
+    }
+  }
+  return OTM_OK;
+}
+
+static otm_status step_handles(otm_server* s) {
+  const double deadline = now_s() + 600.0;
+  while (true) {
+    bool retired = false, admitted = false;
+    OTM_TRY(retire_finished(s, &retired));
+    OTM_TRY(admit_handles(s, &admitted));
+    bool running = false;
+    for (Lane& ln : s->lanes) running |= ln.req >= 0;
+    // return at once unless the queue is blocked behind running requests
+    if (retired || admitted || s->queue.empty() || !running) return OTM_OK;
+    if (now_s() > deadline) {
+      set_error("no serving lane finished within 600 s");
+      return OTM_ERR_TIMEOUT;
+    }
+    std::this_thread::sleep_for(std::chrono::microseconds(20));
+  }
+}
+
 }  // namespace otm
 
 extern "C" {
@@ -479,6 +794,9 @@ otm_status otm_server_config_init(otm_server_config* cfg) {
   cfg->pre_smooth = 2;
   cfg->iters_per_step = 2;
   cfg->power_penal = 1.0f;
+  cfg->batched = 0;
+  cfg->streams = 8;
+  cfg->host_stage_bytes = size_t(1) << 30;
   return OTM_OK;
 }
 
@@ -489,7 +807,8 @@ size_t otm_server_request_bytes(const int reso[3]) {
 
 otm_status otm_server_create(const otm_server_config* cfg, void* stream, otm_server** out) {
   if (!cfg || !out || cfg->max_active < 1 || cfg->max_active > kSrvMaxActive || cfg->pre_smooth < 1 ||
-      cfg->iters_per_step < 1 || cfg->max_iter < 1 || !(cfg->fem_rel_thres > 0))
+      cfg->iters_per_step < 1 || cfg->max_iter < 1 || !(cfg->fem_rel_thres > 0) ||
+      (!cfg->batched && (cfg->streams < 1 || cfg->streams > kSrvMaxStreams)))
     return OTM_ERR_INVALID_ARGUMENT;
   *out = nullptr;
   std::unique_ptr<otm_server> s(new (std::nothrow) otm_server());
@@ -511,6 +830,15 @@ otm_status otm_server_create(const otm_server_config* cfg, void* stream, otm_ser
   OTM_CUDA(cudaMalloc((void**)&s->d_slots, sizeof(int) * cfg->max_active));
   OTM_CUDA(cudaMalloc((void**)&s->d_status, sizeof(SlotStatus) * cfg->max_active));
   OTM_CUDA(cudaMallocHost((void**)&s->h_status, sizeof(SlotStatus) * cfg->max_active));
+  OTM_CUDA(s->ring.init(cfg->host_stage_bytes));
+  s->handles = !cfg->batched;
+  if (s->handles) {
+    s->lanes.resize(std::min(cfg->streams, cfg->max_active));
+    for (Lane& ln : s->lanes) {
+      OTM_CUDA(cudaStreamCreateWithFlags(&ln.stream, cudaStreamNonBlocking));
+      OTM_CUDA(cudaEventCreateWithFlags(&ln.done, cudaEventDisableTiming));
+    }
+  }
   *out = s.release();
   return OTM_OK;
 }
@@ -537,7 +865,11 @@ otm_status otm_server_submit(otm_server* s, const int reso[3], const float* k_ho
   Request r;
   r.id = s->next_id++;
   for (int i = 0; i < 3; i++) r.reso[i] = reso[i];
-  r.k.assign(k_host, k_host + nv);
+  r.pinned = s->ring.alloc(nv, &r.ring_seq);
+  if (r.pinned)
+    std::memcpy(r.pinned, k_host, nv * sizeof(float));
+  else
+    r.k.assign(k_host, k_host + nv);
   r.bytes = bytes;
   r.info.submit_s = now_s();
   r.info.state = 0;
@@ -550,6 +882,14 @@ otm_status otm_server_submit(otm_server* s, const int reso[3], const float* k_ho
 
 otm_status otm_server_step(otm_server* s, int* n_running, int* n_queued) {
   if (!s) return OTM_ERR_INVALID_ARGUMENT;
+  if (s->handles) {
+    const otm_status st = step_handles(s);
+    int nr = 0;
+    for (const Lane& ln : s->lanes) nr += ln.req >= 0;
+    if (n_running) *n_running = nr;
+    if (n_queued) *n_queued = int(s->queue.size());
+    return st;
+  }
   // 1. cancelled requests leave
   for (int sl = 0; sl < int(s->slots.size()); sl++) {
     const int64_t id = s->slots[sl];
@@ -573,7 +913,7 @@ otm_status otm_server_step(otm_server* s, int* n_running, int* n_queued) {
     for (int64_t id : s->queue) {
       const Request& r = s->reqs[id];
       if (free_slots == 0 || used_bytes + r.bytes > s->cfg.hbm_budget_bytes) break;
-      need += r.k.size();
+      need += size_t(r.reso[0]) * r.reso[1] * r.reso[2];
       used_bytes += r.bytes;
       free_slots--;
     }
@@ -593,6 +933,7 @@ otm_status otm_server_step(otm_server* s, int* n_running, int* n_queued) {
       r.state = 3;
       r.status = OTM_ERR_CANCELLED;
       r.info.done_s = now_s();
+      release_field(s, r);
       continue;
     }
     int slot = -1;
@@ -610,7 +951,7 @@ otm_status otm_server_step(otm_server* s, int* n_running, int* n_queued) {
       r.state = 4;
       r.status = st;
       r.info.done_s = now_s();
-      r.k.clear();
+      release_field(s, r);
     }
   }
   if (s->stage_used) OTM_CUDA(cudaEventRecord(s->stage_ev, s->stream));
@@ -652,8 +993,7 @@ otm_status otm_server_step(otm_server* s, int* n_running, int* n_queued) {
         r.state = (st == OTM_OK || st == OTM_ERR_NOT_CONVERGED) ? 2 : 4;
         r.info.done_s = now_s();
         release(s, r);
-        r.k.clear();
-        r.k.shrink_to_fit();
+        release_field(s, r);
       }
     }
   }
@@ -688,5 +1028,10 @@ otm_status otm_server_cancel(otm_server* s, int64_t request_id) {
 }
 
 size_t otm_server_bytes_in_use(const otm_server* s) { return s ? s->bytes_in_use : 0; }
+
+size_t otm_server_bytes_resident(const otm_server* s) {
+  if (!s) return 0;
+  return s->handles ? s->bytes_resident : s->bytes_in_use;
+}
 
 }  // extern "C"

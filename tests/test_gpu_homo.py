@@ -160,6 +160,11 @@ def test_nan_input_is_rejected():
     with pytest.raises(OtmError) as ei:
         H.heatMatrix()
     assert ei.value.status == 7  # OTM_ERR_NAN
+    # the status belongs to the imported field: a valid field afterwards solves normally
+    good, _ = random_k((8, 8, 8), seed=13)
+    H.update(torch.from_numpy(good).cuda())
+    H.reset_displacement()
+    assert np.all(np.isfinite(H.heatMatrix()))
 
 
 def test_iteration_cap_reports_not_converged():
