@@ -13,7 +13,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB_PATH = os.path.join(HERE, "libopentm_b200.so")
 HEADERS = [os.path.join(ROOT, "include", f)
-           for f in ("opentm_b200.h", "opentm_b200_mma.h", "opentm_b200_server.h", "opentm_b200_noalloc.h")]
+           for f in ("opentm_b200.h", "opentm_b200_mma.h", "opentm_b200_server.h", "opentm_b200_noalloc.h",
+                     "opentm_b200_driver.h")]
 
 OTM_OK = 0
 STATUS_NAMES = {
@@ -88,6 +89,29 @@ class PitchedPtr(ctypes.Structure):
                 ("ysize", ctypes.c_size_t)]
 
 
+class DriverConfig(ctypes.Structure):
+    _fields_ = [("reso", ctypes.c_int), ("sym", ctypes.c_int), ("winit", ctypes.c_int), ("model", ctypes.c_int),
+                ("vol_ratio", ctypes.c_double), ("heat_ratio", ctypes.c_double * 2), ("finthres", ctypes.c_double),
+                ("fem_rel_thres", ctypes.c_double), ("target_tensor", ctypes.c_double * 6),
+                ("max_iter", ctypes.c_int), ("init_period", ctypes.c_int), ("seed", ctypes.c_uint64),
+                ("input_path", ctypes.c_char_p), ("output_prefix", ctypes.c_char_p)]
+
+
+class DriverResult(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int), ("converged", ctypes.c_int), ("objective", ctypes.c_double),
+                ("volume", ctypes.c_double), ("volume_bound", ctypes.c_double), ("K", ctypes.c_float * 9)]
+
+
+class ConvergeChecker(ctypes.Structure):
+    _fields_ = [("thres", ctypes.c_double), ("obj", ctypes.c_double * 10), ("p", ctypes.c_int)]
+
+
+class VolumeGovernor(ctypes.Structure):
+    _fields_ = [("low_bound", ctypes.c_float), ("volume_bound", ctypes.c_float), ("decrease", ctypes.c_float),
+                ("decrease_factor", ctypes.c_float), ("val_last", ctypes.c_float), ("vibrate", ctypes.c_float),
+                ("vibrate_count", ctypes.c_int), ("count", ctypes.c_int)]
+
+
 _P = ctypes.c_void_p
 _I3 = ctypes.POINTER(ctypes.c_int)
 _D = ctypes.POINTER(ctypes.c_double)
@@ -151,6 +175,26 @@ SIGNATURES = {
     "otm_server_request_bytes": (ctypes.c_size_t, [_I3]),
     "otm_server_bytes_in_use": (ctypes.c_size_t, [_P]),
     "otm_server_bytes_resident": (ctypes.c_size_t, [_P]),
+    # design driver (include/opentm_b200_driver.h)
+    "otm_driver_config_init": (_S, [ctypes.POINTER(DriverConfig)]),
+    "otm_symmetrize": (_S, [_I3, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P]),
+    "otm_randtri_coeff_count": (ctypes.c_size_t, [ctypes.c_int, ctypes.c_int]),
+    "otm_randtri_coefficients": (_S, [ctypes.c_uint64, ctypes.c_int, ctypes.c_int, _F]),
+    "otm_randtri_field": (_S, [_I3, _P, ctypes.c_int, ctypes.c_int, _F, ctypes.c_int, _P]),
+    "otm_init_density": (_S, [ctypes.POINTER(DriverConfig), _P, ctypes.c_int, _F, _P]),
+    "otm_converge_checker_init": (None, [ctypes.POINTER(ConvergeChecker), ctypes.c_double]),
+    "otm_converge_checker_step": (ctypes.c_int, [ctypes.POINTER(ConvergeChecker), ctypes.c_int, ctypes.c_double]),
+    "otm_volume_governor_init": (None, [ctypes.POINTER(VolumeGovernor)]),
+    "otm_volume_governor_check": (ctypes.c_int, [ctypes.POINTER(VolumeGovernor), ctypes.c_float, ctypes.c_float,
+                                                 ctypes.c_float, ctypes.c_int]),
+    "otm_volume_governor_decrease": (ctypes.c_float, [ctypes.POINTER(VolumeGovernor)]),
+    "otm_run_custom": (_S, [ctypes.POINTER(DriverConfig), _F, _F, _D, ctypes.POINTER(DriverResult)]),
+    "otm_write_density_binary": (_S, [ctypes.c_char_p, _I3, _F]),
+    "otm_read_density_binary": (_S, [ctypes.c_char_p, _I3, _F, ctypes.c_size_t]),
+    "otm_write_vectors": (_S, [ctypes.c_char_p, ctypes.c_int, ctypes.c_size_t, ctypes.POINTER(_F)]),
+    "otm_read_vectors": (_S, [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(_F),
+                              ctypes.c_size_t]),
+    "otm_write_heat_matrix": (_S, [ctypes.c_char_p, _F, ctypes.c_int]),
 }
 
 _lib = None

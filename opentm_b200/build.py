@@ -28,6 +28,8 @@ SOURCES = [
     "otm_server.cu",
     "otm_noalloc.cu",
     "otm_pool.cu",
+    "otm_init.cu",
+    "otm_driver.cu",
 ]
 
 
