@@ -570,6 +570,55 @@ def run_mma384(args):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------------------
+# The design driver: runCustom as the reference's main() runs it
+# ---------------------------------------------------------------------------------------
+def run_design(args):
+    """runInstance(128, {1, 1e-4}, {0.3, 0.2, 0.1, 0.1, 0.05, 0.05}, IWP, oc) (main.cpp:85): the
+    tensor-matching design loop through the C driver. Iterations/s from the driver's own loop
+    clock, as the difference of a run of warmup + steps iterations and one of warmup iterations
+    (both build the solver and capture its graph once)."""
+    import torch
+
+    from opentm_b200 import launch_count
+    from opentm_b200.driver import DesignConfig, InitWay, Model, run_custom
+    torch.cuda.set_device(0)
+    n = N_CELL if args.n == N_CELL else args.n
+    steps, warm = max(args.steps, 1), max(args.warmup, 1)
+    tt = (0.3, 0.2, 0.1, 0.1, 0.05, 0.05)
+    out = {}
+    for model in (Model.oc, Model.mma):
+        base = dict(reso=n, heatRatio=(1.0, 1e-4), target_tensor=tt, winit=InitWay.IWP, model=model)
+        _, a = run_custom(DesignConfig(max_iter=warm, **base))
+        l0 = launch_count()
+        _, b = run_custom(DesignConfig(max_iter=warm + steps, **base))
+        launches = launch_count() - l0
+        k = b["iterations"] - a["iterations"]
+        dt = b["loop_seconds"] - a["loop_seconds"]
+        out[model.name] = {"iterations_per_s": round(k / dt, 3) if k > 0 and dt > 0 else None,
+                           "ms_per_iteration": round(1e3 * dt / k, 3) if k > 0 else None, "timed_iterations": k,
+                           "objective_last": b["objective"], "volume_last": b["volume"],
+                           "init_ms": round(1e3 * b["init_seconds"], 2), "gpu_launches": int(launches)}
+    cpu = None
+    if not args.no_cpu:
+        import oracle as ora
+        from oracle import driver as od
+        ora.set_num_threads(os.cpu_count() or 1)
+        rho0 = od.init_density(od.INIT_IWP, n)
+        t0 = time.perf_counter()
+        od.run_custom(rho0, "oc", heat_ratio=(1.0, 1e-4), target=tt, iters=1, tol=0.01)
+        cpu = {"value": round(1.0 / (time.perf_counter() - t0), 5), "unit": "iterations/s",
+               "cores": ora.num_threads(), "kind": "port",
+               "sample": f"one OC design iteration at {n}^3 of the FP64 restatement (solve tolerance 0.01)"}
+    line = {"metric": f"design iterations/s of runCustom (OC and MMA) at {n}^3",
+            "value": out["oc"]["iterations_per_s"], "unit": "iterations/s", "n_gpus": 1, "steps": steps,
+            "warmup": warm, "ms_per_step": out["oc"]["ms_per_iteration"], "higher_is_better": True,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"runInstance({n}, {{1, 1e-4}}, {list(tt)}, IWP, oc|mma), solve tolerance 0.01"},
+            "models": out, "cpu_baseline": cpu, "gpu_launches": out["oc"]["gpu_launches"]}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -579,7 +628,7 @@ def main():
     ap.add_argument("--n", type=int, default=N_CELL)
     ap.add_argument("--mixed", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="oc", choices=["oc", "serve", "solve256", "mma384"])
+    ap.add_argument("--workload", default="oc", choices=["oc", "serve", "solve256", "mma384", "design"])
     ap.add_argument("--requests", type=int, default=2000)
     ap.add_argument("--rate", type=float, default=0.0, help="Poisson rate; 0 sweeps 50..2000 req/s")
     ap.add_argument("--max-active", type=int, default=64)
@@ -595,6 +644,9 @@ def main():
         return
     if args.workload == "mma384":
         run_mma384(args)
+        return
+    if args.workload == "design":
+        run_design(args)
         return
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

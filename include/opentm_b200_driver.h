@@ -84,6 +84,8 @@ typedef struct otm_driver_result {
   double volume;       /* mean density at exit */
   double volume_bound; /* OC: the governor's volume bound at exit; MMA: 0 */
   float K[9];          /* last K^H (FP32 copy, as heat_tensor_t holds it) */
+  double init_seconds; /* setup and initial density (host clock) */
+  double loop_seconds; /* the design iterations (host clock; every iteration waits for its K^H) */
 } otm_driver_result;
 
 OTM_API otm_status otm_driver_config_init(otm_driver_config* cfg);

@@ -99,7 +99,8 @@ class DriverConfig(ctypes.Structure):
 
 class DriverResult(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int), ("converged", ctypes.c_int), ("objective", ctypes.c_double),
-                ("volume", ctypes.c_double), ("volume_bound", ctypes.c_double), ("K", ctypes.c_float * 9)]
+                ("volume", ctypes.c_double), ("volume_bound", ctypes.c_double), ("K", ctypes.c_float * 9),
+                ("init_seconds", ctypes.c_double), ("loop_seconds", ctypes.c_double)]
 
 
 class ConvergeChecker(ctypes.Structure):

@@ -363,6 +363,9 @@ otm_status otm_run_custom(const otm_driver_config* cfg, const float* rho0_host, 
     return otm_density_backward(reso, F.g_k, F.dk, F.wsum, F.g_rho, n, OTM_WEIGHT_SPLINE4, 1.5f, 0, s);
   };
 
+  OTM_CUDA(cudaStreamSynchronize(s));
+  const double t_loop = now_s();
+  res.init_seconds = t_loop - t_start;
   otm_converge_checker criteria;
   otm_converge_checker_init(&criteria, cfg->finthres);
   FILE* vlog = cfg->output_prefix ? std::fopen(path_of(cfg->output_prefix, "oc_v_log.txt").c_str(), "a") : nullptr;
@@ -426,6 +429,8 @@ otm_status otm_run_custom(const otm_driver_config* cfg, const float* rho0_host, 
     res.volume_bound = gov.volume_bound;
     if (vlog) std::fprintf(vlog, "%g\n", now_s() - t_start);
   }
+  OTM_CUDA(cudaStreamSynchronize(s));
+  res.loop_seconds = now_s() - t_loop;
   res.objective = val;
   std::memcpy(res.K, K, sizeof(K));
   {

@@ -132,7 +132,8 @@ def run_custom(config: DesignConfig, rho0=None):
     del keep
     info = {"iterations": res.iterations, "converged": bool(res.converged), "objective": res.objective,
             "volume": res.volume, "volume_bound": res.volume_bound,
-            "K": np.array(res.K[:], dtype=np.float32).reshape(3, 3), "history": hist[:res.iterations].copy()}
+            "K": np.array(res.K[:], dtype=np.float32).reshape(3, 3), "history": hist[:res.iterations].copy(),
+            "init_seconds": res.init_seconds, "loop_seconds": res.loop_seconds}
     return rho_out, info
 
 
