@@ -7,6 +7,9 @@
 //   homo::MMAOptimizer       optimization/mmaOptimizer.h:12-35
 //   mmasubDevice             optimization/mmaOpt.h:14-19
 //   cfg::HomoConfig          cmdline.h:12-33
+//   ConvergeChecker, VolumeGovernor   homogenization/Framework.cuh:312-411
+//   runCustom                Framework.cu:147-244
+//   runInstance, wrapper_homo main.cpp:17-62
 // Errors the reference reported with printf/exit/exceptions surface as std::runtime_error
 // (homo::Error) carrying the otm_status; a solve that hits the iteration cap prints a
 // warning and continues, as MG_H::solveEquation does (homogenization/MG.cpp:392-428).
@@ -19,7 +22,10 @@
 #include <stdexcept>
 #include <string>
 
+#include <vector>
+
 #include "opentm_b200.h"
+#include "opentm_b200_driver.h"
 #include "opentm_b200_mma.h"
 
 namespace cfg {
@@ -223,6 +229,89 @@ class MMAOptimizer {
 };
 
 }  // namespace homo
+
+// ---- the driver layer (global names, as in the reference) ----
+struct ConvergeChecker {
+  ConvergeChecker(double thres_ = 1e-3) { otm_converge_checker_init(&c_, thres_); }
+  bool is_converge(int iter, double obj) { return otm_converge_checker_step(&c_, iter, obj) != 0; }
+
+ private:
+  otm_converge_checker c_{};
+};
+
+struct VolumeGovernor {
+  VolumeGovernor() { otm_volume_governor_init(&g_); }
+  float get_volume_bound() { return g_.volume_bound; }
+  int volume_check(float value, float lowBound, float volfrac, int itn) {
+    return otm_volume_governor_check(&g_, value, lowBound, volfrac, itn);
+  }
+  float get_current_decrease() { return otm_volume_governor_decrease(&g_); }
+
+ private:
+  otm_volume_governor g_{};
+};
+
+// runCustom (Framework.cu:147-244): the design loop; rho0 (reso^3 values) replaces initDensity.
+// Files are written only when config.outprefix is not empty (the reference always writes them,
+// with OpenVDB densities; here they are in the binary density format).
+inline std::vector<float> runCustom(cfg::HomoConfig config, std::vector<float>* rho0 = nullptr) {
+  otm_driver_config c;
+  otm_driver_config_init(&c);
+  c.reso = config.reso[0];
+  c.sym = int(config.sym);
+  c.winit = int(config.winit);
+  c.model = int(config.model);
+  c.vol_ratio = config.volRatio;
+  c.heat_ratio[0] = config.heatRatio[0];
+  c.heat_ratio[1] = config.heatRatio[1];
+  c.finthres = config.finthres;
+  c.fem_rel_thres = config.femRelThres;
+  for (int i = 0; i < 6; i++) c.target_tensor[i] = config.target_tensor[i];
+  c.max_iter = config.max_iter;
+  c.init_period = config.initperiod;
+  c.input_path = config.inputrho.c_str();
+  c.output_prefix = config.outprefix.empty() ? nullptr : config.outprefix.c_str();
+  const size_t ne = size_t(c.reso) * c.reso * c.reso;
+  if (rho0 && rho0->size() != ne)
+    throw homo::Error(OTM_ERR_INVALID_ARGUMENT, "runCustom: rho0 does not hold reso^3 values");
+  std::vector<float> rho(ne);
+  homo::check(otm_run_custom(&c, rho0 ? rho0->data() : nullptr, rho.data(), nullptr, nullptr), "runCustom");
+  return rho;
+}
+
+// runInstance / wrapper_homo (main.cpp:17-62)
+inline std::vector<float> runInstance(int reso, std::vector<double> heat_ratios, std::vector<double> target_ratio,
+                                      cfg::InitWay initway, cfg::Model model) {
+  cfg::HomoConfig config;
+  config.init();
+  config.reso[0] = config.reso[1] = config.reso[2] = reso;
+  if (heat_ratios.size() != 2 || target_ratio.size() < 6)
+    throw homo::Error(OTM_ERR_INVALID_ARGUMENT, "runInstance: wrong size of heat_ratios or target_ratio");
+  for (int i = 0; i < 2; i++) config.heatRatio[i] = heat_ratios[i];
+  for (int i = 0; i < 6; i++) config.target_tensor[i] = target_ratio[i];
+  config.winit = initway;
+  config.model = model;
+  return runCustom(config);
+}
+
+class wrapper_homo {
+  cfg::HomoConfig config;
+  std::vector<float> rho;
+
+ public:
+  wrapper_homo() { config.init(); }
+  void setDensity(std::vector<float> rho_) { rho = rho_; }
+  void setConfig(int reso, std::vector<double> heat_ratios, std::vector<double> target_ratio, cfg::Model model) {
+    config.init();
+    config.reso[0] = config.reso[1] = config.reso[2] = reso;
+    if (heat_ratios.size() != 2 || target_ratio.size() < 6)
+      throw homo::Error(OTM_ERR_INVALID_ARGUMENT, "setConfig: wrong size of heat_ratios or target_ratio");
+    for (int i = 0; i < 2; i++) config.heatRatio[i] = heat_ratios[i];
+    for (int i = 0; i < 6; i++) config.target_tensor[i] = target_ratio[i];
+    config.model = model;
+  }
+  std::vector<float> optimize() { return runCustom(config, &rho); }
+};
 
 // mmasubDevice (optimization/mmaOpt.h:14-19) with the reference's exact signature.
 inline void mmasubDevice(int ncontrain, int nvar, int itn, double* xvar, double* xmin, double* xmax, double* xold1,

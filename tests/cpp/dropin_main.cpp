@@ -1,6 +1,7 @@
 // Drop-in check of the C++ wrapper: the reference's call sequence (Homogenization_H::update,
 // heatMatrix, Sensitivity; OCOptimizer::filterSens/update; MMAOptimizer::update; mmasubDevice)
-// compiled unchanged against include/otm/homogenization.hpp. Prints K^H and checksums; the
+// compiled unchanged against include/otm/homogenization.hpp, then runCustom / ConvergeChecker /
+// VolumeGovernor of the driver layer. Prints K^H and checksums; the
 // pytest driver compares them with the Python path.
 #include <cmath>
 #include <cstdio>
@@ -98,6 +99,24 @@ int main() {
   for (float v : x) mean += v;
   std::printf("mma_mean %.6f\n", mean / ne);
   cudaDeviceSynchronize();
+  // the design driver as main.cpp calls it, on a small cell with two iterations
+  {
+    cfg::HomoConfig dc;
+    dc.init();
+    dc.reso[0] = dc.reso[1] = dc.reso[2] = 16;
+    dc.max_iter = 2;
+    dc.heatRatio[1] = 1e-4;
+    dc.winit = cfg::InitWay::IWP;
+    dc.model = cfg::Model::oc;
+    std::vector<float> rho = runCustom(dc);
+    double sum = 0;
+    for (float v : rho) sum += v;
+    std::printf("design_sum %.9e\n", sum);
+    ConvergeChecker cc(1e-3);
+    VolumeGovernor vg;
+    vg.volume_check(-1e-3f, 0.25f, 0.5f, 0);
+    std::printf("governor %.7f %d\n", vg.get_volume_bound(), int(cc.is_converge(0, 1.0)));
+  }
   std::printf("ok\n");
   return 0;
 }

@@ -57,3 +57,8 @@ def test_dropin_program_matches_python_path(tmp_path):
     want_vol = ora.oc_update(s, np.full((n, n, n), 0.3), 0.25, 0.001, 0.2, 0.5)[0].mean()
     assert abs(vals["oc_vol"][0] - want_vol) <= 1e-5
     assert abs(vals["mma_mean"][0] - 0.3) <= 2e-3
+    # runCustom through the C++ layer equals the Python driver bit for bit (same library calls)
+    from opentm_b200.driver import DesignConfig, InitWay, Model, run_custom
+    rho, _ = run_custom(DesignConfig(reso=16, max_iter=2, heatRatio=(1.0, 1e-4), winit=InitWay.IWP, model=Model.oc))
+    assert vals["design_sum"][0] == pytest.approx(float(rho.astype(np.float64).sum()), rel=1e-9)
+    assert vals["governor"] == [pytest.approx(0.25, abs=1e-7), 0.0]
