@@ -3,9 +3,11 @@
 // (optimization/mmaOptimizer.cu:18-78, optimization/mmaOpt.cu:429-1062, mmaOpt.cpp:38-73).
 //
 // Every pass over the n design variables is one kernel that also reduces what the next step
-// needs (sums with a fixed-order last-block finalisation, maxima), so a Newton step costs a
-// handful of kernels and one small device-to-host copy per decision; the (m+1) x (m+1) KKT
-// system (m <= 8) is solved in FP64 on the host, where the reference used Eigen.
+// needs (sums with a fixed-order last-block finalisation, maxima). A Newton step is two passes:
+// the step bounds of the direction, then the line-search trial, which recomputes the direction,
+// writes the trial point to spare arrays and reduces both the residual there and the next Newton
+// system (accepting the step swaps the arrays). The (m+1) x (m+1) KKT system (m <= 8) is solved
+// in FP64 on the host, where the reference used Eigen.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -26,7 +28,8 @@ struct MVec {
   double v[kMmaMaxM];
 };
 
-// Work arrays of one subsolve, n (or m * n) doubles each.
+// Work arrays of one subsolve, n (or m * n) doubles each. dx, dxsi, deta hold the line search's
+// trial point, which trades places with xs, xsi, eta when it is accepted.
 struct MmaWork {
   size_t n = 0;
   int m = 0;
@@ -38,7 +41,7 @@ struct MmaWork {
   double* host = nullptr;      // pinned, 96
 };
 
-constexpr int kMmaSlots = 96;
+constexpr int kMmaSlots = 128;  // >= 2 + 3 m + m^2 for m <= 8
 
 template <int NM>
 __device__ __forceinline__ void block_reduce_max(double (&v)[NM], double* smem) {
@@ -159,119 +162,196 @@ __global__ void __launch_bounds__(256) k_mma_setup(size_t n, int itn, const doub
   reduce_to_result<M, 1>(bs, dummy, w.partials, w.result, w.counter);
 }
 
-// Residual of the relaxed KKT conditions at x + steg dx (steg = 0: the current point):
-// result = [sum of squares, max |.|] of the n-part and gvec_i = sum_j P/ux + Q/xl.
+// The per-variable data a subsolver pass reads: the point, its bounds and the approximation.
 template <int M>
-__global__ void __launch_bounds__(256) k_mma_resid(double steg, MVec lam, double epsi, const double* __restrict__ low,
-                                                   const double* __restrict__ upp, MmaWork w) {
-  const size_t n = w.n;
-  double s[M + 1];
-  double mx[1] = {0.0};
+struct MmaElem {
+  double x, xsi, eta, low, upp, al, be, p0, q0, P[M], Q[M];
+};
+
+template <int M>
+__device__ __forceinline__ void load_elem(const MmaWork& w, const double* __restrict__ low,
+                                          const double* __restrict__ upp, size_t j, MmaElem<M>& e) {
+  e.x = w.xs[j];
+  e.xsi = w.xsi[j];
+  e.eta = w.eta[j];
+  e.low = low[j];
+  e.upp = upp[j];
+  e.al = w.alfa[j];
+  e.be = w.beta[j];
+  e.p0 = w.p0[j];
+  e.q0 = w.q0[j];
 #pragma unroll
-  for (int i = 0; i <= M; i++) s[i] = 0.0;
-  for (size_t j = size_t(blockIdx.x) * blockDim.x + threadIdx.x; j < n; j += size_t(gridDim.x) * blockDim.x) {
-    const double x = w.xs[j] + steg * w.dx[j];
-    const double xsi = w.xsi[j] + steg * w.dxsi[j];
-    const double eta = w.eta[j] + steg * w.deta[j];
-    const double uxi = 1.0 / (upp[j] - x), xli = 1.0 / (x - low[j]);
-    double plam = w.p0[j], qlam = w.q0[j];
-#pragma unroll
-    for (int i = 0; i < M; i++) {
-      const double Pij = w.P[i * n + j], Qij = w.Q[i * n + j];
-      plam += Pij * lam.v[i];
-      qlam += Qij * lam.v[i];
-      s[1 + i] += Pij * uxi + Qij * xli;
-    }
-    const double rex = plam * uxi * uxi - qlam * xli * xli - xsi + eta;
-    const double rexsi = xsi * (x - w.alfa[j]) - epsi;
-    const double reeta = eta * (w.beta[j] - x) - epsi;
-    s[0] += rex * rex + rexsi * rexsi + reeta * reeta;
-    mx[0] = fmax(mx[0], fmax(fabs(rex), fmax(fabs(rexsi), fabs(reeta))));
+  for (int i = 0; i < M; i++) {
+    e.P[i] = w.P[i * w.n + j];
+    e.Q[i] = w.Q[i * w.n + j];
   }
-  reduce_to_result<M + 1, 1>(s, mx, w.partials, w.result, w.counter);
 }
 
-// Newton system pieces at the current point: gvec, GG (delx / diagx), GG diag(1/diagx) GG^T.
+// Elements j and j + 1 (j even; n even and every array 16-byte aligned): one 16-byte load per
+// array, twice the bytes in flight per instruction.
 template <int M>
-__global__ void __launch_bounds__(256) k_mma_newton(MVec lam, double epsi, const double* __restrict__ low,
+__device__ __forceinline__ void load_pair(const MmaWork& w, const double* __restrict__ low,
+                                          const double* __restrict__ upp, size_t j, MmaElem<M>& a, MmaElem<M>& b) {
+  auto ld = [j](const double* p, double& u, double& v) {
+    const double2 t = *reinterpret_cast<const double2*>(p + j);
+    u = t.x;
+    v = t.y;
+  };
+  ld(w.xs, a.x, b.x);
+  ld(w.xsi, a.xsi, b.xsi);
+  ld(w.eta, a.eta, b.eta);
+  ld(low, a.low, b.low);
+  ld(upp, a.upp, b.upp);
+  ld(w.alfa, a.al, b.al);
+  ld(w.beta, a.be, b.be);
+  ld(w.p0, a.p0, b.p0);
+  ld(w.q0, a.q0, b.q0);
+#pragma unroll
+  for (int i = 0; i < M; i++) {
+    ld(w.P + i * w.n, a.P[i], b.P[i]);
+    ld(w.Q + i * w.n, a.Q[i], b.Q[i]);
+  }
+}
+
+// Newton direction of x, xsi, eta at e for multiplier lam and its step dlam (subsolv's dx, dxsi,
+// deta, optimization/mmaOpt.cu:429-830), shared by the two passes below so both see the same
+// values without storing them. The five distinct denominators are inverted once.
+template <int M>
+__device__ __forceinline__ void mma_dir(const MmaElem<M>& e, const MVec& lam, const MVec& dlam, double epsi,
+                                        double* dx, double* dxsi, double* deta, double* rxa_out, double* rbx_out) {
+  const double x = e.x;
+  const double rux = 1.0 / (e.upp - x), rxl = 1.0 / (x - e.low);
+  const double rux2 = rux * rux, rxl2 = rxl * rxl;
+  const double rxa = 1.0 / (x - e.al), rbx = 1.0 / (e.be - x);
+  double plam = e.p0, qlam = e.q0, gl = 0.0;
+#pragma unroll
+  for (int i = 0; i < M; i++) {
+    plam += e.P[i] * lam.v[i];
+    qlam += e.Q[i] * lam.v[i];
+    gl += (e.P[i] * rux2 - e.Q[i] * rxl2) * dlam.v[i];
+  }
+  const double dpsidx = plam * rux2 - qlam * rxl2;
+  const double delx = dpsidx - epsi * rxa + epsi * rbx;
+  const double diagx = 2.0 * (plam * rux2 * rux + qlam * rxl2 * rxl) + e.xsi * rxa + e.eta * rbx;
+  const double rd = 1.0 / diagx;
+  *dx = -(delx + gl) * rd;
+  *dxsi = -e.xsi + epsi * rxa - e.xsi * *dx * rxa;
+  *deta = -e.eta + epsi * rbx + e.eta * *dx * rbx;
+  *rxa_out = rxa;
+  *rbx_out = rbx;
+}
+
+// The line search's step bounds: the largest ratios -1.01 dxsi/xsi, -1.01 deta/eta,
+// -1.01 dx/(x - alfa), 1.01 dx/(beta - x), without storing the direction (the trial pass
+// recomputes it). VW consecutive variables per loop step.
+template <int M, int VW>
+__global__ void __launch_bounds__(256) k_mma_dirmax(MVec lam, MVec dlam, double epsi, const double* __restrict__ low,
                                                     const double* __restrict__ upp, MmaWork w) {
-  const size_t n = w.n;
-  constexpr int NS = M + M + M * M;
-  double s[NS];
-  double dummy[1] = {-1e300};
-#pragma unroll
-  for (int i = 0; i < NS; i++) s[i] = 0.0;
-  for (size_t j = size_t(blockIdx.x) * blockDim.x + threadIdx.x; j < n; j += size_t(gridDim.x) * blockDim.x) {
-    const double x = w.xs[j], al = w.alfa[j], be = w.beta[j];
-    const double ux1 = upp[j] - x, xl1 = x - low[j];
-    const double ux2 = ux1 * ux1, xl2 = xl1 * xl1;
-    double plam = w.p0[j], qlam = w.q0[j];
-    double GG[M];
-#pragma unroll
-    for (int i = 0; i < M; i++) {
-      const double Pij = w.P[i * n + j], Qij = w.Q[i * n + j];
-      plam += Pij * lam.v[i];
-      qlam += Qij * lam.v[i];
-      s[i] += Pij / ux1 + Qij / xl1;
-      GG[i] = Pij / ux2 - Qij / xl2;
-    }
-    const double dpsidx = plam / ux2 - qlam / xl2;
-    const double delx = dpsidx - epsi / (x - al) + epsi / (be - x);
-    const double diagx = 2.0 * (plam / (ux2 * ux1) + qlam / (xl2 * xl1)) + w.xsi[j] / (x - al) + w.eta[j] / (be - x);
-    const double dd = delx / diagx, id = 1.0 / diagx;
-#pragma unroll
-    for (int i = 0; i < M; i++) {
-      s[M + i] += GG[i] * dd;
-#pragma unroll
-      for (int k = 0; k < M; k++) s[2 * M + i * M + k] += GG[i] * GG[k] * id;
-    }
-  }
-  reduce_to_result<NS, 1>(s, dummy, w.partials, w.result, w.counter);
-}
-
-// Search direction of x, xsi, eta and the largest step ratios for the line search.
-template <int M>
-__global__ void __launch_bounds__(256) k_mma_direction(MVec lam, MVec dlam, double epsi,
-                                                       const double* __restrict__ low, const double* __restrict__ upp,
-                                                       MmaWork w) {
-  const size_t n = w.n;
   double s[1] = {0.0};
   double mx[4] = {-1e300, -1e300, -1e300, -1e300};
-  for (size_t j = size_t(blockIdx.x) * blockDim.x + threadIdx.x; j < n; j += size_t(gridDim.x) * blockDim.x) {
-    const double x = w.xs[j], al = w.alfa[j], be = w.beta[j], xsi = w.xsi[j], eta = w.eta[j];
-    const double ux1 = upp[j] - x, xl1 = x - low[j];
-    const double ux2 = ux1 * ux1, xl2 = xl1 * xl1;
-    double plam = w.p0[j], qlam = w.q0[j], gl = 0.0;
+  const size_t nq = w.n / VW;
+  for (size_t q = size_t(blockIdx.x) * blockDim.x + threadIdx.x; q < nq; q += size_t(gridDim.x) * blockDim.x) {
+    MmaElem<M> e[VW];
+    if (VW == 2)
+      load_pair<M>(w, low, upp, 2 * q, e[0], e[VW - 1]);
+    else
+      load_elem<M>(w, low, upp, q, e[0]);
 #pragma unroll
-    for (int i = 0; i < M; i++) {
-      const double Pij = w.P[i * n + j], Qij = w.Q[i * n + j];
-      plam += Pij * lam.v[i];
-      qlam += Qij * lam.v[i];
-      gl += (Pij / ux2 - Qij / xl2) * dlam.v[i];
+    for (int v = 0; v < VW; v++) {
+      double dx, dxsi, deta, rxa, rbx;
+      mma_dir<M>(e[v], lam, dlam, epsi, &dx, &dxsi, &deta, &rxa, &rbx);
+      mx[0] = fmax(mx[0], -1.01 * dxsi / e[v].xsi);
+      mx[1] = fmax(mx[1], -1.01 * deta / e[v].eta);
+      mx[2] = fmax(mx[2], -1.01 * dx * rxa);
+      mx[3] = fmax(mx[3], 1.01 * dx * rbx);
     }
-    const double dpsidx = plam / ux2 - qlam / xl2;
-    const double delx = dpsidx - epsi / (x - al) + epsi / (be - x);
-    const double diagx = 2.0 * (plam / (ux2 * ux1) + qlam / (xl2 * xl1)) + xsi / (x - al) + eta / (be - x);
-    const double dx = -delx / diagx - gl / diagx;
-    const double dxsi = -xsi + epsi / (x - al) - (xsi * dx) / (x - al);
-    const double deta = -eta + epsi / (be - x) + (eta * dx) / (be - x);
-    w.dx[j] = dx;
-    w.dxsi[j] = dxsi;
-    w.deta[j] = deta;
-    mx[0] = fmax(mx[0], -1.01 * dxsi / xsi);
-    mx[1] = fmax(mx[1], -1.01 * deta / eta);
-    mx[2] = fmax(mx[2], -1.01 * dx / (x - al));
-    mx[3] = fmax(mx[3], 1.01 * dx / (be - x));
   }
   reduce_to_result<1, 4>(s, mx, w.partials, w.result, w.counter);
 }
 
-__global__ void __launch_bounds__(256) k_mma_commit(double steg, MmaWork w) {
-  for (size_t j = size_t(blockIdx.x) * blockDim.x + threadIdx.x; j < w.n; j += size_t(gridDim.x) * blockDim.x) {
-    w.xs[j] += steg * w.dx[j];
-    w.xsi[j] += steg * w.dxsi[j];
-    w.eta[j] += steg * w.deta[j];
+// One pass at the trial point x + steg dx (steg = 0: the committed point, nothing written): the
+// relaxed KKT residual with the trial multiplier lam ([sum of squares, max |.|] of the n-part and
+// gvec_i = sum_j P/ux + Q/xl) and, at the same point, the pieces of the next Newton system (gvec,
+// GG delx/diagx, GG diag(1/diagx) GG^T), so an accepted step needs no further pass. The trial
+// point goes to xs_out / xsi_out / eta_out; accepting it is a pointer swap. VW consecutive
+// variables per loop step.
+// result = [resid sum of squares, resid gvec (M), newton gvec (M), GG delx/diagx (M),
+//           GG diag(1/diagx) GG^T (M*M), resid max |.|].
+template <int M, int VW>
+__global__ void __launch_bounds__(256) k_mma_trial(double steg, MVec lam, MVec lam_dir, MVec dlam, double epsi,
+                                                   double epsi_dir, const double* __restrict__ low,
+                                                   const double* __restrict__ upp, double* xs_out, double* xsi_out,
+                                                   double* eta_out, MmaWork w) {
+  constexpr int NS = 1 + M + M + M + M * M;
+  double s[NS];
+  double mx[1] = {0.0};
+#pragma unroll
+  for (int i = 0; i < NS; i++) s[i] = 0.0;
+  const size_t nq = w.n / VW;
+  for (size_t q = size_t(blockIdx.x) * blockDim.x + threadIdx.x; q < nq; q += size_t(gridDim.x) * blockDim.x) {
+    MmaElem<M> e[VW];
+    if (VW == 2)
+      load_pair<M>(w, low, upp, 2 * q, e[0], e[VW - 1]);
+    else
+      load_elem<M>(w, low, upp, q, e[0]);
+#pragma unroll
+    for (int v = 0; v < VW; v++) {
+      if (steg != 0.0) {
+        double dx, dxsi, deta, r0, r1;
+        mma_dir<M>(e[v], lam_dir, dlam, epsi_dir, &dx, &dxsi, &deta, &r0, &r1);
+        e[v].x = e[v].x + steg * dx;
+        e[v].xsi = e[v].xsi + steg * dxsi;
+        e[v].eta = e[v].eta + steg * deta;
+      }
+      const double x = e[v].x, xsi = e[v].xsi, eta = e[v].eta, al = e[v].al, be = e[v].be;
+      // residual
+      const double uxi = 1.0 / (e[v].upp - x), xli = 1.0 / (x - e[v].low);
+      double plam = e[v].p0, qlam = e[v].q0;
+#pragma unroll
+      for (int i = 0; i < M; i++) {
+        plam += e[v].P[i] * lam.v[i];
+        qlam += e[v].Q[i] * lam.v[i];
+        s[1 + i] += e[v].P[i] * uxi + e[v].Q[i] * xli;
+      }
+      const double rex = plam * uxi * uxi - qlam * xli * xli - xsi + eta;
+      const double rexsi = xsi * (x - al) - epsi;
+      const double reeta = eta * (be - x) - epsi;
+      s[0] += rex * rex + rexsi * rexsi + reeta * reeta;
+      mx[0] = fmax(mx[0], fmax(fabs(rex), fmax(fabs(rexsi), fabs(reeta))));
+      // Newton system pieces (its gvec is the residual's), with the reciprocals above and of
+      // x - alfa, beta - x, diagx
+      const double rux2 = uxi * uxi, rxl2 = xli * xli;
+      const double rxa = 1.0 / (x - al), rbx = 1.0 / (be - x);
+      double GG[M];
+#pragma unroll
+      for (int i = 0; i < M; i++) GG[i] = e[v].P[i] * rux2 - e[v].Q[i] * rxl2;
+      const double dpsidx = plam * rux2 - qlam * rxl2;
+      const double delx = dpsidx - epsi * rxa + epsi * rbx;
+      const double diagx = 2.0 * (plam * rux2 * uxi + qlam * rxl2 * xli) + xsi * rxa + eta * rbx;
+      const double id = 1.0 / diagx, dd = delx * id;
+#pragma unroll
+      for (int i = 0; i < M; i++) {
+        s[1 + 2 * M + i] += GG[i] * dd;
+#pragma unroll
+        for (int k = 0; k < M; k++) s[1 + 3 * M + i * M + k] += GG[i] * GG[k] * id;
+      }
+    }
+    if (steg != 0.0) {
+      if (VW == 2) {
+        const size_t j = 2 * q;
+        *reinterpret_cast<double2*>(xs_out + j) = make_double2(e[0].x, e[VW - 1].x);
+        *reinterpret_cast<double2*>(xsi_out + j) = make_double2(e[0].xsi, e[VW - 1].xsi);
+        *reinterpret_cast<double2*>(eta_out + j) = make_double2(e[0].eta, e[VW - 1].eta);
+      } else {
+        xs_out[q] = e[0].x;
+        xsi_out[q] = e[0].xsi;
+        eta_out[q] = e[0].eta;
+      }
+    }
   }
+#pragma unroll
+  for (int i = 0; i < M; i++) s[1 + M + i] = s[1 + i];
+  reduce_to_result<NS, 1>(s, mx, w.partials, w.result, w.counter);
 }
 
 __global__ void k_mma_finish(size_t n, double* xvar, double* xold1, double* xold2, const double* xs) {
@@ -388,24 +468,26 @@ struct LaunchSetup {
     k_mma_setup<M><<<nb, 256, 0, s>>>(n, itn, xvar, xmin, xmax, xold1, xold2, df0dx, dgdx, ldg, low, upp, move, w);
   }
 };
+
 template <int M>
-struct LaunchResid {
-  static void run(int nb, cudaStream_t s, double steg, MVec lam, double epsi, const double* low, const double* upp,
-                  MmaWork w) {
-    k_mma_resid<M><<<nb, 256, 0, s>>>(steg, lam, epsi, low, upp, w);
+struct LaunchDirmax {
+  static void run(int nb, bool pairs, cudaStream_t s, MVec lam, MVec dlam, double epsi, const double* low,
+                  const double* upp, MmaWork w) {
+    if (pairs)
+      k_mma_dirmax<M, 2><<<nb, 256, 0, s>>>(lam, dlam, epsi, low, upp, w);
+    else
+      k_mma_dirmax<M, 1><<<nb, 256, 0, s>>>(lam, dlam, epsi, low, upp, w);
   }
 };
 template <int M>
-struct LaunchNewton {
-  static void run(int nb, cudaStream_t s, MVec lam, double epsi, const double* low, const double* upp, MmaWork w) {
-    k_mma_newton<M><<<nb, 256, 0, s>>>(lam, epsi, low, upp, w);
-  }
-};
-template <int M>
-struct LaunchDirection {
-  static void run(int nb, cudaStream_t s, MVec lam, MVec dlam, double epsi, const double* low, const double* upp,
+struct LaunchTrial {
+  static void run(int nb, bool pairs, cudaStream_t s, double steg, MVec lam, MVec lam_dir, MVec dlam, double epsi,
+                  double epsi_dir, const double* low, const double* upp, double* xo, double* xsio, double* etao,
                   MmaWork w) {
-    k_mma_direction<M><<<nb, 256, 0, s>>>(lam, dlam, epsi, low, upp, w);
+    if (pairs)
+      k_mma_trial<M, 2><<<nb, 256, 0, s>>>(steg, lam, lam_dir, dlam, epsi, epsi_dir, low, upp, xo, xsio, etao, w);
+    else
+      k_mma_trial<M, 1><<<nb, 256, 0, s>>>(steg, lam, lam_dir, dlam, epsi, epsi_dir, low, upp, xo, xsio, etao, w);
   }
 };
 
@@ -453,36 +535,55 @@ static otm_status mmasub_run(cudaStream_t s, int m, size_t n, int itn, double* x
     acc(ze * zz - epsi);
     for (int i = 0; i < m; i++) acc(ll[i] * ss[i] - epsi);
   };
-  // residual norm / max at (x + steg dx, y, z, lam, ...)
-  auto residual = [&](double steg, const std::vector<double>& yy, double zz, const std::vector<double>& ll,
-                      const std::vector<double>& mm, double ze, const std::vector<double>& ss, double* nrm,
-                      double* mxv) -> otm_status {
-    for (int i = 0; i < m; i++) lamv.v[i] = ll[i];
-    dispatch_m<LaunchResid>(m, nb, s, steg, lamv, epsi, (const double*)low, (const double*)upp, w);
+  // One pass at x + steg * (direction for lam_dir, dlam): residual norm / max with the trial
+  // multipliers, and the Newton pieces there (cached in newt: gvec, GG delx/diagx, GG GG^T/diagx).
+  // With steg != 0 the trial point is written to the spare arrays w.dx, w.dxsi, w.deta.
+  const int NS = 1 + 3 * m + m * m;
+  // pairs of variables per loop step when every array the passes read is 16-byte aligned at
+  // every row (n even; the work arrays come from the allocator, low and upp from the caller)
+  // (m <= 4: beyond that the pair of elements no longer fits the registers)
+  const bool pairs = m <= 4 && n % 2 == 0 && (reinterpret_cast<uintptr_t>(low) % 16) == 0 &&
+                     (reinterpret_cast<uintptr_t>(upp) % 16) == 0;
+  const int nbp = int(std::min<size_t>(kMaxPartials, std::max<size_t>(1, (n / (pairs ? 2 : 1) + 255) / 256)));
+  std::vector<double> newt(size_t(2 * m + m * m));
+  auto trial = [&](double steg, const std::vector<double>& yy, double zz, const std::vector<double>& ll,
+                   const std::vector<double>& mm, double ze, const std::vector<double>& ss,
+                   const std::vector<double>& ldir, const MVec& dl, double* nrm, double* mxv) -> otm_status {
+    MVec lt{}, ld{};
+    for (int i = 0; i < m; i++) {
+      lt.v[i] = ll[i];
+      ld.v[i] = ldir[i];
+    }
+    dispatch_m<LaunchTrial>(m, nbp, pairs, s, steg, lt, ld, dl, epsi, epsi, (const double*)low, (const double*)upp,
+                            w.dx, w.dxsi, w.deta, w);
     L++;
-    OTM_CHECK_LAUNCH("k_mma_resid");
-    OTM_TRY(fetch(w, s, m + 2));
-    double n2 = w.host[0], mx = w.host[m + 1];
+    OTM_CHECK_LAUNCH("k_mma_trial");
+    OTM_TRY(fetch(w, s, NS + 1));
+    double n2 = w.host[0], mx = w.host[NS];
     for (int i = 0; i < m; i++) gvec[i] = w.host[1 + i];
+    for (size_t i = 0; i < newt.size(); i++) newt[i] = w.host[1 + m + i];
     m_residual(yy, zz, ll, mm, ze, ss, &n2, &mx);
     *nrm = std::sqrt(n2);
     *mxv = mx;
     return OTM_OK;
   };
+  // the trial point becomes the committed one (the work arrays keep owning both sets)
+  auto accept = [&]() {
+    std::swap(w.xs, w.dx);
+    std::swap(w.xsi, w.dxsi);
+    std::swap(w.eta, w.deta);
+  };
 
   std::vector<double> dy(m), dmu(m), ds(m), dl(m), yo(m), lo(m), muo(m), so(m);
   while (epsi > kEpsiMin) {
     double residunorm, residumax;
-    OTM_TRY(residual(0.0, y, z, lam, mu, zet, sv, &residunorm, &residumax));
+    OTM_TRY(trial(0.0, y, z, lam, mu, zet, sv, lam, dlamv, &residunorm, &residumax));
     int ittt = 0;
     while (residumax > 0.9 * epsi && ittt < 200) {
       ittt++;
       for (int i = 0; i < m; i++) lamv.v[i] = lam[i];
-      dispatch_m<LaunchNewton>(m, nb, s, lamv, epsi, (const double*)low, (const double*)upp, w);
-      L++;
-      OTM_CHECK_LAUNCH("k_mma_newton");
-      OTM_TRY(fetch(w, s, 2 * m + m * m));
-      for (int i = 0; i < m; i++) gvec[i] = w.host[i];
+      const double* hn = newt.data();  // Newton pieces at the committed point
+      for (int i = 0; i < m; i++) gvec[i] = hn[i];
       double adl = 0.0;
       for (int i = 0; i < m; i++) adl += a[i] * lam[i];
       const double delz = a0 - adl - epsi / z;
@@ -492,8 +593,8 @@ static otm_status mmasub_run(cudaStream_t s, int m, size_t n, int itn, double* x
         dely[i] = c[i] + d[i] * y[i] - lam[i] - epsi / y[i];
         const double dellam = gvec[i] - a[i] * z - y[i] - b[i] + epsi / lam[i];
         diagy[i] = d[i] + mu[i] / y[i];
-        bb[i] = dellam + dely[i] / diagy[i] - w.host[m + i];
-        for (int k = 0; k < m; k++) AA[size_t(i) * (m + 1) + k] = w.host[2 * m + i * m + k];
+        bb[i] = dellam + dely[i] / diagy[i] - hn[m + i];
+        for (int k = 0; k < m; k++) AA[size_t(i) * (m + 1) + k] = hn[2 * m + i * m + k];
         AA[size_t(i) * (m + 1) + i] += sv[i] / lam[i] + 1.0 / diagy[i];
         AA[size_t(i) * (m + 1) + m] = a[i];
         AA[size_t(m) * (m + 1) + i] = a[i];
@@ -513,9 +614,9 @@ static otm_status mmasub_run(cudaStream_t s, int m, size_t n, int itn, double* x
         dlamv.v[i] = dl[i];
       }
       const double dzet = -zet + epsi / z - zet * dz / z;
-      dispatch_m<LaunchDirection>(m, nb, s, lamv, dlamv, epsi, (const double*)low, (const double*)upp, w);
+      dispatch_m<LaunchDirmax>(m, nbp, pairs, s, lamv, dlamv, epsi, (const double*)low, (const double*)upp, w);
       L++;
-      OTM_CHECK_LAUNCH("k_mma_direction");
+      OTM_CHECK_LAUNCH("k_mma_dirmax");
       OTM_TRY(fetch(w, s, 5));
       double stm = std::max(w.host[1], w.host[2]);  // xsi, eta parts
       for (int i = 0; i < m; i++) {
@@ -538,7 +639,7 @@ static otm_status mmasub_run(cudaStream_t s, int m, size_t n, int itn, double* x
       so = sv;
       const double zo = z, zeto = zet;
       int itto = 0;
-      double resinew = 2 * residunorm, resimax = residumax, used = 0.0;
+      double resinew = 2 * residunorm, resimax = residumax;
       while (resinew > residunorm && itto < 50) {
         itto++;
         for (int i = 0; i < m; i++) {
@@ -549,13 +650,10 @@ static otm_status mmasub_run(cudaStream_t s, int m, size_t n, int itn, double* x
         }
         z = zo + steg * dz;
         zet = zeto + steg * dzet;
-        OTM_TRY(residual(steg, y, z, lam, mu, zet, sv, &resinew, &resimax));
-        used = steg;
+        OTM_TRY(trial(steg, y, z, lam, mu, zet, sv, lo, dlamv, &resinew, &resimax));
         steg /= 2;
       }
-      k_mma_commit<<<nb, 256, 0, s>>>(used, w);
-      L++;
-      OTM_CHECK_LAUNCH("k_mma_commit");
+      accept();  // the last point tried, as the reference commits after its line search
       residunorm = resinew;
       residumax = resimax;
     }
