@@ -88,6 +88,12 @@ otm_status Homo::alloc(void** p, size_t bytes) {
 }
 
 Homo::~Homo() {
+  if (side) {
+    cudaStreamSynchronize(side);  // the coarse-operator chain may still use the buffers
+    cudaStreamDestroy(side);
+  }
+  if (ev_fork) cudaEventDestroy(ev_fork);
+  if (ev_coarse) cudaEventDestroy(ev_coarse);
   for (auto& g : graphs)
     if (g.exec) cudaGraphExecDestroy(g.exec);
   if (loop_exec) cudaGraphExecDestroy(loop_exec);
@@ -161,6 +167,9 @@ otm_status Homo::build(const otm_config& c, cudaStream_t ext_stream, cudaMemPool
     OTM_CUDA(cudaEventCreateWithFlags(&ev_in, cudaEventDisableTiming));
     OTM_CUDA(cudaEventCreateWithFlags(&ev_out, cudaEventDisableTiming));
   }
+  OTM_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+  OTM_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+  OTM_CUDA(cudaEventCreateWithFlags(&ev_coarse, cudaEventDisableTiming));
   if (cfg.profile)
     for (int a = 0; a < 2; a++)
       for (int j = 0; j < kMaxChunk; j++) OTM_CUDA(cudaEventCreate(&prof_ev[a][j]));
@@ -286,6 +295,13 @@ otm_status Homo::build(const otm_config& c, cudaStream_t ext_stream, cudaMemPool
   return OTM_OK;
 }
 
+otm_status Homo::join_coarse() {
+  if (!coarse_pending) return OTM_OK;
+  OTM_CUDA(cudaStreamWaitEvent(stream, ev_coarse, 0));
+  coarse_pending = false;
+  return OTM_OK;
+}
+
 otm_status Homo::enter() {
   if (external) return OTM_OK;
   OTM_CUDA(cudaEventRecord(ev_in, user_stream));
@@ -311,6 +327,7 @@ otm_status Homo::update(const float* kin, int pitchT) {
   if (pitchT <= 0) pitchT = d0.nx;
   if (pitchT < d0.nx) return invalid("pitchT smaller than the x resolution");
   OTM_TRY(enter());
+  OTM_TRY(join_coarse());  // a previous field's coarse chain may still read ks
   const size_t nv = d0.nv();
   OTM_CUDA(cudaMemsetAsync(flags, 0, 2 * sizeof(int), stream));  // import / coarsest status of this field
   k_import<<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(d0, kin, pitchT, cfg.power_penal, ks, kraw, flags);
@@ -328,20 +345,23 @@ otm_status Homo::update(const float* kin, int pitchT) {
     OTM_CHECK_LAUNCH("k_to16");
     launched(2);
   }
+  // the coarse chain on the side stream, after the import (and the 16-bit copies)
+  OTM_CUDA(cudaEventRecord(ev_fork, stream));
+  OTM_CUDA(cudaStreamWaitEvent(side, ev_fork, 0));
   for (int l = 1; l < L; l++) {
     const bool cb = (l < L - 1);  // smoothed levels use the colour-blocked stencil order
     const size_t nvc = lv[l].d.nv();
     if (l == 1)
-      k_galerkin_fine<<<ceil_div(nvc, kBlock), kBlock, 0, stream>>>(lv[0].d, lv[1].d, ks, table, lv[1].st, cb,
-                                                                    mixed ? kmax_bits : nullptr, op.c0);
+      k_galerkin_fine<<<ceil_div(nvc, kBlock), kBlock, 0, side>>>(lv[0].d, lv[1].d, ks, table, lv[1].st, cb,
+                                                                  mixed ? kmax_bits : nullptr, op.c0);
     else
-      k_galerkin_coarse<<<ceil_div(nvc, kBlock), kBlock, 0, stream>>>(lv[l - 1].d, lv[l].d, lv[l - 1].st, lv[l].st,
-                                                                      cb);
+      k_galerkin_coarse<<<ceil_div(nvc, kBlock), kBlock, 0, side>>>(lv[l - 1].d, lv[l].d, lv[l - 1].st, lv[l].st,
+                                                                    cb);
     OTM_CHECK_LAUNCH("galerkin");
     launched(1);
   }
   if (L == 1) {
-    k_fine_stencil<<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(d0, ks, op, lv[0].st);
+    k_fine_stencil<<<ceil_div(nv, kBlock), kBlock, 0, side>>>(d0, ks, op, lv[0].st);
     OTM_CHECK_LAUNCH("k_fine_stencil");
     launched(1);
   }
@@ -350,11 +370,13 @@ otm_status Homo::update(const float* kin, int pitchT) {
     const int use_smem = abytes <= size_t(kMaxDynSmem);
     if (use_smem)
       OTM_CUDA(cudaFuncSetAttribute(k_coarsest_build, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
-    k_coarsest_build<<<1, 1024, use_smem ? abytes : 0, stream>>>(lv.back().d, lv.back().st, Ainv, flags + 1,
-                                                                  use_smem);
+    k_coarsest_build<<<1, 1024, use_smem ? abytes : 0, side>>>(lv.back().d, lv.back().st, Ainv, flags + 1,
+                                                                use_smem);
   }
   OTM_CHECK_LAUNCH("k_coarsest_build");
   launched(1);
+  OTM_CUDA(cudaEventRecord(ev_coarse, side));
+  coarse_pending = true;
   updated = true;
   solved = false;
   return leave();
@@ -575,6 +597,7 @@ void Homo::iteration(int j) {
 }
 
 otm_status Homo::run_chunk(int iters) {
+  OTM_TRY(join_coarse());
   if (!cfg.use_graphs) {
     for (int i = 0; i < iters; i++) iteration(i);
     OTM_CHECK_LAUNCH("iteration");
@@ -651,6 +674,7 @@ otm_status Homo::check_flags() {
 // body is one iteration followed by k_loop_ctrl, so a solve needs no host round trip until it
 // has finished. Built on first use (and again when the solver type changes).
 otm_status Homo::launch_loop() {
+  OTM_TRY(join_coarse());
   if (!loop_exec || loop_solver != cfg.solver) {
     if (loop_exec) cudaGraphExecDestroy(loop_exec);
     loop_exec = nullptr;
@@ -745,8 +769,9 @@ void Homo::launch_solve_start() {
 // flags_host / sc_host.
 otm_status Homo::launch_device_solve(bool with_heat) {
   const size_t nv = lv[0].d.nv();
-  launch_solve_start();
+  launch_solve_start();  // needs only the conductivities: runs alongside the coarse chain
   OTM_CHECK_LAUNCH("solve init");
+  OTM_TRY(join_coarse());
   OTM_TRY(launch_loop());
   if (mixed) {
     k_x64_to_x<<<ceil_div(3 * nv, kBlock), kBlock, 0, stream>>>(3 * nv, x64, x);
@@ -769,6 +794,7 @@ otm_status Homo::solve_impl(bool with_heat) {
   const bool device_loop = cfg.use_graphs && !cfg.profile;
   heat_ready = false;
   if (!device_loop) {
+    OTM_TRY(join_coarse());
     OTM_CUDA(cudaMemcpyAsync(flags_host, flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream));
     OTM_CUDA(cudaStreamSynchronize(stream));
     OTM_TRY(check_flags());

@@ -37,6 +37,12 @@ struct Homo {
   cudaStream_t stream = nullptr;       // private stream (graph capture needs a non-legacy stream)
   cudaStream_t user_stream = nullptr;  // ordering with the caller
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  // The coarse operators (Galerkin stencils of levels >= 1 and the coarsest inverse) are built
+  // on a side stream, concurrently with the solve start, which needs only the conductivities;
+  // ev_coarse marks their completion and join_coarse() orders the main stream after it.
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_coarse = nullptr;
+  bool coarse_pending = false;
   std::vector<Level> lv;
   TemplateMatrices tm{};
   FineOp op{};
@@ -96,6 +102,7 @@ struct Homo {
                    bool external_mode = false);
   void launch_solve_init();
   void launch_heat_matrix();
+  otm_status join_coarse();
   otm_status enter();
   otm_status leave();
   otm_status update(const float* kin, int pitchT);

@@ -394,6 +394,7 @@ static otm_status admit(otm_server* s, Request& r, int slot) {
   otm_status st = H.update(kdev, d0.nx);
   cudaFreeAsync(kdev, s->stream);
   OTM_TRY(st);
+  OTM_TRY(H.join_coarse());  // the batched kernels read the coarse stencils directly
   H.launch_solve_init();
   // descriptor of the request for the batched kernels
   ReqDesc D;

@@ -940,30 +940,39 @@ __device__ __forceinline__ void elem_energy(const Dims& d, size_t e, const float
   const size_t r00 = (size_t(y) + size_t(d.ny) * z) * d.nx, r10 = (size_t(y1) + size_t(d.ny) * z) * d.nx;
   const size_t r01 = (size_t(y) + size_t(d.ny) * z1) * d.nx, r11 = (size_t(y1) + size_t(d.ny) * z1) * d.nx;
   const size_t idx[8] = {r00 + x, r00 + x1, r10 + x, r10 + x1, r01 + x, r01 + x1, r11 + x, r11 + x1};
-  float dv[3][8];
+  // KE_ij depends only on the Hamming distance |i ^ j| (c0, c1, c2, c3 for 0..3 differing bits), so
+  // the 8-point Walsh-Hadamard transform W diagonalises it: KE = W diag(lam) W / 8 with lam_k =
+  // l(popcount k), l(0) = c0 + 3c1 + 3c2 + c3, l(1) = c0 + c1 - c2 - c3, l(2) = c0 - c1 - c2 + c3,
+  // l(3) = c0 - 3c1 + 3c2 - c3. Then E_ab = sum_k lam_k/8 w_a[k] w_b[k] with w = W (disp - chi).
+  float w[3][8];
 #pragma unroll
-  for (int c = 0; c < 3; c++)
+  for (int c = 0; c < 3; c++) {
 #pragma unroll
-    for (int j = 0; j < 8; j++) dv[c][j] = ef.disp[j][c] - __ldg(chi + c * nv + idx[j]);
-  // KE d using the Hamming structure: (KE d)_i = c0 d_i + c1 sum_{|i^j|=1} d_j + c2 sum_{|i^j|=2} d_j + c3 d_{7-i}
-  float Kd[3][8];
+    for (int j = 0; j < 8; j++) w[c][j] = ef.disp[j][c] - __ldg(chi + c * nv + idx[j]);
 #pragma unroll
-  for (int c = 0; c < 3; c++)
+    for (int s = 1; s < 8; s <<= 1)
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
-      const float s1 = dv[c][i ^ 1] + dv[c][i ^ 2] + dv[c][i ^ 4];
-      const float s2 = dv[c][i ^ 3] + dv[c][i ^ 5] + dv[c][i ^ 6];
-      Kd[c][i] = op.c0 * dv[c][i] + op.c1 * s1 + op.c2 * s2 + op.c3 * dv[c][i ^ 7];
-    }
+      for (int i = 0; i < 8; i++)
+        if (!(i & s)) {
+          const float a = w[c][i], b = w[c][i | s];
+          w[c][i] = a + b;
+          w[c][i | s] = a - b;
+        }
+  }
+  const float l0 = 0.125f * (op.c0 + 3.f * op.c1 + 3.f * op.c2 + op.c3);
+  const float l1 = 0.125f * (op.c0 + op.c1 - op.c2 - op.c3);
+  const float l2 = 0.125f * (op.c0 - op.c1 - op.c2 + op.c3);
+  const float l3 = 0.125f * (op.c0 - 3.f * op.c1 + 3.f * op.c2 - op.c3);
   int cnt = 0;
 #pragma unroll
   for (int a = 0; a < 3; a++)
 #pragma unroll
     for (int bq = a; bq < 3; bq++) {
-      float s = 0.f;
-#pragma unroll
-      for (int i = 0; i < 8; i++) s += dv[a][i] * Kd[bq][i];
-      E[cnt++] = s;
+      const float* u = w[a];
+      const float* v = w[bq];
+      const float s1 = u[1] * v[1] + u[2] * v[2] + u[4] * v[4];
+      const float s2 = u[3] * v[3] + u[5] * v[5] + u[6] * v[6];
+      E[cnt++] = l0 * (u[0] * v[0]) + l1 * s1 + l2 * s2 + l3 * (u[7] * v[7]);
     }
 }
 
