@@ -25,13 +25,58 @@ def launch_count() -> int:
     return int(lib().otm_launch_count())
 
 
-__all__ = ["launch_count", "Server", 
+__all__ = ["launch_count", "Server", "pinned_empty", "copy_to_device", "copy_to_host", 
     "HomoConfig", "Homogenization_H", "OCOptimizer", "MMAOptimizer", "DensityFilter", "OtmError", "lib",
     "WEIGHT_SPLINE4", "WEIGHT_LINEAR", "filter_forward", "filter_backward",
 ]
 
 WEIGHT_SPLINE4 = 0
 WEIGHT_LINEAR = 1
+
+
+class _HostBlock:
+    """Owner of one otm_host_alloc block; freed when the last array viewing it goes."""
+
+    def __init__(self, nbytes: int):
+        self.ptr = ctypes.c_void_p()
+        check(lib().otm_host_alloc(ctypes.c_size_t(nbytes), ctypes.byref(self.ptr)), "otm_host_alloc")
+
+    def __del__(self):
+        try:
+            if self.ptr:
+                lib().otm_host_free(self.ptr)
+        except Exception:
+            pass
+
+
+def pinned_empty(shape, dtype=np.float32) -> np.ndarray:
+    """A numpy array in page-locked host memory from otm_host_alloc (cudaHostAlloc): the fast
+    source and target of per-step host<->device copies (torch.from_numpy(a) is a pinned tensor)."""
+    dt = np.dtype(dtype)
+    count = int(np.prod(shape)) if np.ndim(shape) else int(shape)
+    blk = _HostBlock(max(count * dt.itemsize, 1))
+    buf = (ctypes.c_char * (count * dt.itemsize)).from_address(blk.ptr.value)
+    buf._otm_block = blk  # the array keeps buf alive, buf keeps the block
+    return np.frombuffer(buf, dtype=dt, count=count).reshape(shape)
+
+
+def copy_to_device(dst, src: np.ndarray, stream=None) -> None:
+    """Asynchronous copy of a host array (page-locked, e.g. from pinned_empty) into the CUDA
+    tensor dst on the current (or given) stream."""
+    if src.nbytes != dst.numel() * dst.element_size() or not src.flags.c_contiguous or not dst.is_contiguous():
+        raise ValueError("copy_to_device needs contiguous arrays of the same size")
+    check(lib().otm_copy_to_device(ctypes.c_void_p(_ptr(dst)), ctypes.c_void_p(src.ctypes.data),
+                                   ctypes.c_size_t(src.nbytes), ctypes.c_void_p(_stream(stream))),
+          "otm_copy_to_device")
+
+
+def copy_to_host(dst: np.ndarray, src, stream=None) -> None:
+    """Asynchronous copy of the CUDA tensor src into a host array (page-locked) on the current (or
+    given) stream; synchronise before reading dst."""
+    if dst.nbytes != src.numel() * src.element_size() or not dst.flags.c_contiguous or not src.is_contiguous():
+        raise ValueError("copy_to_host needs contiguous arrays of the same size")
+    check(lib().otm_copy_to_host(ctypes.c_void_p(dst.ctypes.data), ctypes.c_void_p(_ptr(src)),
+                                 ctypes.c_size_t(dst.nbytes), ctypes.c_void_p(_stream(stream))), "otm_copy_to_host")
 
 
 def _ptr(t) -> int:

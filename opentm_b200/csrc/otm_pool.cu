@@ -49,3 +49,38 @@ cudaError_t scratch_malloc(void** p, size_t bytes, cudaStream_t s) {
 }
 
 }  // namespace otm
+
+extern "C" {
+
+otm_status otm_host_alloc(size_t bytes, void** out) {
+  if (!out || bytes == 0) return OTM_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  const cudaError_t e = cudaHostAlloc(out, bytes, cudaHostAllocPortable);
+  if (e != cudaSuccess) {
+    *out = nullptr;
+    return otm::cuda_fail(e, "cudaHostAlloc");
+  }
+  return OTM_OK;
+}
+
+otm_status otm_copy_to_device(void* dst_dev, const void* src_host, size_t bytes, void* stream) {
+  if ((!dst_dev || !src_host) && bytes) return OTM_ERR_INVALID_ARGUMENT;
+  if (!bytes) return OTM_OK;
+  const cudaError_t e = cudaMemcpyAsync(dst_dev, src_host, bytes, cudaMemcpyHostToDevice, (cudaStream_t)stream);
+  return e == cudaSuccess ? OTM_OK : otm::cuda_fail(e, "otm_copy_to_device");
+}
+
+otm_status otm_copy_to_host(void* dst_host, const void* src_dev, size_t bytes, void* stream) {
+  if ((!dst_host || !src_dev) && bytes) return OTM_ERR_INVALID_ARGUMENT;
+  if (!bytes) return OTM_OK;
+  const cudaError_t e = cudaMemcpyAsync(dst_host, src_dev, bytes, cudaMemcpyDeviceToHost, (cudaStream_t)stream);
+  return e == cudaSuccess ? OTM_OK : otm::cuda_fail(e, "otm_copy_to_host");
+}
+
+otm_status otm_host_free(void* p) {
+  if (!p) return OTM_OK;
+  const cudaError_t e = cudaFreeHost(p);
+  return e == cudaSuccess ? OTM_OK : otm::cuda_fail(e, "cudaFreeHost");
+}
+
+}  // extern "C"

@@ -259,3 +259,21 @@ def test_mixed_precision_stationary_refinement():
     check_against_oracle(k, C, E, sens)
     st = H.stats()
     assert st.refinements == st.iterations > 0 and max(st.rel_res) <= 1e-6
+
+
+def test_pinned_host_arrays_and_copies():
+    """otm_host_alloc arrays and the library's host<->device copies round-trip exactly, on the
+    current stream, and report size mismatches."""
+    from opentm_b200 import copy_to_device, copy_to_host, pinned_empty
+    a = pinned_empty((16, 8, 4))
+    a[...] = np.random.default_rng(3).random(a.shape, dtype=np.float32)
+    t = torch.empty(a.shape, dtype=torch.float32, device="cuda")
+    copy_to_device(t, a)
+    t.mul_(2.0)
+    b = pinned_empty(a.shape)
+    copy_to_host(b, t)
+    torch.cuda.current_stream().synchronize()
+    assert np.array_equal(b, 2.0 * a)
+    assert torch.from_numpy(a).is_pinned()
+    with pytest.raises(ValueError):
+        copy_to_device(t, pinned_empty((3,)))
