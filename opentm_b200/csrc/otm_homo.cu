@@ -167,9 +167,14 @@ otm_status Homo::build(const otm_config& c, cudaStream_t ext_stream, cudaMemPool
     OTM_CUDA(cudaEventCreateWithFlags(&ev_in, cudaEventDisableTiming));
     OTM_CUDA(cudaEventCreateWithFlags(&ev_out, cudaEventDisableTiming));
   }
-  OTM_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
-  OTM_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
-  OTM_CUDA(cudaEventCreateWithFlags(&ev_coarse, cudaEventDisableTiming));
+  // a handle of its own gets the side stream; the server's handles (external mode) already run
+  // many requests side by side on their lanes, and a second stream per lane would exceed the
+  // device's hardware queues and serialise unrelated lanes
+  if (!external) {
+    OTM_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+    OTM_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    OTM_CUDA(cudaEventCreateWithFlags(&ev_coarse, cudaEventDisableTiming));
+  }
   if (cfg.profile)
     for (int a = 0; a < 2; a++)
       for (int j = 0; j < kMaxChunk; j++) OTM_CUDA(cudaEventCreate(&prof_ev[a][j]));
@@ -345,23 +350,26 @@ otm_status Homo::update(const float* kin, int pitchT) {
     OTM_CHECK_LAUNCH("k_to16");
     launched(2);
   }
-  // the coarse chain on the side stream, after the import (and the 16-bit copies)
-  OTM_CUDA(cudaEventRecord(ev_fork, stream));
-  OTM_CUDA(cudaStreamWaitEvent(side, ev_fork, 0));
+  // the coarse chain on the side stream (if any), after the import (and the 16-bit copies)
+  cudaStream_t cs = side ? side : stream;
+  if (side) {
+    OTM_CUDA(cudaEventRecord(ev_fork, stream));
+    OTM_CUDA(cudaStreamWaitEvent(side, ev_fork, 0));
+  }
   for (int l = 1; l < L; l++) {
     const bool cb = (l < L - 1);  // smoothed levels use the colour-blocked stencil order
     const size_t nvc = lv[l].d.nv();
     if (l == 1)
-      k_galerkin_fine<<<ceil_div(nvc, kBlock), kBlock, 0, side>>>(lv[0].d, lv[1].d, ks, table, lv[1].st, cb,
-                                                                  mixed ? kmax_bits : nullptr, op.c0);
+      k_galerkin_fine<<<ceil_div(nvc, kBlock), kBlock, 0, cs>>>(lv[0].d, lv[1].d, ks, table, lv[1].st, cb,
+                                                                mixed ? kmax_bits : nullptr, op.c0);
     else
-      k_galerkin_coarse<<<ceil_div(nvc, kBlock), kBlock, 0, side>>>(lv[l - 1].d, lv[l].d, lv[l - 1].st, lv[l].st,
-                                                                    cb);
+      k_galerkin_coarse<<<ceil_div(nvc, kBlock), kBlock, 0, cs>>>(lv[l - 1].d, lv[l].d, lv[l - 1].st, lv[l].st,
+                                                                  cb);
     OTM_CHECK_LAUNCH("galerkin");
     launched(1);
   }
   if (L == 1) {
-    k_fine_stencil<<<ceil_div(nv, kBlock), kBlock, 0, side>>>(d0, ks, op, lv[0].st);
+    k_fine_stencil<<<ceil_div(nv, kBlock), kBlock, 0, cs>>>(d0, ks, op, lv[0].st);
     OTM_CHECK_LAUNCH("k_fine_stencil");
     launched(1);
   }
@@ -370,13 +378,15 @@ otm_status Homo::update(const float* kin, int pitchT) {
     const int use_smem = abytes <= size_t(kMaxDynSmem);
     if (use_smem)
       OTM_CUDA(cudaFuncSetAttribute(k_coarsest_build, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem));
-    k_coarsest_build<<<1, 1024, use_smem ? abytes : 0, side>>>(lv.back().d, lv.back().st, Ainv, flags + 1,
-                                                                use_smem);
+    k_coarsest_build<<<1, 1024, use_smem ? abytes : 0, cs>>>(lv.back().d, lv.back().st, Ainv, flags + 1,
+                                                              use_smem);
   }
   OTM_CHECK_LAUNCH("k_coarsest_build");
   launched(1);
-  OTM_CUDA(cudaEventRecord(ev_coarse, side));
-  coarse_pending = true;
+  if (side) {
+    OTM_CUDA(cudaEventRecord(ev_coarse, side));
+    coarse_pending = true;
+  }
   updated = true;
   solved = false;
   return leave();
