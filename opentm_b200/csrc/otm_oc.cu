@@ -315,8 +315,14 @@ otm_status otm_oc_update(int ne, const float* sens, float* rho, float volratio, 
   double* partials = (double*)(scratch + sizeof(OcState));
   cudaMemsetAsync(st, 0, sizeof(OcState), s);
   k_oc_maxabs<<<nb, kBlock, 0, s>>>(ne, sens, partials, st);
+  // the tree passes run four blocks per SM: a thread then sums a few dozen elements before its
+  // 31 candidate sums are reduced, instead of the reduction costing as much as its elements
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    sms = 148;
+  const int nbt = std::min(nb, 4 * sms);
   for (int i = 0; i < (kOcSteps + kTreeDepth - 1) / kTreeDepth; i++)
-    k_oc_tree_pass<<<nb, kBlock, 0, s>>>(ne, sens, rho, volratio, min_rho, step_limit, damp, partials, st);
+    k_oc_tree_pass<<<nbt, kBlock, 0, s>>>(ne, sens, rho, volratio, min_rho, step_limit, damp, partials, st);
   k_oc_apply<<<ceil_div(size_t(ne), kBlock), kBlock, 0, s>>>(ne, sens, rho, min_rho, step_limit, damp, st);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess && iters_out) {
