@@ -107,48 +107,72 @@ __global__ void __launch_bounds__(256) k_conv_tiled(Dims d, const float* __restr
   float* val = sm;
   float* msk = sm + SX * SY * SZ;  // only used without periodicity
   const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY, z0 = blockIdx.z * kTZ;
-  const int tid = threadIdx.y * kTX + threadIdx.x;
-  for (int i = tid; i < SX * SY * SZ; i += 256) {
-    const int lx = i % SX, ly = (i / SX) % SY, lz = i / (SX * SY);
-    int gx = x0 + lx - H, gy = y0 + ly - H, gz = z0 + lz - H;
-    const bool in = gx >= 0 && gx < d.nx && gy >= 0 && gy < d.ny && gz >= 0 && gz < d.nz;
-    float v = 0.f, m = 0.f;
-    if (in || periodic) {
-      if (gx < 0 || gx >= d.nx) gx = ((gx % d.nx) + d.nx) % d.nx;
-      if (gy < 0 || gy >= d.ny) gy = ((gy % d.ny) + d.ny) % d.ny;
-      if (gz < 0 || gz >= d.nz) gz = ((gz % d.nz) + d.nz) % d.nz;
-      const size_t row = size_t(gy) + size_t(d.ny) * gz;
-      v = __ldg(src + row * src_pitch + gx);
-      if (!kFwd) {
-        const size_t q = row * d.nx + gx;
-        if (MODE == 3) v *= __ldg(dk_in + q);
-        v /= __ldg(ws_in + q);
+  // stage the tile row by row: x from the thread's lane (two passes cover SX = 32 + 2H), the
+  // (y, z) row from one small division, the wrapped x coordinates computed once
+  int gxs[2];
+  bool inx[2];
+#pragma unroll
+  for (int k = 0; k < 2; k++) {
+    int gx = x0 + int(threadIdx.x) + k * kTX - H;
+    inx[k] = gx >= 0 && gx < d.nx;
+    if (!inx[k]) gx = ((gx % d.nx) + d.nx) % d.nx;
+    gxs[k] = gx;
+  }
+  for (int rowi = threadIdx.y; rowi < SY * SZ; rowi += kTY) {
+    const int ly = rowi % SY, lz = rowi / SY;
+    int gy = y0 + ly - H, gz = z0 + lz - H;
+    const bool inyz = gy >= 0 && gy < d.ny && gz >= 0 && gz < d.nz;
+    if (gy < 0 || gy >= d.ny) gy = ((gy % d.ny) + d.ny) % d.ny;
+    if (gz < 0 || gz >= d.nz) gz = ((gz % d.nz) + d.nz) % d.nz;
+    const size_t row = size_t(gy) + size_t(d.ny) * gz;
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+      const int lx = int(threadIdx.x) + k * kTX;
+      if (lx >= SX) continue;
+      const int gx = gxs[k];
+      float v = 0.f, m = 0.f;
+      if ((inx[k] && inyz) || periodic) {
+        v = __ldg(src + row * src_pitch + gx);
+        if (!kFwd) {
+          const size_t q = row * d.nx + gx;
+          if (MODE == 3) v *= __ldg(dk_in + q);
+          v /= __ldg(ws_in + q);
+        }
+        m = 1.f;
       }
-      m = 1.f;
+      val[rowi * SX + lx] = v;
+      if (!periodic) msk[rowi * SX + lx] = m;
     }
-    val[i] = v;
-    if (!periodic) msk[i] = m;
   }
   __syncthreads();
   const int gx = x0 + threadIdx.x, gy = y0 + threadIdx.y;
   if (gx >= d.nx || gy >= d.ny) return;
-#pragma unroll 1
+  // the four z outputs of this thread together: each tap's weight and offset serve all four;
+  // every output still sums its taps in the reference's order
+  float sum[kTZ], wsv[kTZ];
+#pragma unroll
+  for (int tz = 0; tz < kTZ; tz++) sum[tz] = wsv[tz] = 0.f;
+  const int base = H * SX * SY + (threadIdx.y + H) * SX + (threadIdx.x + H);
+#pragma unroll 2
+  for (int t = 0; t < tl.n; t++) {
+    const float w = tl.w[t];
+    const int li = base + (kFwd ? tl.doff[t] : -tl.doff[t]);
+#pragma unroll
+    for (int tz = 0; tz < kTZ; tz++) {
+      sum[tz] += w * val[li + tz * SX * SY];
+      if (kFwd && !periodic) wsv[tz] += w * msk[li + tz * SX * SY];
+    }
+  }
+#pragma unroll
   for (int tz = 0; tz < kTZ; tz++) {
     const int gz = z0 + tz;
     if (gz >= d.nz) break;
-    float sum = 0.f, ws = 0.f;
-    const int base = (tz + H) * SX * SY + (threadIdx.y + H) * SX + (threadIdx.x + H);
-#pragma unroll 4
-    for (int t = 0; t < tl.n; t++) {
-      const float w = tl.w[t];
-      const int li = base + (kFwd ? tl.doff[t] : -tl.doff[t]);
-      sum += w * val[li];
-      if (kFwd && !periodic) ws += w * msk[li];
-    }
+    const float sumv = sum[tz];
+    float ws = wsv[tz];
     const size_t row = size_t(gy) + size_t(d.ny) * gz;
     if (kFwd) {
       if (periodic) ws = wsum_all;
-      const float out = sum / ws;
+      const float out = sumv / ws;
       if (dst) dst[row * dst_pitch + gx] = out;
       if (ws_out) ws_out[row * d.nx + gx] = ws;
       if (MODE == 1) {
@@ -158,7 +182,7 @@ __global__ void __launch_bounds__(256) k_conv_tiled(Dims d, const float* __restr
         dkout[row * d.nx + gx] = (k0 - kmin) * dpw;
       }
     } else {
-      dst[row * dst_pitch + gx] = sum;
+      dst[row * dst_pitch + gx] = sumv;
     }
   }
 }
