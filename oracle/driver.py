@@ -1,7 +1,8 @@
 """Restatement of OpenTM's design driver -- TEST INFRASTRUCTURE ONLY.
 
-Only ``tests/`` may import this module, as the checker of ``opentm_b200.driver``; the product
-never imports it. It restates, with numpy and the FP64 oracle in this package:
+Only ``tests/`` (as the checker of ``opentm_b200.driver``) and ``bench.py``'s CPU-baseline leg of
+the design workload (as the timed CPU baseline) may import this module; the product never
+imports it. It restates, with numpy and the FP64 oracle in this package:
 
 * initDensity (Framework.cu:63-145): the TPMS fields P, G, D, IWP, the sphere example, the
   thresholded noise, and randTri (homogenization/Framework.cuh:237-310) with the
