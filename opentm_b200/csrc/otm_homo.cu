@@ -541,6 +541,18 @@ void Homo::vcycle(int l) {
     for (int c = passes - 1; c >= 0; c--) gs(l, c);
 }
 
+// rho = r . z, then p = (z - zbar) + beta p, q = A p and alpha (z in its storage type VT).
+template <typename VT>
+void Homo::pcg_direction(const VT* z, const float* r, bool face, int nb) {
+  const Dims d0 = lv[0].d;
+  const size_t nv = d0.nv();
+  launch_pdl(k_dot_rz<VT>, dim3(nb), dim3(kBlock), 0, stream, nv, r, z, partials, sc);
+  if (face)
+    launch_pdl(k_update_p_apply_dot<true, VT>, dim3(nb), dim3(kBlock), 0, stream, d0, ks, op, z, p, q, partials, sc);
+  else
+    launch_pdl(k_update_p_apply_dot<false, VT>, dim3(nb), dim3(kBlock), 0, stream, d0, ks, op, z, p, q, partials, sc);
+}
+
 void Homo::iteration(int j) {
   prof_slot = j;
   const Dims d0 = lv[0].d;
@@ -553,17 +565,11 @@ void Homo::iteration(int j) {
     // residual replacements (k_update_x64r requests them, k_resid64 mode 2 performs them)
     const unsigned int* kmax_bits = (const unsigned int*)(flags + 2);
     vcycle(0);
-    float* zf = x;  // the FP32 solution buffer holds z during a mixed solve
+    // z = xscale_c * u16 is read in place by the two kernels that use it
     if (cfg.precision == OTM_PRECISION_MIXED_BF16)
-      launch_pdl(k_z16<__nv_bfloat16>, dim3(ceil_div(nv, kBlock)), dim3(kBlock), 0, stream, nv,
-                 (const __nv_bfloat16*)u16, zf, sc);
+      pcg_direction((const __nv_bfloat16*)u16, r, face, nb);
     else
-      launch_pdl(k_z16<__half>, dim3(ceil_div(nv, kBlock)), dim3(kBlock), 0, stream, nv, (const __half*)u16, zf, sc);
-    launch_pdl(k_dot_rz, dim3(nb), dim3(kBlock), 0, stream, nv, r, zf, partials, sc);
-    if (face)
-      launch_pdl(k_update_p_apply_dot<true>, dim3(nb), dim3(kBlock), 0, stream, d0, ks, op, zf, p, q, partials, sc);
-    else
-      launch_pdl(k_update_p_apply_dot<false>, dim3(nb), dim3(kBlock), 0, stream, d0, ks, op, zf, p, q, partials, sc);
+      pcg_direction((const __half*)u16, r, face, nb);
     launch_pdl(k_update_x64r, dim3(nb), dim3(kBlock), 0, stream, nv, x64, r, p, q, partials, sc, kmax_bits, op.c0,
                cfg.max_iter);
     if (face)
@@ -572,7 +578,7 @@ void Homo::iteration(int j) {
     else
       launch_pdl(k_resid64<false>, dim3(nb), dim3(kBlock), 0, stream, d0, ks, op, x64, b, r, partials, sc, kmax_bits,
                  cfg.max_iter, 2);
-    launched(5);
+    launched(4);
   } else if (mixed) {
     // FP64 refinement step: residual, one 16-bit V-cycle on the scaled residual, update
     const unsigned int* kmax_bits = (const unsigned int*)(flags + 2);
@@ -588,11 +594,7 @@ void Homo::iteration(int j) {
     launched(2);
   } else if (cfg.solver == OTM_SOLVER_PCG) {
     vcycle(0);
-    launch_pdl(k_dot_rz, dim3(nb), dim3(kBlock), 0, stream, nv, r, z, partials, sc);
-    if (face)
-      launch_pdl(k_update_p_apply_dot<true>, dim3(nb), dim3(kBlock), 0, stream, d0, ks, op, z, p, q, partials, sc);
-    else
-      launch_pdl(k_update_p_apply_dot<false>, dim3(nb), dim3(kBlock), 0, stream, d0, ks, op, z, p, q, partials, sc);
+    pcg_direction((const float*)z, r, face, nb);
     launch_pdl(k_update_xr, dim3(nb), dim3(kBlock), 0, stream, nv, x, r, p, q, partials, sc, cfg.max_iter);
     launched(3);
   } else {

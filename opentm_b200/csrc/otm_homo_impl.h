@@ -110,6 +110,8 @@ struct Homo {
   template <typename T>
   void fine_ops16(int what, int color);
   void vcycle(int l);
+  template <typename VT>
+  void pcg_direction(const VT* z, const float* r, bool face, int nb);
   void iteration(int j);
   void launched(uint64_t n) {
     if (!capturing) count_launches(n);

@@ -2,6 +2,8 @@
 // updates with deterministic FP64 reductions, K^H and sensitivity kernels.
 #pragma once
 
+#include <type_traits>
+
 #include "otm_mg_kernels.cuh"
 
 namespace otm {
@@ -194,14 +196,23 @@ __global__ void __launch_bounds__(kBlock) k_init_residual(Dims d, const float* _
 }
 
 // rho = r . z, zbar = mean z, rbar-correction; beta = rho / rho_old (0 on the first step).
-__device__ __forceinline__ void dot_rz_body(size_t nv, const float* __restrict__ r, const float* __restrict__ z,
+// A 16-bit z (the mixed-precision V-cycle's result on the scaled residual) is read as
+// xscale_c * u, in solution units.
+template <typename VT = float>
+__device__ __forceinline__ void dot_rz_body(size_t nv, const float* __restrict__ r, const VT* __restrict__ z,
                                             double* partials, SolveScalars* sc, unsigned int blk, unsigned int nblk) {
+  constexpr bool kScaled = !std::is_same<VT, float>::value;
   __shared__ double smem[32 * 9];
+  double zs[3] = {1.0, 1.0, 1.0};
+  if (kScaled)
+#pragma unroll
+    for (int c = 0; c < 3; c++) zs[c] = sc->xscale[c];
   double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   for (size_t i = size_t(blk) * blockDim.x + threadIdx.x; i < nv; i += size_t(nblk) * blockDim.x) {
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-      const double rc = r[c * nv + i], zc = z[c * nv + i];
+      const double rc = r[c * nv + i];
+      const double zc = kScaled ? zs[c] * double(ld(z + c * nv + i)) : double(ld(z + c * nv + i));
       v[c] += rc * zc;
       v[3 + c] += zc;
       v[6 + c] += rc;
@@ -229,11 +240,12 @@ __device__ __forceinline__ void dot_rz_body(size_t nv, const float* __restrict__
   }
 }
 
-static __global__ void __launch_bounds__(kBlock) k_dot_rz(size_t nv, const float* __restrict__ r,
-                                                   const float* __restrict__ z, double* partials, SolveScalars* sc) {
+template <typename VT>
+__global__ void __launch_bounds__(kBlock) k_dot_rz(size_t nv, const float* __restrict__ r, const VT* __restrict__ z,
+                                                   double* partials, SolveScalars* sc) {
   pdl_wait();
   if (solve_done(sc)) return;
-  dot_rz_body(nv, r, z, partials, sc, blockIdx.x, gridDim.x);
+  dot_rz_body<VT>(nv, r, z, partials, sc, blockIdx.x, gridDim.x);
 }
 
 // p = (z - zbar) + beta p
@@ -306,20 +318,23 @@ __global__ void __launch_bounds__(kBlock) k_apply_dot(Dims d, const float* __res
 //   p = (z - zbar) + beta p,  q = A p = A z + beta q,  alpha = rho / (p . q).
 // A annihilates constants (periodic Laplacian), so A p follows from A z and the previous q
 // without a second gather. beta == 0 (first iteration) ignores the old p and q entirely.
-template <bool kFace>
+// A 16-bit z is xscale_c * u: the gather runs on u and A z = xscale_c * (A u).
+template <bool kFace, typename VT>
 __global__ void __launch_bounds__(kBlock) k_update_p_apply_dot(Dims d, const float* __restrict__ ks, FineOp op,
-                                                               const float* __restrict__ z, float* __restrict__ p,
+                                                               const VT* __restrict__ z, float* __restrict__ p,
                                                                float* __restrict__ q, double* partials,
                                                                SolveScalars* sc) {
+  constexpr bool kScaled = !std::is_same<VT, float>::value;
   pdl_wait();
   if (solve_done(sc)) return;
   __shared__ double smem[32 * 3];
   const size_t nv = d.nv();
-  float be[3], zb[3];
+  float be[3], zb[3], zs[3];
 #pragma unroll
   for (int c = 0; c < 3; c++) {
     be[c] = float(sc->beta[c]);
     zb[c] = float(sc->zmean[c]);
+    zs[c] = kScaled ? float(sc->xscale[c]) : 1.f;
   }
   double v[3] = {0, 0, 0};
   for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nv; i += size_t(gridDim.x) * blockDim.x) {
@@ -339,8 +354,12 @@ __global__ void __launch_bounds__(kBlock) k_update_p_apply_dot(Dims d, const flo
     }
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-      const float zc = __ldg(z + c * nv + i);
-      const float az = diag * zc - acc[c];
+      float zc = ld(z + c * nv + i);
+      float az = diag * zc - acc[c];
+      if (kScaled) {
+        zc *= zs[c];
+        az *= zs[c];
+      }
       float pc = zc - zb[c], qc = az;
       if (be[c] != 0.f) {
         pc += be[c] * po[c];
@@ -642,19 +661,6 @@ __global__ void __launch_bounds__(kBlock) k_resid64(Dims d, const float* __restr
       sc->counter[T_RES] = 0;
     }
   }
-}
-
-// z = xscale_c * u: the 16-bit V-cycle's result on the scaled residual, back in solution units
-// (the preconditioned residual of the mixed PCG).
-template <typename VT>
-__global__ void __launch_bounds__(kBlock) k_z16(size_t nv, const VT* __restrict__ u, float* __restrict__ z,
-                                                const SolveScalars* sc) {
-  pdl_wait();
-  if (solve_done(sc)) return;
-  const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i >= nv) return;
-#pragma unroll
-  for (int c = 0; c < 3; c++) z[c * nv + i] = float(sc->xscale[c] * double(ld(u + c * nv + i)));
 }
 
 // Mixed PCG step: x64 += alpha p (FP64), r -= alpha q, ||r||^2 and max|r| -> relative residual,
