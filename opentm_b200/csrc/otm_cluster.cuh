@@ -78,14 +78,14 @@ __device__ __forceinline__ const float* cl_uplane(const ClLevel& L, const int* t
   return rb[e >> 16] + L.u_off + ((e & 0xffff) + 1) * L.ups;
 }
 
-// Writes value v of case c at (plane z, in-plane u index p) into every ghost copy of plane z.
-__device__ __forceinline__ void cl_push(const ClLevel& L, const int* tab, float* const* rb, int z, int p, int c,
-                                        float v) {
-#pragma unroll
-  for (int k = 0; k < 2; k++) {
-    const int e = tab[L.tab_off + L.d.nz + 2 * z + k];
-    if (e >= 0) rb[e >> 16][L.u_off + c * L.ucs + (e & 0xffff) * L.ups + p] = v;
-  }
+// The ghost copies of plane z of u held by the neighbouring CTAs, at in-plane u index p of case
+// 0 (null where plane z feeds fewer than two ghost copies). Taken before the stores of a vertex.
+__device__ __forceinline__ void cl_ghosts(const ClLevel& L, const int* tab, float* const* rb, int z, int p,
+                                          float*& g0, float*& g1) {
+  const int* pt = tab + L.tab_off + L.d.nz + 2 * z;
+  const int e0 = pt[0], e1 = pt[1];
+  g0 = e0 >= 0 ? rb[e0 >> 16] + L.u_off + (e0 & 0xffff) * L.ups + p : nullptr;
+  g1 = e1 >= 0 ? rb[e1 >> 16] + L.u_off + (e1 & 0xffff) * L.ups + p : nullptr;
 }
 
 // 27-point products of one vertex shared by a team of kTw lanes of one warp: lane k of the
@@ -118,10 +118,11 @@ __device__ __forceinline__ void cl_apply_team(const float* sp, size_t sstride, c
     for (int c = 0; c < 3; c++) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], off);
 }
 
-// One Gauss-Seidel colour pass over this CTA's vertices of the colour (gs_coarse_body, the
-// off-diagonal sum formed by a lane team); updated edge-plane values are pushed to the ghosts.
-// Vertices are enumerated over power-of-two index ranges (shifts and masks instead of
-// divisions); indices past nx/2 or ny/2 are idle.
+// One Gauss-Seidel colour pass over this CTA's vertices of the colour (gs_coarse_body); updated
+// edge-plane values are pushed to the ghosts. Vertices are enumerated over power-of-two index
+// ranges (shifts and masks instead of divisions); indices past nx/2 or ny/2 are idle. Only the
+// warps that hold a vertex run the body, and every load of a vertex (right-hand side, inverse
+// diagonal, ghost targets) is issued before its first store, so no store orders a reload.
 template <bool kSmemSt, int kTwl>
 __device__ __forceinline__ void cl_gs_t(const ClLevel& L, const float* __restrict__ f_glob, float* sm, const int* tab,
                                         float* const* rb, int rank, int color) {
@@ -134,9 +135,11 @@ __device__ __forceinline__ void cl_gs_t(const ClLevel& L, const float* __restric
   const int n = npl << (lhx + lhy);
   if (n == 0) return;  // uniform over the CTA
   const int cs = L.cs, ucs = L.ucs, urs = L.urs, ups = L.ups;
+  const int u_off = L.u_off, f_off = L.f_off, st_off = L.st_off, inv_off = L.inv_off;
+  const float* st_glob = L.st;
   const size_t nv = d.nv();
-  // every lane of a warp runs the same number of rounds (the team shuffles need all 32)
-  const int total = ((n << kTwl) + int(blockDim.x) - 1) / int(blockDim.x) * int(blockDim.x);
+  // whole warps only (the team shuffles need all 32 lanes of a warp)
+  const int total = ((n << kTwl) + 31) & ~31;
   for (int g = threadIdx.x; g < total; g += blockDim.x) {
     const int t0 = g >> kTwl, lane = g & ((1 << kTwl) - 1);
     const int i0 = t0 & ((1 << lhx) - 1), j0 = (t0 >> lhx) & ((1 << lhy) - 1), pk0 = t0 >> (lhx + lhy);
@@ -146,34 +149,43 @@ __device__ __forceinline__ void cl_gs_t(const ClLevel& L, const float* __restric
     const int xm = wrapm(x - 1, nx), xp = wrapm(x + 1, nx);
     const int ym = wrapm(y - 1, ny) * urs, y0 = y * urs, yp = wrapm(y + 1, ny) * urs;
     const int zl = z - z0;
-    const float* uz = sm + L.u_off + zl * ups;  // local planes zl, zl+1, zl+2 = z-1, z, z+1
+    const float* uz = sm + u_off + zl * ups;  // local planes zl, zl+1, zl+2 = z-1, z, z+1
     const float* const pu[3] = {uz, uz + ups, uz + 2 * ups};
     const int lidx = zl * plane + y * nx + x;  // own-vertex index (f, r, stencils)
-    const float* sp = kSmemSt ? sm + L.st_off + lidx * 27 : L.st + cb_index(d, x, y, z);
+    const float* sp = kSmemSt ? sm + st_off + lidx * 27 : st_glob + cb_index(d, x, y, z);
     const size_t sstride = kSmemSt ? size_t(1) : nv;
     float acc[3];
     cl_apply_team<kSmemSt, true, (1 << kTwl)>(sp, sstride, pu, xm, x, xp, ym, y0, yp, ucs, lane, acc);
     if (active && lane == 0) {
-      const float inv = kSmemSt ? sm[L.inv_off + lidx] : 1.0f / __ldg(sp + 13 * sstride);
+      const float inv = kSmemSt ? sm[inv_off + lidx] : 1.0f / __ldg(sp + 13 * sstride);
+      float fv[3];
+#pragma unroll
+      for (int c = 0; c < 3; c++)
+        fv[c] = f_off >= 0 ? sm[f_off + c * cs + lidx] : __ldg(f_glob + c * nv + size_t(z) * plane + y * nx + x);
       const int pu_idx = y0 + x;
+      float *g0, *g1;
+      cl_ghosts(L, tab, rb, z, pu_idx, g0, g1);
+      float* own = sm + u_off + (zl + 1) * ups + pu_idx;
 #pragma unroll
       for (int c = 0; c < 3; c++) {
-        const float f = L.f_off >= 0 ? sm[L.f_off + c * cs + lidx] : __ldg(f_glob + c * nv + size_t(z) * plane + y * nx + x);
-        const float v = (f - acc[c]) * inv;
-        sm[L.u_off + c * ucs + (zl + 1) * ups + pu_idx] = v;
-        cl_push(L, tab, rb, z, pu_idx, c, v);
+        const float v = (fv[c] - acc[c]) * inv;
+        own[c * ucs] = v;
+        if (g0) g0[c * ucs] = v;
+        if (g1) g1[c * ucs] = v;
       }
     }
   }
 }
 
-// The first level (global stencils) runs one lane per vertex; the others a team of 8.
+// One lane per vertex on every level: the 27 products with compile-time offsets cost fewer
+// instructions than a lane team's shared offsets and shuffles, and on the small levels the
+// pass is bound by instruction issue, not by the latency of one vertex.
 __device__ __forceinline__ void cl_gs(const ClLevel& L, const float* f_glob, float* sm, const int* tab,
                                       float* const* rb, int rank, int color) {
   if (L.st_off < 0)
     cl_gs_t<false, 0>(L, f_glob, sm, tab, rb, rank, color);
   else
-    cl_gs_t<true, 3>(L, f_glob, sm, tab, rb, rank, color);
+    cl_gs_t<true, 0>(L, f_glob, sm, tab, rb, rank, color);
 }
 
 // r = f - A u on this CTA's vertices (resid_coarse_body, the sum formed by a lane team).
@@ -187,8 +199,11 @@ __device__ __forceinline__ void cl_resid_t(const ClLevel& L, const float* __rest
   const int n = (z1 - z0) << (lnx + lny);
   if (n == 0) return;  // uniform over the CTA
   const int cs = L.cs, ucs = L.ucs, urs = L.urs, ups = L.ups;
+  const int u_off = L.u_off, f_off = L.f_off, r_off = L.r_off, st_off = L.st_off;
+  const float* st_glob = L.st;
+  float* rg = L.rg;
   const size_t nv = d.nv();
-  const int total = ((n << kTwl) + int(blockDim.x) - 1) / int(blockDim.x) * int(blockDim.x);
+  const int total = ((n << kTwl) + 31) & ~31;  // whole warps only
   for (int g = threadIdx.x; g < total; g += blockDim.x) {
     const int t0 = g >> kTwl, lane = g & ((1 << kTwl) - 1);
     const int x0 = t0 & ((1 << lnx) - 1), y0i = (t0 >> lnx) & ((1 << lny) - 1), zl0 = t0 >> (lnx + lny);
@@ -197,22 +212,24 @@ __device__ __forceinline__ void cl_resid_t(const ClLevel& L, const float* __rest
     const int z = z0 + zl;
     const int xm = wrapm(x - 1, nx), xp = wrapm(x + 1, nx);
     const int ym = wrapm(y - 1, ny) * urs, y0 = y * urs, yp = wrapm(y + 1, ny) * urs;
-    const float* uz = sm + L.u_off + zl * ups;
+    const float* uz = sm + u_off + zl * ups;
     const float* const pu[3] = {uz, uz + ups, uz + 2 * ups};
     const int lidx = zl * plane + y * nx + x;
-    const float* sp = kSmemSt ? sm + L.st_off + lidx * 27 : L.st + cb_index(d, x, y, z);
+    const float* sp = kSmemSt ? sm + st_off + lidx * 27 : st_glob + cb_index(d, x, y, z);
     const size_t sstride = kSmemSt ? size_t(1) : nv;
     float acc[3];
     cl_apply_team<kSmemSt, false, (1 << kTwl)>(sp, sstride, pu, xm, x, xp, ym, y0, yp, ucs, lane, acc);
     if (active && lane == 0) {
       const size_t gi = size_t(z) * plane + y * nx + x;
+      float fv[3];  // all loads before the first store
+#pragma unroll
+      for (int c = 0; c < 3; c++) fv[c] = f_off >= 0 ? sm[f_off + c * cs + lidx] : __ldg(f_glob + c * nv + gi);
 #pragma unroll
       for (int c = 0; c < 3; c++) {
-        const float f = L.f_off >= 0 ? sm[L.f_off + c * cs + lidx] : __ldg(f_glob + c * nv + gi);
-        if (L.r_off >= 0)
-          sm[L.r_off + c * cs + lidx] = f - acc[c];
+        if (r_off >= 0)
+          sm[r_off + c * cs + lidx] = fv[c] - acc[c];
         else
-          L.rg[c * nv + gi] = f - acc[c];
+          rg[c * nv + gi] = fv[c] - acc[c];
       }
     }
   }
@@ -343,18 +360,29 @@ __device__ __forceinline__ void cl_prolong(const ClLevel& F, const ClLevel& C, f
     const float* p1 = cl_uplane(C, tab, rb, Z1);
     const int r0 = Y0 * C.urs, r1 = Y1 * C.urs;
     const int pu_idx = y * F.urs + x;
+    // every load (coarse values, possibly in other CTAs, the old fine values and the ghost
+    // targets) before the first store
+    float a[3], uo[3];
+    float* uf = sm + F.u_off + (zl + 1) * F.ups + pu_idx;
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       const float* u0 = p0 + c * C.ucs;
       const float* u1 = p1 + c * C.ucs;
-      const float a = wz0 * (wy0 * (wx0 * u0[r0 + X0] + wx1 * u0[r0 + X1]) +
-                             wy1 * (wx0 * u0[r1 + X0] + wx1 * u0[r1 + X1])) +
-                      wz1 * (wy0 * (wx0 * u1[r0 + X0] + wx1 * u1[r0 + X1]) +
-                             wy1 * (wx0 * u1[r1 + X0] + wx1 * u1[r1 + X1]));
-      float* uf = sm + F.u_off + c * F.ucs + (zl + 1) * F.ups + pu_idx;
-      const float v = *uf + a;
-      *uf = v;
-      cl_push(F, tab, rb, z, pu_idx, c, v);
+      a[c] = wz0 * (wy0 * (wx0 * u0[r0 + X0] + wx1 * u0[r0 + X1]) +
+                    wy1 * (wx0 * u0[r1 + X0] + wx1 * u0[r1 + X1])) +
+             wz1 * (wy0 * (wx0 * u1[r0 + X0] + wx1 * u1[r0 + X1]) +
+                    wy1 * (wx0 * u1[r1 + X0] + wx1 * u1[r1 + X1]));
+      uo[c] = uf[c * F.ucs];
+    }
+    float *g0, *g1;
+    cl_ghosts(F, tab, rb, z, pu_idx, g0, g1);
+    const int fucs = F.ucs;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const float v = uo[c] + a[c];
+      uf[c * fucs] = v;
+      if (g0) g0[c * fucs] = v;
+      if (g1) g1[c * fucs] = v;
     }
   }
 }
