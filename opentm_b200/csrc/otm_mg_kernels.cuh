@@ -92,14 +92,17 @@ __device__ __forceinline__ bool last_block_n(unsigned int* counter, unsigned int
 }
 
 // Fixed-order sum of NV partial columns (partials[b * NV + i], b < nb) inside one block.
+// The partials of the other blocks are read from L2 (ld.global.cg: never a stale L1 line),
+// with the loop unrolled so that several rounds of loads are in flight at once.
 template <int NV>
 __device__ __forceinline__ void reduce_partials(const double* partials, int nb, double (&out)[NV], double* smem) {
   double v[NV];
 #pragma unroll
   for (int i = 0; i < NV; i++) v[i] = 0.0;
+#pragma unroll 4
   for (int b = threadIdx.x; b < nb; b += blockDim.x) {
 #pragma unroll
-    for (int i = 0; i < NV; i++) v[i] += ((volatile const double*)partials)[b * NV + i];
+    for (int i = 0; i < NV; i++) v[i] += __ldcg(partials + b * NV + i);
   }
   block_reduce_f64<NV>(v, smem);
 #pragma unroll

@@ -86,8 +86,9 @@ __device__ __forceinline__ void reduce_to_result(double (&s)[NS], double (&mx)[N
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int i = warp; i < W; i += int(blockDim.x >> 5)) {
       double acc = i < NS ? 0.0 : -1e300;
+#pragma unroll 8
       for (int b = lane; b < int(gridDim.x); b += 32) {
-        const double v = ((volatile double*)partials)[b * W + i];
+        const double v = __ldcg(partials + b * W + i);  // L2: never a stale L1 line
         acc = i < NS ? acc + v : fmax(acc, v);
       }
 #pragma unroll

@@ -57,7 +57,8 @@ __global__ void __launch_bounds__(kBlock) k_oc_maxabs(int ne, const float* __res
   }
   if (last_block(&st->counter)) {
     double b = 0.0;
-    for (int i = threadIdx.x; i < int(gridDim.x); i += blockDim.x) b = fmax(b, ((volatile double*)partials)[i]);
+#pragma unroll 4
+    for (int i = threadIdx.x; i < int(gridDim.x); i += blockDim.x) b = fmax(b, __ldcg(partials + i));
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) b = fmax(b, __shfl_down_sync(0xffffffffu, b, off));
     __syncthreads();
@@ -157,7 +158,9 @@ __global__ void __launch_bounds__(kBlock) k_oc_tree_pass(int ne, const float* __
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int t = warp; t < kTreeNodes; t += int(blockDim.x >> 5)) {
       double a = 0.0;
-      for (int b = lane; b < int(gridDim.x); b += 32) a += ((volatile double*)partials)[t * gridDim.x + b];
+      const double* col = partials + size_t(t) * gridDim.x;
+#pragma unroll 8
+      for (int b = lane; b < int(gridDim.x); b += 32) a += __ldcg(col + b);  // L2: never a stale L1 line
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
       if (lane == 0) tot[t] = a;

@@ -610,10 +610,11 @@ __global__ void __launch_bounds__(kBlock) k_resid64(Dims d, const float* __restr
   if (last_block(&sc->counter[T_RES])) {
     // parallel fixed-order finalisation: 6 sums and 3 maxima over the blocks' partials
     double t[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll 4
     for (int bq = threadIdx.x; bq < int(gridDim.x); bq += blockDim.x)
 #pragma unroll
       for (int i = 0; i < 9; i++) {
-        const double val = ((volatile double*)partials)[bq * 9 + i];
+        const double val = __ldcg(partials + bq * 9 + i);
         t[i] = i < 6 ? t[i] + val : fmax(t[i], val);
       }
     double ts[6];
@@ -713,10 +714,11 @@ static __global__ void __launch_bounds__(kBlock) k_update_x64r(size_t nv, double
   }
   if (last_block(&sc->counter[T_RR])) {
     double t[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll 4
     for (int bq = threadIdx.x; bq < int(gridDim.x); bq += blockDim.x)
 #pragma unroll
       for (int i = 0; i < 6; i++) {
-        const double val = ((volatile double*)partials)[bq * 6 + i];
+        const double val = __ldcg(partials + bq * 6 + i);
         t[i] = i < 3 ? t[i] + val : fmax(t[i], val);
       }
     double ts[3] = {t[0], t[1], t[2]};
