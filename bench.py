@@ -198,7 +198,7 @@ def run_ours(args, rank, world, local_rank):
     main = timed_loop("fp32", args.steps, args.warmup)
     clk = clocks.stop()
     e2e = timed_loop("fp32", args.steps, args.warmup, e2e=True)
-    # the same loop again with CUDA events around the first fine-level sweep of every iteration
+    # the same loop again with CUDA events around the first fine-level post-smoothing sweep of every iteration
     # (the event nodes need the chunked iteration graphs instead of the device-side loop)
     prof = timed_loop("fp32", args.steps, args.warmup, profile=True)
     mixed = None

@@ -70,7 +70,7 @@ typedef struct otm_config {
   int warm_start;        /* reuse the previous solutions as initial guesses; default 1 (homogenization.cu:184) */
   int check_every;       /* iterations between host convergence checks; default 4 */
   int use_graphs;        /* capture the iteration loop in a CUDA graph; default 1 */
-  int profile;           /* time the first fine-level smoothing sweep of every iteration with CUDA
+  int profile;           /* time the first fine-level post-smoothing sweep of every iteration with CUDA
                             events recorded inside the graph; default 0 */
   int cluster_cycle;     /* run the levels with <= 32^3 unknowns and the coarsest solve in one
                             thread-block-cluster launch when they fit; default 1 */

@@ -396,7 +396,8 @@ otm_status Homo::update(const float* kin, int pitchT) {
 // V-cycle and iteration (MG_H::v_cycle, homogenization/MG.cpp:46-71).
 // ---------------------------------------------------------------------------------------
 // Fine-level operations of the mixed form on 16-bit storage T: what = 0 colour pass,
-// 1 residual, 2 restriction to level 1, 3 prolongation from level 1.
+// 1 residual, 2 restriction to level 1, 3 prolongation from level 1, 4 zero fill and first
+// colour-pair pass.
 template <typename T>
 void Homo::fine_ops16(int what, int color) {
   Level& L = lv[0];
@@ -421,10 +422,33 @@ void Homo::fine_ops16(int what, int color) {
     case 2:
       k_restrict<3, T><<<ceil_div(lv[1].d.nv(), kBlock), kBlock, 0, stream>>>(L.d, lv[1].d, r, lv[1].f, sc);
       break;
+    case 4:  // zero fill + first colour-pair pass (paired colours only)
+      k_gs_fine_pair_first<3, T, T><<<ceil_div(nv >> 3, kBlock), kBlock, 0, stream>>>(L.d, kk, op0, u, L.f, sc, fs);
+      break;
     default:
       k_prolong<3, T><<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(L.d, lv[1].d, lv[1].u, u, sc);
       break;
   }
+  launched(1);
+}
+
+// The zero fill of level l's correction and the first colour pass of its first sweep.
+void Homo::gs_first(int l) {
+  Level& L = lv[l];
+  const size_t nsub = L.d.nv() >> 3;
+  if (l == 0 && mixed) {
+    if (cfg.precision == OTM_PRECISION_MIXED_BF16)
+      fine_ops16<__nv_bfloat16>(4, 0);
+    else
+      fine_ops16<__half>(4, 0);
+    return;
+  }
+  if (l == 0)
+    launch_pdl(k_gs_fine_pair_first<3, float, float>, dim3(ceil_div(nsub, kBlock)), dim3(kBlock), 0, stream, L.d,
+               (const float*)ks, op, L.u, (const float*)L.f, (const SolveScalars*)sc, (const double*)nullptr);
+  else
+    launch_pdl(k_gs_coarse_first<3>, dim3(ceil_div(nsub, kBlock)), dim3(kBlock), 0, stream, L.d, (const float*)L.st,
+               L.u, (const float*)L.f, (const SolveScalars*)sc);
   launched(1);
 }
 
@@ -490,20 +514,24 @@ void Homo::vcycle(int l) {
   }
   const bool m16 = (l == 0 && mixed);
   const bool bf = cfg.precision == OTM_PRECISION_MIXED_BF16;
-  if (m16)
-    cudaMemsetAsync(u16, 0, 3 * nv * 2, stream);
-  else
-    cudaMemsetAsync(L.u, 0, 3 * nv * sizeof(float), stream);
+  // the first pass of the first sweep starts from u = 0: one kernel writes the zero fill and the
+  // pass's values (not for the fine level with face entries, whose colours are not paired)
+  const bool first_fused = cfg.pre_smooth > 0 && !(l == 0 && face);
+  if (!first_fused) {
+    if (m16)
+      cudaMemsetAsync(u16, 0, 3 * nv * 2, stream);
+    else
+      cudaMemsetAsync(L.u, 0, 3 * nv * sizeof(float), stream);
+  }
   // the fine level of the cube element sweeps colour pairs (4 launches), coarse levels 8 colours
   const int passes = (l == 0 && !face) ? 4 : 8;
-  for (int s = 0; s < cfg.pre_smooth; s++) {
-    const bool timed = cfg.profile && l == 0 && s == 0 && prof_slot >= 0;
-    // inside a stream capture only an "external" event record becomes a graph node
-    const unsigned int evflag = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
-    if (timed) cudaEventRecordWithFlags(prof_ev[0][prof_slot], stream, evflag);
-    for (int c = 0; c < passes; c++) gs(l, c);
-    if (timed) cudaEventRecordWithFlags(prof_ev[1][prof_slot], stream, evflag);
-  }
+  for (int s = 0; s < cfg.pre_smooth; s++)
+    for (int c = 0; c < passes; c++) {
+      if (s == 0 && c == 0 && first_fused)
+        gs_first(l);
+      else
+        gs(l, c);
+    }
   Level& C = lv[l + 1];
   if (m16) {
     if (bf) {
@@ -537,8 +565,15 @@ void Homo::vcycle(int l) {
     launch_pdl(k_prolong<3>, dim3(ceil_div(nv, kBlock)), dim3(kBlock), 0, stream, L.d, C.d, C.u, L.u, sc);
     launched(1);
   }
-  for (int s = 0; s < cfg.post_smooth; s++)
+  for (int s = 0; s < cfg.post_smooth; s++) {
+    // the profiled sweep: the first post-smoothing sweep of the fine level (plain colour passes)
+    const bool timed = cfg.profile && l == 0 && s == 0 && prof_slot >= 0;
+    // inside a stream capture only an "external" event record becomes a graph node
+    const unsigned int evflag = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
+    if (timed) cudaEventRecordWithFlags(prof_ev[0][prof_slot], stream, evflag);
     for (int c = passes - 1; c >= 0; c--) gs(l, c);
+    if (timed) cudaEventRecordWithFlags(prof_ev[1][prof_slot], stream, evflag);
+  }
 }
 
 // rho = r . z, then p = (z - zbar) + beta p, q = A p and alpha (z in its storage type VT).

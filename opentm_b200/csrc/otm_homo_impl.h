@@ -87,7 +87,7 @@ struct Homo {
   int* flags_host = nullptr;  // pinned copy of flags[0..1]
   bool heat_ready = false;    // K^H of the last solve_impl(true) is already in sc_host->kh
   bool capturing = false;
-  // profiling: events around the first fine-level sweep of iteration j of a chunk
+  // profiling: events around the first fine-level post-smoothing sweep of iteration j of a chunk
   cudaEvent_t prof_ev[2][kMaxChunk] = {};
   int prof_slot = -1;
   int prof_sweeps = 0;
@@ -112,6 +112,7 @@ struct Homo {
   void vcycle(int l);
   template <typename VT>
   void pcg_direction(const VT* z, const float* r, bool face, int nb);
+  void gs_first(int l);
   void iteration(int j);
   void launched(uint64_t n) {
     if (!capturing) count_launches(n);

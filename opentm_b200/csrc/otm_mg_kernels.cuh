@@ -327,6 +327,58 @@ __global__ void __launch_bounds__(kBlock) k_gs_fine_pair(Dims d, int pair, const
   gs_fine_pair_body<NC, KT, VT>(d, pair, ks, op, u, f, fscale, size_t(blockIdx.x) * blockDim.x + threadIdx.x);
 }
 
+// The first colour-pair pass of a sweep that starts from u = 0: the neighbour products vanish,
+// so the pass writes u = f / a_vv at the vertices of colour pair 0 (the vertical pair
+// (2i, 2j, 2k), (2i, 2j, 2k+1)) and zero at the other six vertices of the 2x2x2 block, in place of
+// the zero fill and the pass. a_vv, its summation order and the scaling of f are those of
+// gs_fine_pair_body, so the values equal the pass's (which subtracts products with zero).
+template <int NC, typename KT, typename VT>
+__global__ void __launch_bounds__(kBlock) k_gs_fine_pair_first(Dims d, const KT* __restrict__ ks, FineOp op, VT* u,
+                                                                const float* __restrict__ f, const SolveScalars* sc,
+                                                                const double* fscale = nullptr) {
+  pdl_wait();
+  if (sc && solve_done(sc)) return;
+  const int hx = d.nx >> 1, hy = d.ny >> 1;
+  const size_t nsub = d.nv() >> 3;
+  const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= nsub) return;
+  const Coord3 c3_ = split3(t, hx, hy);
+  const int x = 2 * c3_.x, y = 2 * c3_.y, z = 2 * c3_.z;
+  const size_t nv = d.nv();
+  const int xs[2] = {wrapm(x - 1, d.nx), x};
+  const int ys[2] = {wrapm(y - 1, d.ny), y};
+  int zs[3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) zs[a] = wrapm(z - 1 + a, d.nz);  // element planes z-1 .. z+1
+  float kk[3][4];
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 4; b++) kk[a][b] = ld(ks + (size_t(ys[b >> 1]) + size_t(d.ny) * zs[a]) * d.nx + xs[b & 1]);
+  float fv[2][NC];
+#pragma unroll
+  for (int h = 0; h < 2; h++)
+#pragma unroll
+    for (int c = 0; c < NC; c++)
+      fv[h][c] = __ldg(f + c * nv + (size_t(y) + size_t(d.ny) * (z + h)) * d.nx + x) * (fscale ? float(fscale[c]) : 1.f);
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    float ksum8 = 0.f;
+#pragma unroll
+    for (int b = 0; b < 8; b++) ksum8 += kk[h + (b >> 2)][b & 3];
+    const float inv = 1.0f / (op.c0 * ksum8);
+    const size_t v = (size_t(y) + size_t(d.ny) * (z + h)) * d.nx + x;
+#pragma unroll
+    for (int c = 0; c < NC; c++) {
+      VT* uc = u + c * nv;
+      st(uc + v, fv[h][c] * inv);
+      st(uc + v + 1, 0.f);
+      st(uc + v + d.nx, 0.f);
+      st(uc + v + d.nx + 1, 0.f);
+    }
+  }
+}
+
 // r = f - A u on the fine level for every vertex.
 template <bool kFace, int NC, typename KT, typename VT>
 __device__ __forceinline__ void resid_fine_body(const Dims& d, const KT* __restrict__ ks, const FineOp& op,
@@ -403,6 +455,36 @@ __global__ void __launch_bounds__(kBlock) k_gs_coarse(Dims d, int color, const f
   pdl_wait();
   if (sc && solve_done(sc)) return;
   gs_coarse_body<NC>(d, color, st, u, f, size_t(blockIdx.x) * blockDim.x + threadIdx.x);
+}
+
+// The first colour pass of a coarse-level sweep that starts from u = 0: u = f / a_vv at colour 0,
+// zero at the other seven vertices of the 2x2x2 block, in place of the zero fill and the pass
+// (the same values as gs_coarse_body, which subtracts products with zero).
+template <int NC>
+__global__ void __launch_bounds__(kBlock) k_gs_coarse_first(Dims d, const float* __restrict__ st, float* u,
+                                                             const float* __restrict__ f, const SolveScalars* sc) {
+  pdl_wait();
+  if (sc && solve_done(sc)) return;
+  const int hx = d.nx >> 1, hy = d.ny >> 1;
+  const size_t nv = d.nv(), nsub = nv >> 3;
+  const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= nsub) return;
+  const Coord3 q = split3(t, hx, hy);
+  const int x = 2 * q.x, y = 2 * q.y, z = 2 * q.z;
+  const float inv = 1.0f / __ldg(st + size_t(13) * nv + t);  // colour 0: stencil index t
+#pragma unroll
+  for (int c = 0; c < NC; c++) {
+    float* uc = u + c * nv;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const size_t v = (size_t(y) + size_t(d.ny) * (z + h)) * d.nx + x;
+      const float a = h == 0 ? __ldg(f + c * nv + v) * inv : 0.f;
+      uc[v] = a;
+      uc[v + 1] = 0.f;
+      uc[v + d.nx] = 0.f;
+      uc[v + d.nx + 1] = 0.f;
+    }
+  }
 }
 
 template <int NC>
