@@ -78,6 +78,9 @@ struct Homo {
   bool external = false;
   cudaMemPool_t pool = nullptr;
   std::vector<void*> allocations;
+  // the first iteration of a device-loop solve runs outside the loop graph and waits for the
+  // side stream's coarse chain only before its first coarse level (set while it is launched)
+  bool join_in_cycle = false;
   size_t bytes_allocated = 0;
   std::vector<ChunkGraph> graphs;
   // the whole iteration loop as one graph (conditional while node), used without profiling

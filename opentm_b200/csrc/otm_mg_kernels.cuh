@@ -654,47 +654,96 @@ __device__ __forceinline__ int axis_targets(int t, int (&O)[2], float (&w)[2]) {
 }
 
 // Deeper levels: A_c(V, V+O) = sum_{d,o} P(2V+d, V) A_f(2V+d, o) P(2V+d+o, V+O).
-static __global__ void __launch_bounds__(kBlock) k_galerkin_coarse(Dims df, Dims dc, const float* __restrict__ stf,
-                                                             float* __restrict__ stc, int cb_out) {
-  const size_t nvc = dc.nv(), nvf = df.nv();
-  const size_t V = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (V >= nvc) return;
-  const Coord3 c3_ = split3(V, dc.nx, dc.ny);
-    const int X = c3_.x, Y = c3_.y, Z = c3_.z;
+// NSPLIT warps share 32 coarse vertices (one per lane): warp w forms the products of the fine
+// offsets d in [w * 27 / NSPLIT, (w + 1) * 27 / NSPLIT) with compile-time offsets, in the order
+// of d, and the partials of the warps are then summed in warp order through shared memory. With
+// NSPLIT = 1 a thread forms all 729 products of its vertex, a chain of loads that makes every
+// level's launch latency-bound; NSPLIT = 27 gives each warp a code path of its own.
+template <int NSPLIT>
+struct GalerkinShape {
+  static constexpr int kGroups = NSPLIT >= 8 ? 1 : 8 / NSPLIT;  // 32-vertex groups per block
+  static constexpr int kThreads = NSPLIT * 32 * kGroups;
+  static constexpr size_t kSmem = size_t(kGroups) * NSPLIT * 27 * 32 * sizeof(float);
+};
+
+template <int DD>
+__device__ __forceinline__ void galerkin_dd(const Dims& df, int X, int Y, int Z, const float* __restrict__ stf,
+                                            float (&acc)[27]) {
+  constexpr int dx = DD % 3 - 1, dy = (DD / 3) % 3 - 1, dz = DD / 9 - 1;
+  const float wv = (dx ? 0.5f : 1.f) * (dy ? 0.5f : 1.f) * (dz ? 0.5f : 1.f);
+  const size_t nvf = df.nv();
+  const int fx = wrapm(2 * X + dx, df.nx), fy = wrapm(2 * Y + dy, df.ny), fz = wrapm(2 * Z + dz, df.nz);
+  const size_t sb = cb_index(df, fx, fy, fz);
+  float sv[27];
+#pragma unroll
+  for (int o = 0; o < 27; o++) sv[o] = __ldg(stf + size_t(o) * nvf + sb);
+#pragma unroll
+  for (int o = 0; o < 27; o++) {
+    const float s = wv * sv[o];
+    const int ox = o % 3 - 1, oy = (o / 3) % 3 - 1, oz = o / 9 - 1;
+    int Ox[2], Oy[2], Oz[2];
+    float wx[2], wy[2], wz[2];
+    const int nx = axis_targets(dx + ox, Ox, wx);
+    const int ny = axis_targets(dy + oy, Oy, wy);
+    const int nz = axis_targets(dz + oz, Oz, wz);
+#pragma unroll
+    for (int iz = 0; iz < 2; iz++)
+#pragma unroll
+      for (int iy = 0; iy < 2; iy++)
+#pragma unroll
+        for (int ix = 0; ix < 2; ix++) {
+          if (ix < nx && iy < ny && iz < nz) {
+            const int O = (Ox[ix] + 1) + 3 * (Oy[iy] + 1) + 9 * (Oz[iz] + 1);
+            acc[O] += s * wx[ix] * wy[iy] * wz[iz];
+          }
+        }
+  }
+}
+
+template <int D0, int D1>
+__device__ __forceinline__ void galerkin_range(const Dims& df, int X, int Y, int Z, const float* __restrict__ stf,
+                                               float (&acc)[27]) {
+  galerkin_dd<D0>(df, X, Y, Z, stf, acc);
+  if constexpr (D0 + 1 < D1) galerkin_range<D0 + 1, D1>(df, X, Y, Z, stf, acc);
+}
+
+// warp-uniform dispatch of warp w's offset range
+template <int NSPLIT, int W>
+__device__ __forceinline__ void galerkin_warp(int w, const Dims& df, int X, int Y, int Z,
+                                              const float* __restrict__ stf, float (&acc)[27]) {
+  constexpr int G = 27 / NSPLIT;
+  if (w == W)
+    galerkin_range<W * G, (W + 1) * G>(df, X, Y, Z, stf, acc);
+  else if constexpr (W + 1 < NSPLIT)
+    galerkin_warp<NSPLIT, W + 1>(w, df, X, Y, Z, stf, acc);
+}
+
+template <int NSPLIT>
+__global__ void __launch_bounds__(GalerkinShape<NSPLIT>::kThreads)
+    k_galerkin_coarse(Dims df, Dims dc, const float* __restrict__ stf, float* __restrict__ stc, int cb_out) {
+  static_assert(27 % NSPLIT == 0, "the fine offsets split evenly");
+  extern __shared__ float gpart[];  // [group][w][O][lane]
+  const int warp = int(threadIdx.x >> 5), lane = int(threadIdx.x & 31);
+  const int group = warp / NSPLIT, w = warp - group * NSPLIT;
+  const size_t nvc = dc.nv();
+  const size_t V = (size_t(blockIdx.x) * GalerkinShape<NSPLIT>::kGroups + group) * 32 + lane;
+  const bool ok = V < nvc;
+  const Coord3 c3_ = split3(ok ? V : 0, dc.nx, dc.ny);
+  const int X = c3_.x, Y = c3_.y, Z = c3_.z;
   float acc[27];
 #pragma unroll
   for (int o = 0; o < 27; o++) acc[o] = 0.f;
+  galerkin_warp<NSPLIT, 0>(w, df, X, Y, Z, stf, acc);
+  float* gp = gpart + size_t(group) * NSPLIT * 27 * 32;
 #pragma unroll
-  for (int dd = 0; dd < 27; dd++) {
-    const int dx = dd % 3 - 1, dy = (dd / 3) % 3 - 1, dz = dd / 9 - 1;
-    const float wv = (dx ? 0.5f : 1.f) * (dy ? 0.5f : 1.f) * (dz ? 0.5f : 1.f);
-    const int fx = wrapm(2 * X + dx, df.nx), fy = wrapm(2 * Y + dy, df.ny), fz = wrapm(2 * Z + dz, df.nz);
-    const size_t sb = cb_index(df, fx, fy, fz);
+  for (int o = 0; o < 27; o++) gp[(w * 27 + o) * 32 + lane] = acc[o];
+  __syncthreads();
+  for (int O = w; O < 27; O += NSPLIT) {
+    float a = 0.f;
 #pragma unroll
-    for (int o = 0; o < 27; o++) {
-      const float s = wv * __ldg(stf + size_t(o) * nvf + sb);
-      const int ox = o % 3 - 1, oy = (o / 3) % 3 - 1, oz = o / 9 - 1;
-      int Ox[2], Oy[2], Oz[2];
-      float wx[2], wy[2], wz[2];
-      const int nx = axis_targets(dx + ox, Ox, wx);
-      const int ny = axis_targets(dy + oy, Oy, wy);
-      const int nz = axis_targets(dz + oz, Oz, wz);
-#pragma unroll
-      for (int iz = 0; iz < 2; iz++)
-#pragma unroll
-        for (int iy = 0; iy < 2; iy++)
-#pragma unroll
-          for (int ix = 0; ix < 2; ix++) {
-            if (ix < nx && iy < ny && iz < nz) {
-              const int O = (Ox[ix] + 1) + 3 * (Oy[iy] + 1) + 9 * (Oz[iz] + 1);
-              acc[O] += s * wx[ix] * wy[iy] * wz[iz];
-            }
-          }
-    }
+    for (int q = 0; q < NSPLIT; q++) a += gp[(q * 27 + O) * 32 + lane];
+    if (ok) stc[size_t(O) * nvc + (cb_out ? cb_index(dc, X, Y, Z) : V)] = a;
   }
-  const size_t out = cb_out ? cb_index(dc, X, Y, Z) : V;
-#pragma unroll
-  for (int o = 0; o < 27; o++) stc[size_t(o) * nvc + out] = acc[o];
 }
 
 }  // namespace otm
