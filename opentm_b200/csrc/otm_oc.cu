@@ -318,12 +318,13 @@ otm_status otm_oc_update(int ne, const float* sens, float* rho, float volratio, 
   double* partials = (double*)(scratch + sizeof(OcState));
   cudaMemsetAsync(st, 0, sizeof(OcState), s);
   k_oc_maxabs<<<nb, kBlock, 0, s>>>(ne, sens, partials, st);
-  // the tree passes run four blocks per SM: a thread then sums a few dozen elements before its
+  // the tree passes run two blocks per SM: a thread then sums a few dozen elements before its
   // 31 candidate sums are reduced, instead of the reduction costing as much as its elements
+  // (one pass at 128^3: 38.8 / 26.9 / 32.0 / 39.0 us with 1 / 2 / 4 / 8 blocks per SM)
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
     sms = 148;
-  const int nbt = std::min(nb, 4 * sms);
+  const int nbt = std::min(nb, 2 * sms);
   for (int i = 0; i < (kOcSteps + kTreeDepth - 1) / kTreeDepth; i++)
     k_oc_tree_pass<<<nbt, kBlock, 0, s>>>(ne, sens, rho, volratio, min_rho, step_limit, damp, partials, st);
   k_oc_apply<<<ceil_div(size_t(ne), kBlock), kBlock, 0, s>>>(ne, sens, rho, min_rho, step_limit, damp, st);
