@@ -436,7 +436,7 @@ void Homo::fine_ops16(int what, int color) {
       k_gs_fine_pair_first<3, T, T><<<ceil_div(nv >> 3, kBlock), kBlock, 0, stream>>>(L.d, kk, op0, u, L.f, sc, fs);
       break;
     default:
-      k_prolong<3, T><<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(L.d, lv[1].d, lv[1].u, u, sc);
+      k_prolong8<3, T><<<ceil_div(lv[1].d.nv(), kBlock), kBlock, 0, stream>>>(L.d, lv[1].d, lv[1].u, u, sc);
       break;
   }
   launched(1);
@@ -578,7 +578,8 @@ void Homo::vcycle(int l) {
     else
       fine_ops16<__half>(3, 0);
   } else {
-    launch_pdl(k_prolong<3>, dim3(ceil_div(nv, kBlock)), dim3(kBlock), 0, stream, L.d, C.d, C.u, L.u, sc);
+    launch_pdl(k_prolong8<3, float>, dim3(ceil_div(C.d.nv(), kBlock)), dim3(kBlock), 0, stream, L.d, C.d,
+               (const float*)C.u, L.u, (const SolveScalars*)sc);
     launched(1);
   }
   for (int s = 0; s < cfg.post_smooth; s++) {

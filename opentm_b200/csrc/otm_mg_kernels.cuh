@@ -590,6 +590,52 @@ __global__ void __launch_bounds__(kBlock) k_prolong(Dims df, Dims dc, const floa
   prolong_body<NC, VT>(df, dc, uc, uf, size_t(blockIdx.x) * blockDim.x + threadIdx.x);
 }
 
+// u_f += P u_c with one thread per coarse vertex: its 2x2x2 block of coarse values (per case)
+// is loaded once and interpolated to the 8 fine vertices (2X + dx, 2Y + dy, 2Z + dz), each with
+// the expression and weights of prolong_body (the same values; 24 coarse loads per 8 fine
+// vertices instead of per vertex). Needs even fine dimensions (every level with a coarser one).
+template <int NC, typename VT>
+__global__ void __launch_bounds__(kBlock) k_prolong8(Dims df, Dims dc, const float* __restrict__ uc, VT* uf,
+                                                      const SolveScalars* sc) {
+  pdl_wait();
+  if (sc && solve_done(sc)) return;
+  const size_t nvc = dc.nv(), nvf = df.nv();
+  const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= nvc) return;
+  const Coord3 q = split3(t, dc.nx, dc.ny);
+  const int Xs[2] = {q.x, wrapm(q.x + 1, dc.nx)};
+  const int Ys[2] = {q.y, wrapm(q.y + 1, dc.ny)};
+  const int Zs[2] = {q.z, wrapm(q.z + 1, dc.nz)};
+#pragma unroll
+  for (int c = 0; c < NC; c++) {
+    const float* u = uc + c * nvc;
+    float b[2][2][2];  // [z][y][x] offsets 0 / +1 from (X, Y, Z)
+#pragma unroll
+    for (int zi = 0; zi < 2; zi++)
+#pragma unroll
+      for (int yi = 0; yi < 2; yi++)
+#pragma unroll
+        for (int xi = 0; xi < 2; xi++)
+          b[zi][yi][xi] = __ldg(u + (size_t(Ys[yi]) + size_t(dc.ny) * Zs[zi]) * dc.nx + Xs[xi]);
+#pragma unroll
+    for (int dz = 0; dz < 2; dz++)
+#pragma unroll
+      for (int dy = 0; dy < 2; dy++)
+#pragma unroll
+        for (int dx = 0; dx < 2; dx++) {
+          const float wx1 = dx ? 0.5f : 0.f, wy1 = dy ? 0.5f : 0.f, wz1 = dz ? 0.5f : 0.f;
+          const float wx0 = 1.f - wx1, wy0 = 1.f - wy1, wz0 = 1.f - wz1;
+          const float a = wz0 * (wy0 * (wx0 * b[0][0][0] + wx1 * b[0][0][dx]) +
+                                 wy1 * (wx0 * b[0][dy][0] + wx1 * b[0][dy][dx])) +
+                          wz1 * (wy0 * (wx0 * b[dz][0][0] + wx1 * b[dz][0][dx]) +
+                                 wy1 * (wx0 * b[dz][dy][0] + wx1 * b[dz][dy][dx]));
+          const size_t v = (size_t(2 * q.x + dx) + size_t(df.nx) * (size_t(2 * q.y + dy) +
+                                                                     size_t(df.ny) * (2 * q.z + dz)));
+          st(uf + c * nvf + v, ld(uf + c * nvf + v) + a);
+        }
+  }
+}
+
 // ------------------------------------------------------------------------------------
 // Galerkin coarse operators (homogenization/grid_ex.cu:16-227, restrict_stencil_*).
 // ------------------------------------------------------------------------------------
