@@ -22,7 +22,8 @@
 
 namespace otm {
 
-constexpr int kCl = 8;             // CTAs per cluster (portable cluster size)
+constexpr int kCl = 16;            // CTAs per cluster (non-portable size, opted in at set-up): one
+                                   // 32^3 colour pass at 16 CTAs loads half the stencils per SM of 8
 constexpr int kClThreads = 512;
 constexpr int kClMaxLevels = 8;
 constexpr int kClMaxNv = 32768;    // unknowns of the first level handled by the cluster (32^3)

@@ -281,7 +281,8 @@ otm_status Homo::build(const otm_config& c, cudaStream_t ext_stream, cudaMemPool
       const size_t bytes = cl_plan(dims.data(), int(dims.size()), &cd);
       if (bytes > 0 &&
           cudaFuncSetAttribute(k_vcycle_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem) ==
-              cudaSuccess) {
+              cudaSuccess &&
+          cudaFuncSetAttribute(k_vcycle_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
         cudaLaunchConfig_t lc{};
         lc.gridDim = dim3(kCl);
         lc.blockDim = dim3(kClThreads);
