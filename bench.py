@@ -132,7 +132,7 @@ def run_ours(args, rank, world, local_rank):
 
     def make(precision, profile=False):
         H = Homogenization_H(HomoConfig(reso=n, femRelThres=TOL, pre_smooth=2, post_smooth=2, max_iter=200,
-                                        precision=precision, profile=profile))
+                                        precision=precision, profile=profile, smoother=args.smoother))
         df = DensityFilter((n, n, n), FILTER_R, 1, True, P_SIMP, K0, KMIN)
         oc = OCOptimizer(ne, 0.001, MOVE, DAMP)
         return H, df, oc
@@ -227,11 +227,14 @@ def run_ours(args, rank, world, local_rank):
         launch_ms = pr.sweep_ms / pr.sweeps / pr.launches_per_sweep
         bytes_launch = pr.sweep_bytes / pr.launches_per_sweep
         achieved = bytes_launch / (launch_ms * 1e-3) / 1e9
+        kname = ("k_tile_smooth<post> (prolongation + 2 tiled Gauss-Seidel sweeps, 3 load cases)" if pr.kernel_kind == 1
+                 else "k_gs_fine_pair (one colour-pair pass, 3 load cases)")
+        tkey = "k_tile_smooth_post" if pr.kernel_kind == 1 else "k_gs_fine_pair"
         traffic = None
         tp = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(tp):
-            traffic = json.load(open(tp)).get(f"k_gs_fine_pair_dram_bytes_per_launch_n{n}")
-        roofline = {"bound": "hbm", "kernel": "k_gs_fine_pair (one colour-pair pass, 3 load cases)",
+            traffic = json.load(open(tp)).get(f"{tkey}_dram_bytes_per_launch_n{n}")
+        roofline = {"bound": "hbm", "kernel": kname,
                     "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                     "frac": round(achieved / hbm, 4), "traffic": traffic,
                     "peak_kind": f"{peak_kind} hbm_gbs", "launch_us": round(launch_ms * 1e3, 3),
@@ -245,7 +248,7 @@ def run_ours(args, rank, world, local_rank):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"OC loop, {n}^3 periodic cell, 3 load cases, V(2,2)-PCG to rel.res {TOL}",
                    "reso": n, "tol": TOL, "l2": "flushed (256 MB write) before every timed step",
-                   "replicas": world, "precision": "fp32"},
+                   "replicas": world, "precision": "fp32", "smoother": args.smoother},
         "p50_ms": round(float(np.percentile(lat, 50)), 4), "p99_ms": round(float(np.percentile(lat, 99)), 4),
         "pcg_iterations_last_step": main["iters"],
         "e2e": {"value": round(args.steps * world / t_e2e, 3), "unit": UNIT, "h2d_bytes_per_step": 4 * ne,
@@ -494,7 +497,7 @@ def run_solve(args, n, k, label, field, headline):
     res = {}
     for prec in ("fp32", "bf16", "fp16"):
         H = Homogenization_H(HomoConfig(reso=n, femRelThres=TOL, pre_smooth=2, post_smooth=2, precision=prec,
-                                        warm_start=False, max_iter=200))
+                                        warm_start=False, max_iter=200, smoother=args.smoother))
         sens = torch.empty_like(kd)
         H.update(kd)
         H.heatMatrix()  # builds the solve graph
@@ -661,6 +664,8 @@ def main():
     ap.add_argument("--iters-per-step", type=int, default=2)
     ap.add_argument("--batched", action="store_true", help="serve: batched form instead of handles on streams")
     ap.add_argument("--streams", type=int, default=8, help="serve: requests running at once in the handle form")
+    ap.add_argument("--smoother", default="color", choices=["tiled", "color"],
+                    help="fine-level smoother: global colour-pair passes (default) or shared-memory tiles")
     args = ap.parse_args()
     if args.workload == "serve":
         run_serve(args)

@@ -114,6 +114,7 @@ class HomoConfig:
     use_graphs: bool = True
     profile: bool = False
     cluster_cycle: bool = True
+    smoother: str = "color"
 
     def to_c(self) -> _lib.Config:
         reso = self.reso if not isinstance(self.reso, int) else (self.reso,) * 3
@@ -123,7 +124,8 @@ class HomoConfig:
             precision=self.precision, coarsest_max_dof=int(self.coarsest_max_dof),
             power_penal=float(self.power_penal), warm_start=int(bool(self.warm_start)),
             check_every=int(self.check_every), use_graphs=int(bool(self.use_graphs)),
-            profile=int(bool(self.profile)), cluster_cycle=int(bool(self.cluster_cycle)))
+            profile=int(bool(self.profile)), cluster_cycle=int(bool(self.cluster_cycle)),
+            smoother=self.smoother)
 
 
 class Homogenization_H:

@@ -28,6 +28,7 @@ OTM_ERR_NOT_READY = 12
 
 PRECISION = {"fp32": 0, "bf16": 1, "fp16": 2}
 SOLVER = {"pcg": 0, "vcycle": 1}
+SMOOTHER = {"color": 0, "tiled": 1}
 
 
 class OtmError(RuntimeError):
@@ -52,6 +53,7 @@ class Config(ctypes.Structure):
         ("use_graphs", ctypes.c_int),
         ("profile", ctypes.c_int),
         ("cluster_cycle", ctypes.c_int),
+        ("smoother", ctypes.c_int),
     ]
 
 
@@ -64,12 +66,13 @@ class SolveStats(ctypes.Structure):
         ("levels", ctypes.c_int),
         ("coarsest_reso", ctypes.c_int * 3),
         ("cluster_level", ctypes.c_int),
+        ("smoother", ctypes.c_int),
     ]
 
 
 class Profile(ctypes.Structure):
     _fields_ = [("sweeps", ctypes.c_int), ("sweep_ms", ctypes.c_double), ("sweep_bytes", ctypes.c_double),
-                ("launches_per_sweep", ctypes.c_int)]
+                ("launches_per_sweep", ctypes.c_int), ("kernel_kind", ctypes.c_int)]
 
 
 class ServerConfig(ctypes.Structure):
@@ -258,6 +261,8 @@ def default_config(reso=(128, 128, 128), **kw) -> Config:
             v = PRECISION[v]
         if k == "solver" and isinstance(v, str):
             v = SOLVER[v]
+        if k == "smoother" and isinstance(v, str):
+            v = SMOOTHER[v]
         if not hasattr(cfg, k):
             raise TypeError(f"unknown config field {k}")
         setattr(cfg, k, v)

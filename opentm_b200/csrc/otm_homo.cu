@@ -20,6 +20,8 @@
 #include "otm_solver_kernels.cuh"
 #include "otm_template.h"
 
+#include <cudaTypedefs.h>
+
 namespace otm {
 
 static thread_local std::string g_last_error;
@@ -141,6 +143,7 @@ otm_status Homo::build(const otm_config& c, cudaStream_t ext_stream, cudaMemPool
   if (cfg.check_every > kMaxChunk) cfg.check_every = kMaxChunk;
   if (cfg.coarsest_max_dof < 8) cfg.coarsest_max_dof = 8;
   if (cfg.solver != OTM_SOLVER_PCG && cfg.solver != OTM_SOLVER_VCYCLE) return invalid("unknown solver");
+  if (cfg.smoother != OTM_SMOOTHER_COLOR && cfg.smoother != OTM_SMOOTHER_TILED) return invalid("unknown smoother");
   if (cfg.precision < OTM_PRECISION_FP32 || cfg.precision > OTM_PRECISION_MIXED_FP16)
     return invalid("unknown precision");
   if (cfg.precision != OTM_PRECISION_FP32 && !mixed_supported()) {
@@ -304,11 +307,63 @@ otm_status Homo::build(const otm_config& c, cudaStream_t ext_stream, cudaMemPool
       cudaGetLastError();  // a refused attribute or occupancy query leaves no error behind
     }
   }
+  // the tile-staged fine smoother: cube elements (no face couplings), every axis a multiple of the
+  // tile, a coarser level to correct from, at least one sweep in each leg, and the PCG solver. Block
+  // Jacobi across the tile faces leaves the mode that is constant inside each tile and alternates in
+  // sign from tile to tile almost undamped (a smoother factor near -1): preconditioned CG is not
+  // affected by that (the preconditioner stays symmetric positive definite), but stationary V-cycles
+  // would stall on it, so they keep the global colour passes.
+  if (cfg.smoother == OTM_SMOOTHER_TILED && cfg.solver == OTM_SOLVER_PCG && !face && lv.size() > 1 &&
+      tile_fits(lv[0].d) && cfg.pre_smooth > 0 && cfg.post_smooth > 0) {
+    OTM_TRY(tile_attributes());
+    tiled = true;
+  }
   stats.levels = int(lv.size());
   stats.cluster_level = cluster_l;
+  stats.smoother = tiled ? OTM_SMOOTHER_TILED : OTM_SMOOTHER_COLOR;
   stats.coarsest_reso[0] = lv.back().d.nx;
   stats.coarsest_reso[1] = lv.back().d.ny;
   stats.coarsest_reso[2] = lv.back().d.nz;
+  return OTM_OK;
+}
+
+// Dynamic shared memory of the tile kernels (a per-function attribute of the current device; set
+// at every build, which is cheap) and the TMA map of the fine right-hand side: a 4-D tensor
+// {nx, ny, nz, 3 cases} of FP32 whose {16, 16, 8, 3} boxes are the tiles' right-hand sides.
+otm_status Homo::tile_attributes() {
+  const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  OTM_CUDA(cudaFuncSetAttribute(k_tile_smooth<false, float, float>, a, int(kTileSmemPre)));
+  OTM_CUDA(cudaFuncSetAttribute(k_tile_smooth<true, float, float>, a, int(kTileSmemPost)));
+  OTM_CUDA(cudaFuncSetAttribute(k_tile_resid<float, float>, a, int(kTileSmemResid)));
+  OTM_CUDA(cudaFuncSetAttribute(k_tile_smooth<false, __nv_bfloat16, __nv_bfloat16>, a, int(kTileSmemPre)));
+  OTM_CUDA(cudaFuncSetAttribute(k_tile_smooth<true, __nv_bfloat16, __nv_bfloat16>, a, int(kTileSmemPost)));
+  OTM_CUDA(cudaFuncSetAttribute(k_tile_resid<__nv_bfloat16, __nv_bfloat16>, a, int(kTileSmemResid)));
+  OTM_CUDA(cudaFuncSetAttribute(k_tile_smooth<false, __half, __half>, a, int(kTileSmemPre)));
+  OTM_CUDA(cudaFuncSetAttribute(k_tile_smooth<true, __half, __half>, a, int(kTileSmemPost)));
+  OTM_CUDA(cudaFuncSetAttribute(k_tile_resid<__half, __half>, a, int(kTileSmemResid)));
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    OTM_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+    if (q != cudaDriverEntryPointSuccess || !fn) {
+      set_error("cuTensorMapEncodeTiled is not available from the driver");
+      return OTM_ERR_UNSUPPORTED;
+    }
+    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  const Dims d = lv[0].d;
+  const cuuint64_t dims[4] = {cuuint64_t(d.nx), cuuint64_t(d.ny), cuuint64_t(d.nz), 3};
+  const cuuint64_t strides[3] = {cuuint64_t(d.nx) * 4, cuuint64_t(d.nx) * d.ny * 4, cuuint64_t(d.nv()) * 4};
+  const cuuint32_t box[4] = {cuuint32_t(kTX), cuuint32_t(kTY), cuuint32_t(kTZ), 3};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  const CUresult r = encode(&fmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, lv[0].f, dims, strides, box, estr,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed for the fine right-hand side");
+    return OTM_ERR_CUDA;
+  }
   return OTM_OK;
 }
 
@@ -523,6 +578,17 @@ void Homo::vcycle(int l) {
     launched(1);
     return;
   }
+  if (l == 0 && tiled) {
+    const double* fs = mixed ? (const double*)sc->fscale : nullptr;
+    if (!mixed)
+      vcycle_fine_tiled<float, float>(ks, L.u, L.r, op, fs);
+    else if (cfg.precision == OTM_PRECISION_MIXED_BF16)
+      vcycle_fine_tiled<__nv_bfloat16, __nv_bfloat16>((const __nv_bfloat16*)k16, (__nv_bfloat16*)u16,
+                                                      (__nv_bfloat16*)r16, op0, fs);
+    else
+      vcycle_fine_tiled<__half, __half>((const __half*)k16, (__half*)u16, (__half*)r16, op0, fs);
+    return;
+  }
   const bool m16 = (l == 0 && mixed);
   const bool bf = cfg.precision == OTM_PRECISION_MIXED_BF16;
   // the first pass of the first sweep starts from u = 0: one kernel writes the zero fill and the
@@ -594,6 +660,38 @@ void Homo::vcycle(int l) {
   }
 }
 
+// The fine level of the V-cycle with the tile kernels: pre-smoothing from u = 0 into u, the
+// residual into r, its restriction, the coarse cycle, then prolongation and post-smoothing in one
+// launch that reads u and writes the result (the preconditioned residual) into r.
+template <typename KT, typename VT>
+void Homo::vcycle_fine_tiled(const KT* k, VT* u, VT* r, const FineOp& fop, const double* fs) {
+  Level& L = lv[0];
+  Level& C = lv[1];
+  const unsigned nt = tile_count(L.d);
+  launch_pdl(k_tile_smooth<false, KT, VT>, dim3(nt), dim3(kSmoothThreads), kTileSmemPre, stream, fmap, L.d, C.d, k,
+             fop, (const VT*)nullptr, (const float*)nullptr, u, fs, cfg.pre_smooth, sc);
+  launch_pdl(k_tile_resid<KT, VT>, dim3(nt), dim3(kResidThreads), kTileSmemResid, stream, fmap, L.d, k, fop,
+             (const VT*)u, r, fs, sc);
+  launch_pdl(k_restrict<3, VT>, dim3(ceil_div(C.d.nv(), kBlock)), dim3(kBlock), 0, stream, L.d, C.d, (const VT*)r,
+             C.f, (const SolveScalars*)sc);
+  launched(3);
+  if (join_in_cycle) {
+    // the coarse levels need the operators of the side stream's chain from here on
+    if (coarse_pending) cudaStreamWaitEvent(stream, ev_coarse, 0);
+    coarse_pending = false;
+    join_in_cycle = false;
+  }
+  vcycle(1);
+  // the profiled region: the post-smoothing launch (prolongation + post_smooth sweeps)
+  const bool timed = cfg.profile && prof_slot >= 0;
+  const unsigned int evflag = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
+  if (timed) cudaEventRecordWithFlags(prof_ev[0][prof_slot], stream, evflag);
+  launch_pdl(k_tile_smooth<true, KT, VT>, dim3(nt), dim3(kSmoothThreads), kTileSmemPost, stream, fmap, L.d, C.d, k,
+             fop, (const VT*)u, (const float*)C.u, r, fs, cfg.post_smooth, sc);
+  if (timed) cudaEventRecordWithFlags(prof_ev[1][prof_slot], stream, evflag);
+  launched(1);
+}
+
 // rho = r . z, then p = (z - zbar) + beta p, q = A p and alpha (z in its storage type VT).
 template <typename VT>
 void Homo::pcg_direction(const VT* z, const float* r, bool face, int nb) {
@@ -612,7 +710,8 @@ void Homo::iteration(int j) {
   const size_t nv = d0.nv();
   const int nb = reduce_blocks(nv);
   float* r = lv[0].f;  // Krylov residual is the V-cycle's level-0 right-hand side
-  float* z = lv[0].u;  // and the V-cycle's level-0 result is the preconditioned residual
+  void* zv = fine_z();  // and the V-cycle's level-0 result is the preconditioned residual
+  float* z = (float*)zv;
   if (mixed && cfg.solver == OTM_SOLVER_PCG) {
     // PCG with the 16-bit V-cycle as preconditioner, the solution in FP64 and exact FP64
     // residual replacements (k_update_x64r requests them, k_resid64 mode 2 performs them)
@@ -620,9 +719,9 @@ void Homo::iteration(int j) {
     vcycle(0);
     // z = xscale_c * u16 is read in place by the two kernels that use it
     if (cfg.precision == OTM_PRECISION_MIXED_BF16)
-      pcg_direction((const __nv_bfloat16*)u16, r, face, nb);
+      pcg_direction((const __nv_bfloat16*)zv, r, face, nb);
     else
-      pcg_direction((const __half*)u16, r, face, nb);
+      pcg_direction((const __half*)zv, r, face, nb);
     launch_pdl(k_update_x64r, dim3(nb), dim3(kBlock), 0, stream, nv, x64, r, p, q, partials, sc, kmax_bits, op.c0,
                cfg.max_iter);
     if (face)
@@ -641,9 +740,9 @@ void Homo::iteration(int j) {
       launch_pdl(k_resid64<false>, dim3(nb), dim3(kBlock), 0, stream, d0, ks, op, x64, b, r, partials, sc, kmax_bits, cfg.max_iter, 0);
     vcycle(0);
     if (cfg.precision == OTM_PRECISION_MIXED_BF16)
-      launch_pdl(k_update64<__nv_bfloat16>, dim3(ceil_div(nv, kBlock)), dim3(kBlock), 0, stream, nv, x64, (const __nv_bfloat16*)u16, sc);
+      launch_pdl(k_update64<__nv_bfloat16>, dim3(ceil_div(nv, kBlock)), dim3(kBlock), 0, stream, nv, x64, (const __nv_bfloat16*)zv, sc);
     else
-      launch_pdl(k_update64<__half>, dim3(ceil_div(nv, kBlock)), dim3(kBlock), 0, stream, nv, x64, (const __half*)u16, sc);
+      launch_pdl(k_update64<__half>, dim3(ceil_div(nv, kBlock)), dim3(kBlock), 0, stream, nv, x64, (const __half*)zv, sc);
     launched(2);
   } else if (cfg.solver == OTM_SOLVER_PCG) {
     vcycle(0);
@@ -920,7 +1019,10 @@ otm_status Homo::solve_impl(bool with_heat) {
     // retry from a zero initial guess, then give up.
   }
   otm_status st = OTM_OK;
-  if (sc_host->nan) {
+  if (sc_host->timeout) {
+    set_error("a tile kernel's bounded wait for its right-hand-side copy ran out");
+    st = OTM_ERR_TIMEOUT;
+  } else if (sc_host->nan) {
     set_error("MG numerical explode");
     st = OTM_ERR_DIVERGED;
   } else {
@@ -1076,6 +1178,7 @@ otm_status otm_config_init(otm_config* cfg) {
   cfg->use_graphs = 1;
   cfg->profile = 0;
   cfg->cluster_cycle = 1;
+  cfg->smoother = OTM_SMOOTHER_COLOR;
   return OTM_OK;
 }
 
@@ -1187,8 +1290,18 @@ otm_status otm_homo_get_profile(otm_homo* h, otm_profile* prof, int reset) {
   const double nv = double(H.lv[0].d.nv());
   prof->sweeps = H.prof_sweeps;
   prof->sweep_ms = H.prof_ms;
-  prof->sweep_bytes = nv * (4.0 + 3.0 * (4.0 + 4.0 + 4.0));
-  prof->launches_per_sweep = H.face ? 8 : 4;
+  if (H.tiled) {
+    // one post-smoothing launch: u_in, u_out (3 cases, storage type), k (storage type), f (FP32,
+    // 3 cases, counted once) and the coarse correction (FP32, 3 cases, one eighth of the vertices)
+    const double s = H.mixed ? 2.0 : 4.0;
+    prof->sweep_bytes = nv * (3.0 * s + 3.0 * s + s + 12.0 + 12.0 / 8.0);
+    prof->launches_per_sweep = 1;
+    prof->kernel_kind = 1;
+  } else {
+    prof->sweep_bytes = nv * (4.0 + 3.0 * (4.0 + 4.0 + 4.0));
+    prof->launches_per_sweep = H.face ? 8 : 4;
+    prof->kernel_kind = 0;
+  }
   if (reset) {
     H.prof_sweeps = 0;
     H.prof_ms = 0.0;

@@ -9,6 +9,7 @@
 #include "otm_solver_kernels.cuh"
 #include "otm_cluster.cuh"
 #include "otm_tail.cuh"
+#include "otm_tile.cuh"
 #include "otm_template.h"
 
 namespace otm {
@@ -65,6 +66,10 @@ struct Homo {
   int cluster_l = -1;       // first level handled by the cluster kernel (-1: none)
   size_t cluster_smem = 0;  // its dynamic shared memory per CTA
   ClDesc cl_desc{};         // its level layout (pointers filled per launch)
+  // fine level smoothed by the tile kernels (one launch per smoothing leg); the post-smoothing
+  // leg writes the preconditioned residual to the residual buffer (lv[0].r, or r16)
+  bool tiled = false;
+  CUtensorMap fmap{};  // TMA map of the fine right-hand side (3 cases, FP32) for the tile kernels
   int tail_l = -1;          // first level handled by the single-CTA tail kernel (-1: none)
   size_t tail_smem = 0;     // its dynamic shared memory
   int nc = 0;
@@ -105,6 +110,7 @@ struct Homo {
                    bool external_mode = false);
   void launch_solve_init();
   void launch_heat_matrix();
+  otm_status tile_attributes();
   otm_status join_coarse();
   otm_status enter();
   otm_status leave();
@@ -113,6 +119,10 @@ struct Homo {
   template <typename T>
   void fine_ops16(int what, int color);
   void vcycle(int l);
+  template <typename KT, typename VT>
+  void vcycle_fine_tiled(const KT* k, VT* u, VT* r, const FineOp& fop, const double* fs);
+  // the fine level's V-cycle result (the preconditioned residual / correction)
+  void* fine_z() const { return tiled ? (mixed ? r16 : (void*)lv[0].r) : (mixed ? u16 : (void*)lv[0].u); }
   template <typename VT>
   void pcg_direction(const VT* z, const float* r, bool face, int nb);
   void gs_first(int l);

@@ -49,6 +49,7 @@ struct SolveScalars {
   double rr_repl[3];  // ||r||^2 at the last replacement
   int repl;           // 1: the next replacement kernel recomputes r = b - A x64
   int nrepl;          // replacements (FP64 residuals) of the current solve
+  int timeout;        // 1 if a kernel's bounded wait for its own asynchronous copy ran out
 };
 
 // Dynamic shared memory limit every large-shared-memory kernel is opted in to. It is one fixed

@@ -193,6 +193,7 @@ __global__ void __launch_bounds__(kBlock) k_init_residual(Dims d, const float* _
       }
       sc->done = all ? 1 : 0;
       sc->nan = bad ? 1 : 0;
+      sc->timeout = 0;
       sc->iter = 0;
       sc->first = 1;
       sc->counter[T_INIT] = 0;
@@ -645,6 +646,7 @@ __global__ void __launch_bounds__(kBlock) k_resid64(Dims d, const float* __restr
       if (init == 1) {
         sc->iter = 0;
         sc->nan = 0;
+        sc->timeout = 0;
         sc->first = 1;
         sc->nrepl = 0;
       }

@@ -20,6 +20,13 @@ def rel_diag(c_gpu: np.ndarray, c_ref: np.ndarray) -> float:
     return float((np.abs(np.diag(c_gpu) - d) / np.abs(d)).max())
 
 
+def rel_entries(c_gpu: np.ndarray, c_ref: np.ndarray) -> np.ndarray:
+    """Error of every K^H entry on its own scale: |dK_ij| / sqrt(|K_ii K_jj|) (for a diagonal entry
+    that is |dK_ii| / |K_ii|)."""
+    d = np.sqrt(np.abs(np.outer(np.diag(c_ref), np.diag(c_ref))))
+    return np.abs(np.asarray(c_gpu) - c_ref) / d
+
+
 def rel_field(a: np.ndarray, b: np.ndarray) -> tuple[float, float]:
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)

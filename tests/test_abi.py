@@ -34,7 +34,7 @@ def test_config_defaults_mirror_homoconfig():
 
 def test_status_strings_and_version():
     L = _lib.lib()
-    assert L.otm_abi_version() == 1
+    assert L.otm_abi_version() == 2
     assert L.otm_status_string(0) == b"ok"
     assert L.otm_status_string(5) == b"not converged"
 

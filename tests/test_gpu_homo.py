@@ -5,7 +5,8 @@ import numpy as np
 import pytest
 
 import oracle as ora
-from tests.helpers import DC_TEST, KH_TOL, SENS_TOL, oracle_solution, random_k, rel_c, rel_diag, rel_field
+from tests.helpers import (DC_TEST, KH_TOL, SENS_TOL, oracle_solution, random_k, rel_c, rel_diag, rel_entries,
+                           rel_field)
 
 torch = pytest.importorskip("torch")
 
@@ -35,6 +36,7 @@ def check_against_oracle(k, C, E, sens, dC=DC_TEST):
     ref = oracle_solution(k)
     assert rel_c(C, ref["C"]) <= KH_TOL, (C, ref["C"])
     assert rel_diag(C, ref["C"]) <= KH_TOL
+    assert rel_entries(C, ref["C"]).max() <= KH_TOL, rel_entries(C, ref["C"])
     for a in range(6):
         mx, l2 = rel_field(E[a], ref["energy"][a])
         assert mx <= SENS_TOL and l2 <= SENS_TOL, (a, mx, l2)
@@ -197,12 +199,15 @@ def test_profile_events_inside_graphs():
     k, _ = random_k((32, 32, 32), seed=15)
     for graphs in (True, False):
         H = Homogenization_H(HomoConfig(reso=32, femRelThres=1e-6, pre_smooth=2, post_smooth=2, profile=True,
-                                        use_graphs=graphs))
+                                        use_graphs=graphs, smoother="tiled"))
         H.update(torch.from_numpy(k).cuda())
         H.heatMatrix()
         pr = H.profile()
         assert pr.sweeps == H.stats().iterations > 0
-        assert pr.sweep_ms > 0 and pr.sweep_bytes == 32 ** 3 * 40
+        # the tiled smoother's timed region is its post-smoothing launch: u in and out, k, f (3 cases,
+        # FP32) and the coarse correction
+        assert pr.kernel_kind == 1 and pr.launches_per_sweep == 1
+        assert pr.sweep_ms > 0 and pr.sweep_bytes == 32 ** 3 * (12 + 12 + 4 + 12 + 1.5)
         # a following library call still works (no stale error from the event queries)
         H.heatMatrix_nosolve()
 
@@ -277,3 +282,38 @@ def test_pinned_host_arrays_and_copies():
     assert torch.from_numpy(a).is_pinned()
     with pytest.raises(ValueError):
         copy_to_device(t, pinned_empty((3,)))
+
+
+@pytest.mark.parametrize("precision", ["fp32", "bf16", "fp16"])
+@pytest.mark.parametrize("shape", [(32, 32, 32), (16, 16, 16), (48, 32, 64), (64, 64, 64)])
+def test_tiled_smoother_matches_color_passes(precision, shape):
+    """The fine level in 16^3 shared-memory tiles (one launch per smoothing leg, block Jacobi across
+    tile faces) meets the oracle gates, agrees with the global colour-pair passes, and needs at most
+    a few more PCG iterations."""
+    nz, ny, nx = shape
+    k, _ = random_k(shape, seed=60 + nx + 2 * ny + 3 * nz)
+    H1, C1, E1, s1 = gpu_run(k, tol=1e-7, precision=precision, smoother="tiled")
+    H2, C2, E2, s2 = gpu_run(k, tol=1e-7, precision=precision, smoother="color")
+    assert rel_c(C1, C2) <= 2e-6
+    assert H1.stats().iterations <= H2.stats().iterations + 3
+    check_against_oracle(k, C1, E1, s1)
+
+
+def test_vcycle_solver_keeps_color_passes():
+    """Stationary V-cycles (MG_H::solveEquation) keep the global colour passes even when the tiled
+    smoother is asked for: block Jacobi across tile faces would not damp every error mode."""
+    k, _ = random_k((16, 16, 16), seed=5)
+    H, C, E, sens = gpu_run(k, tol=1e-7, solver="vcycle", smoother="tiled")
+    assert H.stats().smoother == 0
+    check_against_oracle(k, C, E, sens)
+    H, _, _, _ = gpu_run(k, tol=1e-7, smoother="tiled")
+    assert H.stats().smoother == 1
+
+
+def test_tiled_graphs_and_repeat_bitwise():
+    k, _ = random_k((32, 32, 32), seed=72)
+    _, C1, E1, s1 = gpu_run(k, use_graphs=True, smoother="tiled")
+    _, C2, E2, s2 = gpu_run(k, use_graphs=False, smoother="tiled")
+    _, C3, E3, s3 = gpu_run(k, use_graphs=True, smoother="tiled")
+    assert np.array_equal(C1, C2) and np.array_equal(E1, E2) and np.array_equal(s1, s2)
+    assert np.array_equal(C1, C3) and np.array_equal(s1, s3)
