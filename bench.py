@@ -227,9 +227,10 @@ def run_ours(args, rank, world, local_rank):
         launch_ms = pr.sweep_ms / pr.sweeps / pr.launches_per_sweep
         bytes_launch = pr.sweep_bytes / pr.launches_per_sweep
         achieved = bytes_launch / (launch_ms * 1e-3) / 1e9
-        kname = ("k_tile_smooth<post> (prolongation + 2 tiled Gauss-Seidel sweeps, 3 load cases)" if pr.kernel_kind == 1
+        kname = ("k_tile_sweep (tiled post-smoothing leg: prolongation + 2 Gauss-Seidel sweeps, one launch each, "
+                 "3 load cases)" if pr.kernel_kind == 1
                  else "k_gs_fine_pair (one colour-pair pass, 3 load cases)")
-        tkey = "k_tile_smooth_post" if pr.kernel_kind == 1 else "k_gs_fine_pair"
+        tkey = "k_tile_sweep" if pr.kernel_kind == 1 else "k_gs_fine_pair"
         traffic = None
         tp = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(tp):
@@ -664,8 +665,8 @@ def main():
     ap.add_argument("--iters-per-step", type=int, default=2)
     ap.add_argument("--batched", action="store_true", help="serve: batched form instead of handles on streams")
     ap.add_argument("--streams", type=int, default=8, help="serve: requests running at once in the handle form")
-    ap.add_argument("--smoother", default="color", choices=["tiled", "color"],
-                    help="fine-level smoother: global colour-pair passes (default) or shared-memory tiles")
+    ap.add_argument("--smoother", default="tiled", choices=["tiled", "color"],
+                    help="fine-level smoother: shared-memory tiles (default) or global colour-pair passes")
     args = ap.parse_args()
     if args.workload == "serve":
         run_serve(args)

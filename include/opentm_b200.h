@@ -53,10 +53,11 @@ typedef enum otm_precision {
 typedef enum otm_smoother {
   OTM_SMOOTHER_COLOR = 0, /* one launch per colour pair over the whole level: the reference's global
                              colour order (homogenization/grid.cu:318-471) */
-  OTM_SMOOTHER_TILED = 1  /* fine level in 16^3 shared-memory tiles, one launch per smoothing leg:
+  OTM_SMOOTHER_TILED = 1  /* fine level in 16 x 16 x 8 shared-memory tiles, one launch per sweep:
                              colour-ordered Gauss-Seidel inside a tile, the tile halo held at the
-                             leg's starting values (block Jacobi across tile faces); used with the
-                             PCG solver when every axis is a multiple of 16, else the colour passes */
+                             sweep's starting values, consecutive sweeps on two tilings shifted by
+                             half a tile; used with the PCG solver when nx, ny are multiples of 16
+                             and nz of 8, else the colour passes */
 } otm_smoother;
 
 typedef enum otm_solver {
@@ -83,7 +84,7 @@ typedef struct otm_config {
                             events recorded inside the graph; default 0 */
   int cluster_cycle;     /* run the levels with <= 32^3 unknowns and the coarsest solve in one
                             thread-block-cluster launch when they fit; default 1 */
-  int smoother;          /* otm_smoother of the fine level; default OTM_SMOOTHER_COLOR */
+  int smoother;          /* otm_smoother of the fine level; default OTM_SMOOTHER_TILED */
 } otm_config;
 
 typedef struct otm_solve_stats {
@@ -97,7 +98,7 @@ typedef struct otm_solve_stats {
   int coarsest_reso[3];   /* coarsest level cells per axis */
   int cluster_level;      /* first level of the one-launch cluster cycle, -1 when not used */
   int smoother;           /* otm_smoother the fine level runs with (OTM_SMOOTHER_TILED only with the PCG
-                             solver and every axis a multiple of 16) */
+                             solver and nx, ny multiples of 16, nz of 8) */
 } otm_solve_stats;
 
 /* Event-timed fine-level smoother sweeps collected while profile != 0. */
@@ -107,8 +108,8 @@ typedef struct otm_profile {
   double sweep_bytes;     /* algorithmic bytes of one sweep: nv * (4 + 3 * (4 + 4 + 4)) in FP32 */
   int launches_per_sweep; /* kernel launches per sweep */
   int kernel_kind;        /* 0: the timed region is one colour-pair sweep (launches_per_sweep passes);
-                             1: it is one tiled post-smoothing launch (prolongation + post_smooth sweeps),
-                             sweep_bytes then being that launch's algorithmic bytes */
+                             1: it is the tiled post-smoothing leg (prolongation + post_smooth sweeps, one
+                             launch per sweep), sweep_bytes then being that leg's algorithmic bytes */
 } otm_profile;
 
 /* Pitched 3-D device array, layout-identical to cudaPitchedPtr. */

@@ -114,7 +114,7 @@ class HomoConfig:
     use_graphs: bool = True
     profile: bool = False
     cluster_cycle: bool = True
-    smoother: str = "color"
+    smoother: str = "tiled"
 
     def to_c(self) -> _lib.Config:
         reso = self.reso if not isinstance(self.reso, int) else (self.reso,) * 3

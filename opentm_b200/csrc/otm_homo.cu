@@ -316,6 +316,8 @@ otm_status Homo::build(const otm_config& c, cudaStream_t ext_stream, cudaMemPool
   if (cfg.smoother == OTM_SMOOTHER_TILED && cfg.solver == OTM_SOLVER_PCG && !face && lv.size() > 1 &&
       tile_fits(lv[0].d) && cfg.pre_smooth > 0 && cfg.post_smooth > 0) {
     OTM_TRY(tile_attributes());
+    // the second buffer of the sweep ping-pong (the fine correction's storage type)
+    OTM_TRY(alloc(&u2, 3 * lv[0].d.nv() * (mixed ? 2 : sizeof(float))));
     tiled = true;
   }
   stats.levels = int(lv.size());
@@ -329,17 +331,20 @@ otm_status Homo::build(const otm_config& c, cudaStream_t ext_stream, cudaMemPool
 
 // Dynamic shared memory of the tile kernels (a per-function attribute of the current device; set
 // at every build, which is cheap) and the TMA map of the fine right-hand side: a 4-D tensor
-// {nx, ny, nz, 3 cases} of FP32 whose {16, 16, 8, 3} boxes are the tiles' right-hand sides.
+// {nx, ny, nz, 3 cases} of FP32 read in boxes {8, 8, 4, 3}, eight per tile.
 otm_status Homo::tile_attributes() {
   const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
-  OTM_CUDA(cudaFuncSetAttribute(k_tile_smooth<false, float, float>, a, int(kTileSmemPre)));
-  OTM_CUDA(cudaFuncSetAttribute(k_tile_smooth<true, float, float>, a, int(kTileSmemPost)));
+  OTM_CUDA(cudaFuncSetAttribute(k_tile_sweep<kFromZero, float, float>, a, int(kTileSmemSweep)));
+  OTM_CUDA(cudaFuncSetAttribute(k_tile_sweep<kFromU, float, float>, a, int(kTileSmemSweep)));
+  OTM_CUDA(cudaFuncSetAttribute(k_tile_sweep<kFromUProlong, float, float>, a, int(kTileSmemProlong)));
   OTM_CUDA(cudaFuncSetAttribute(k_tile_resid<float, float>, a, int(kTileSmemResid)));
-  OTM_CUDA(cudaFuncSetAttribute(k_tile_smooth<false, __nv_bfloat16, __nv_bfloat16>, a, int(kTileSmemPre)));
-  OTM_CUDA(cudaFuncSetAttribute(k_tile_smooth<true, __nv_bfloat16, __nv_bfloat16>, a, int(kTileSmemPost)));
+  OTM_CUDA(cudaFuncSetAttribute(k_tile_sweep<kFromZero, __nv_bfloat16, __nv_bfloat16>, a, int(kTileSmemSweep)));
+  OTM_CUDA(cudaFuncSetAttribute(k_tile_sweep<kFromU, __nv_bfloat16, __nv_bfloat16>, a, int(kTileSmemSweep)));
+  OTM_CUDA(cudaFuncSetAttribute(k_tile_sweep<kFromUProlong, __nv_bfloat16, __nv_bfloat16>, a, int(kTileSmemProlong)));
   OTM_CUDA(cudaFuncSetAttribute(k_tile_resid<__nv_bfloat16, __nv_bfloat16>, a, int(kTileSmemResid)));
-  OTM_CUDA(cudaFuncSetAttribute(k_tile_smooth<false, __half, __half>, a, int(kTileSmemPre)));
-  OTM_CUDA(cudaFuncSetAttribute(k_tile_smooth<true, __half, __half>, a, int(kTileSmemPost)));
+  OTM_CUDA(cudaFuncSetAttribute(k_tile_sweep<kFromZero, __half, __half>, a, int(kTileSmemSweep)));
+  OTM_CUDA(cudaFuncSetAttribute(k_tile_sweep<kFromU, __half, __half>, a, int(kTileSmemSweep)));
+  OTM_CUDA(cudaFuncSetAttribute(k_tile_sweep<kFromUProlong, __half, __half>, a, int(kTileSmemProlong)));
   OTM_CUDA(cudaFuncSetAttribute(k_tile_resid<__half, __half>, a, int(kTileSmemResid)));
   static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
   if (!encode) {
@@ -355,7 +360,7 @@ otm_status Homo::tile_attributes() {
   const Dims d = lv[0].d;
   const cuuint64_t dims[4] = {cuuint64_t(d.nx), cuuint64_t(d.ny), cuuint64_t(d.nz), 3};
   const cuuint64_t strides[3] = {cuuint64_t(d.nx) * 4, cuuint64_t(d.nx) * d.ny * 4, cuuint64_t(d.nv()) * 4};
-  const cuuint32_t box[4] = {cuuint32_t(kTX), cuuint32_t(kTY), cuuint32_t(kTZ), 3};
+  const cuuint32_t box[4] = {cuuint32_t(kFBX), cuuint32_t(kFBY), cuuint32_t(kFBZ), 3};
   const cuuint32_t estr[4] = {1, 1, 1, 1};
   const CUresult r = encode(&fmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, lv[0].f, dims, strides, box, estr,
                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
@@ -660,21 +665,29 @@ void Homo::vcycle(int l) {
   }
 }
 
-// The fine level of the V-cycle with the tile kernels: pre-smoothing from u = 0 into u, the
-// residual into r, its restriction, the coarse cycle, then prolongation and post-smoothing in one
-// launch that reads u and writes the result (the preconditioned residual) into r.
+// The fine level of the V-cycle with the tile kernels. Pre-smoothing: one launch per sweep,
+// starting from u = 0, tilings 0, 1, 0, ... (ping-pong between u and u2); the residual of its
+// result into r and the restriction; the coarse cycle; post-smoothing with the tilings mirrored
+// (the last sweep on tiling 0), the first sweep adding the prolongation of the coarse correction,
+// the last one writing the V-cycle's result (the preconditioned residual) into r.
 template <typename KT, typename VT>
 void Homo::vcycle_fine_tiled(const KT* k, VT* u, VT* r, const FineOp& fop, const double* fs) {
   Level& L = lv[0];
   Level& C = lv[1];
   const unsigned nt = tile_count(L.d);
-  launch_pdl(k_tile_smooth<false, KT, VT>, dim3(nt), dim3(kSmoothThreads), kTileSmemPre, stream, fmap, L.d, C.d, k,
-             fop, (const VT*)nullptr, (const float*)nullptr, u, fs, cfg.pre_smooth, sc);
+  VT* buf[2] = {u, (VT*)u2};
+  const int npre = cfg.pre_smooth, npost = cfg.post_smooth;
+  launch_pdl(k_tile_sweep<kFromZero, KT, VT>, dim3(nt), dim3(kSmoothThreads), kTileSmemSweep, stream, fmap, L.d, C.d,
+             k, fop, (const VT*)nullptr, (const float*)nullptr, buf[0], fs, 0, 0, sc);
+  for (int s = 1; s < npre; s++)
+    launch_pdl(k_tile_sweep<kFromU, KT, VT>, dim3(nt), dim3(kSmoothThreads), kTileSmemSweep, stream, fmap, L.d, C.d,
+               k, fop, (const VT*)buf[(s - 1) & 1], (const float*)nullptr, buf[s & 1], fs, s & 1, 0, sc);
+  VT* pre = buf[(npre - 1) & 1];
   launch_pdl(k_tile_resid<KT, VT>, dim3(nt), dim3(kResidThreads), kTileSmemResid, stream, fmap, L.d, k, fop,
-             (const VT*)u, r, fs, sc);
+             (const VT*)pre, r, fs, sc);
   launch_pdl(k_restrict<3, VT>, dim3(ceil_div(C.d.nv(), kBlock)), dim3(kBlock), 0, stream, L.d, C.d, (const VT*)r,
              C.f, (const SolveScalars*)sc);
-  launched(3);
+  launched(npre + 2);
   if (join_in_cycle) {
     // the coarse levels need the operators of the side stream's chain from here on
     if (coarse_pending) cudaStreamWaitEvent(stream, ev_coarse, 0);
@@ -682,14 +695,24 @@ void Homo::vcycle_fine_tiled(const KT* k, VT* u, VT* r, const FineOp& fop, const
     join_in_cycle = false;
   }
   vcycle(1);
-  // the profiled region: the post-smoothing launch (prolongation + post_smooth sweeps)
+  // the profiled region: the post-smoothing leg (post_smooth single-sweep launches)
   const bool timed = cfg.profile && prof_slot >= 0;
   const unsigned int evflag = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
   if (timed) cudaEventRecordWithFlags(prof_ev[0][prof_slot], stream, evflag);
-  launch_pdl(k_tile_smooth<true, KT, VT>, dim3(nt), dim3(kSmoothThreads), kTileSmemPost, stream, fmap, L.d, C.d, k,
-             fop, (const VT*)u, (const float*)C.u, r, fs, cfg.post_smooth, sc);
+  VT* in = pre;
+  for (int s = 0; s < npost; s++) {
+    VT* out = (s == npost - 1) ? r : (in == buf[0] ? buf[1] : buf[0]);
+    const int shift = (npost - 1 - s) & 1;
+    if (s == 0)
+      launch_pdl(k_tile_sweep<kFromUProlong, KT, VT>, dim3(nt), dim3(kSmoothThreads), kTileSmemProlong, stream, fmap,
+                 L.d, C.d, k, fop, (const VT*)in, (const float*)C.u, out, fs, shift, 1, sc);
+    else
+      launch_pdl(k_tile_sweep<kFromU, KT, VT>, dim3(nt), dim3(kSmoothThreads), kTileSmemSweep, stream, fmap, L.d,
+                 C.d, k, fop, (const VT*)in, (const float*)nullptr, out, fs, shift, 1, sc);
+    in = out;
+  }
   if (timed) cudaEventRecordWithFlags(prof_ev[1][prof_slot], stream, evflag);
-  launched(1);
+  launched(npost);
 }
 
 // rho = r . z, then p = (z - zbar) + beta p, q = A p and alpha (z in its storage type VT).
@@ -1178,7 +1201,7 @@ otm_status otm_config_init(otm_config* cfg) {
   cfg->use_graphs = 1;
   cfg->profile = 0;
   cfg->cluster_cycle = 1;
-  cfg->smoother = OTM_SMOOTHER_COLOR;
+  cfg->smoother = OTM_SMOOTHER_TILED;
   return OTM_OK;
 }
 
@@ -1291,11 +1314,13 @@ otm_status otm_homo_get_profile(otm_homo* h, otm_profile* prof, int reset) {
   prof->sweeps = H.prof_sweeps;
   prof->sweep_ms = H.prof_ms;
   if (H.tiled) {
-    // one post-smoothing launch: u_in, u_out (3 cases, storage type), k (storage type), f (FP32,
-    // 3 cases, counted once) and the coarse correction (FP32, 3 cases, one eighth of the vertices)
+    // the post-smoothing leg, one launch per sweep: each reads u_in and k and writes u_out (storage
+    // type, 3 cases) and reads f (FP32, 3 cases); the first also reads the coarse correction (FP32,
+    // 3 cases, one eighth of the vertices)
     const double s = H.mixed ? 2.0 : 4.0;
-    prof->sweep_bytes = nv * (3.0 * s + 3.0 * s + s + 12.0 + 12.0 / 8.0);
-    prof->launches_per_sweep = 1;
+    const int n = H.cfg.post_smooth;
+    prof->sweep_bytes = nv * (n * (3.0 * s + s + 12.0 + 3.0 * s) + 12.0 / 8.0);
+    prof->launches_per_sweep = n;
     prof->kernel_kind = 1;
   } else {
     prof->sweep_bytes = nv * (4.0 + 3.0 * (4.0 + 4.0 + 4.0));

@@ -55,6 +55,7 @@ struct Homo {
   void* k16 = nullptr;
   void* u16 = nullptr;
   void* r16 = nullptr;
+  void* u2 = nullptr;  // tiled smoother: second buffer of the sweep ping-pong (fine storage type)
   FineOp op0{};  // op / c0
   float* ks = nullptr;    // solver conductivity 1e-9 + k^p
   float* kraw = nullptr;  // conductivity as imported

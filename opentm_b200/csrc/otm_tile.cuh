@@ -1,27 +1,32 @@
 // otm_tile.cuh -- tile-staged fine-level smoother and residual (sm_100a).
 //
-// The fine level's Gauss-Seidel smoothing runs one launch per smoothing leg instead of one
-// launch per colour pair: every CTA stages a tile of 16 x 16 x 8 vertices plus a one-site halo in
-// shared memory, as one float4 per site {u_case0, u_case1, u_case2, k_e} (k_e the conductivity of
-// the element whose lower corner is the site), runs all colour-pair passes of all sweeps of the leg
-// inside the tile with the halo held at the values it had when the leg started, and writes the
-// tile's interior back once. Inside a tile this is the colour-ordered Gauss-Seidel sweep of the
-// reference smoother (homogenization/grid.cu:318-471, colours in the order 0,4,1,5,2,6,3,7, the
-// pairs (cx,cy,0)/(cx,cy,1) updated together because the cube element couples no vertices one
-// edge apart); across tile faces it is block Jacobi (hybrid Gauss-Seidel). The leg after the
-// coarse-grid correction adds the trilinear prolongation P u_c while it stages the tile and
-// writes its result to a second buffer, so that no tile reads a halo another tile has already
-// overwritten. Pre-smoothing forward, post-smoothing in the reverse pair order: the V-cycle stays
-// symmetric (the post leg's smoother is the transpose of the pre leg's), as PCG needs.
+// The fine level's Gauss-Seidel smoothing runs one launch per sweep instead of one launch per
+// colour pair: every CTA stages a tile of 16 x 16 x 8 vertices plus a one-site halo in shared
+// memory, as one float4 per site {u_case0, u_case1, u_case2, k_e} (k_e the conductivity of the
+// element whose lower corner is the site), runs the four colour-pair passes of the sweep inside
+// the tile with the halo held at the values it had when the sweep started, and writes the tile's
+// interior to a second buffer (so that no tile reads a halo another tile has already overwritten).
+// Inside a tile this is the colour-ordered Gauss-Seidel sweep of the reference smoother
+// (homogenization/grid.cu:318-471, colours in the order 0,4,1,5,2,6,3,7, the pairs (cx,cy,0) /
+// (cx,cy,1) updated together because the cube element couples no vertices one edge apart); across
+// tile faces it is block Jacobi. Block Jacobi alone leaves the error that is constant inside each
+// tile and alternates in sign from tile to tile nearly undamped, so consecutive sweeps alternate
+// between two tilings, the second shifted by half a tile along every axis: the faces of one tiling
+// lie inside the tiles of the other. The first sweep after the coarse-grid correction adds the
+// trilinear prolongation P u_c while it stages the tile. Pre-smoothing runs forward with the
+// tilings 0, 1, 0, ..., post-smoothing in the reverse pair order with the tilings mirrored, so the
+// V-cycle stays symmetric (the post leg is the transpose of the pre leg), as PCG needs.
 //
-// The tile's right-hand side (3 cases, FP32, 24 KB) arrives by one TMA tensor copy
-// (cp.async.bulk.tensor, a 4-D box {16, 16, 8, 3} of the level's right-hand side, completion on an
-// mbarrier) issued at kernel entry, so it lands while the threads stage the sites.
+// The tile's right-hand side (3 cases, FP32, 24 KB) arrives by TMA tensor copies
+// (cp.async.bulk.tensor of eight 4-D boxes {8, 8, 4, 3}, whose periodic origins a shifted tile
+// may wrap, completion on one mbarrier) issued at kernel entry, so it lands while the threads
+// stage the sites.
 //
 // Shared-memory layout of the sites: site (lx, ly, lz), lx, ly in [0, 18), lz in [0, 10), lies at
-// lz * 324 + ly * 18 + (lx odd ? 9 + lx / 2 : lx / 2): within a row the even and the odd sites
-// are stored apart, so that the 8 lanes of a quarter warp, which update every other site of a row,
-// read 8 consecutive float4 (one 128-byte wavefront, no bank conflict).
+// lz * 342 + ly * 19 + (lx odd ? 9 + lx / 2 : lx / 2): within a row the even and the odd sites are
+// stored apart, so that the 8 lanes that update every other site of a row read 8 consecutive
+// float4, and rows are padded to 19 float4 so that the rows two apart, which the other lanes of a
+// warp read, start in other banks.
 //
 // A thread owns a column segment of 4 vertices of one colour pair and streams the 6 planes around
 // it: every staged plane is read once (8 neighbour sites + the own site's conductivity) and added
@@ -38,24 +43,30 @@ namespace otm {
 constexpr int kTX = 16, kTY = 16, kTZ = 8;                    // interior vertices of a tile
 constexpr int kSX = kTX + 2, kSY = kTY + 2, kSZ = kTZ + 2;    // staged sites (one halo site each side)
 constexpr int kSHalf = kSX / 2;                               // sites of one parity in a row
-constexpr int kSPlane = kSX * kSY;                            // 324
-constexpr int kSSites = kSPlane * kSZ;                        // 3240
+constexpr int kSRow = kSX + 1;                                // row pitch in float4 (padded)
+constexpr int kSPlane = kSRow * kSY;                          // 342
+constexpr int kSSites = kSPlane * kSZ;                        // 3420
 constexpr int kSmoothThreads = 128;                           // 8 x 8 pair columns x 2 segments
 constexpr int kResidThreads = 256;                            // one thread per column
 constexpr int kSeg = 4;                                       // vertices per thread and pass
 constexpr int kCX = kTX / 2 + 2, kCY = kTY / 2 + 2, kCZ = kTZ / 2 + 2;  // staged coarse sites
 constexpr int kCSites = kCX * kCY * kCZ;                      // 600
-constexpr int kFElems = 3 * kTX * kTY * kTZ;                  // right-hand-side box (6144 floats)
+constexpr int kFElems = 3 * kTX * kTY * kTZ;                  // right-hand side of a tile (6144 floats)
+constexpr int kFBX = 8, kFBY = 8, kFBZ = 4;                   // TMA box of the right-hand side (x 3 cases)
+constexpr int kFBox = kFBX * kFBY * kFBZ * 3;                 // 768 floats per box
+constexpr int kFCase = kFBX * kFBY * kFBZ;                    // case stride inside a box (256)
 static_assert((kTX / 2) * (kTY / 2) * (kTZ / kSeg) == kSmoothThreads, "one thread per column segment");
 static_assert(kTX * kTY == kResidThreads, "one thread per column");
+static_assert(kSeg == kFBZ && kTX == 2 * kFBX && kTY == 2 * kFBY && kTZ == 2 * kFBZ,
+              "a column segment lies in one right-hand-side box along z; 2 x 2 x 2 boxes per tile");
 
-// Dynamic shared memory: [right-hand-side box][mbarrier][sites][coarse block (post leg)], after
-// rounding the base up to 128 bytes (the TMA destination's alignment).
+// Dynamic shared memory: [right-hand-side boxes][mbarrier][sites][coarse block], after rounding the
+// base up to 128 bytes (the TMA destination's alignment).
 constexpr size_t kOffBar = size_t(kFElems) * sizeof(float);
 constexpr size_t kOffSites = kOffBar + 128;
 constexpr size_t kOffCoarse = kOffSites + size_t(kSSites) * sizeof(float4);
-constexpr size_t kTileSmemPre = kOffCoarse + 128;                                      // 76,672 B
-constexpr size_t kTileSmemPost = kOffCoarse + size_t(kCSites) * sizeof(float4) + 128;  // 86,272 B
+constexpr size_t kTileSmemSweep = kOffCoarse + 128;                                      // 79,552 B
+constexpr size_t kTileSmemProlong = kOffCoarse + size_t(kCSites) * sizeof(float4) + 128;  // 89,152 B
 constexpr size_t kTileSmemResid = kOffCoarse + 128;
 constexpr uint32_t kFBytes = uint32_t(kFElems * sizeof(float));
 
@@ -72,38 +83,55 @@ __host__ __device__ inline unsigned tile_count(const Dims& d) {
 }
 
 __device__ __forceinline__ int tsite(int lx, int ly, int lz) {
-  return lz * kSPlane + ly * kSX + ((lx & 1) ? kSHalf + (lx >> 1) : (lx >> 1));
+  return lz * kSPlane + ly * kSRow + ((lx & 1) ? kSHalf + (lx >> 1) : (lx >> 1));
 }
-__device__ __forceinline__ int rsite(int lx, int ly, int lz) { return lz * kSPlane + ly * kSX + lx; }
+__device__ __forceinline__ int rsite(int lx, int ly, int lz) { return lz * kSPlane + ly * kSRow + lx; }
 
-// Origin (x0, y0, z0) of tile b, tiles ordered x fastest so that neighbouring CTAs share halos.
-__device__ __forceinline__ void tile_origin(const Dims& d, unsigned b, int& x0, int& y0, int& z0) {
+// Origin (x0, y0, z0) of tile b of tiling `shift` (0: tiles at multiples of the tile size; 1:
+// shifted by half a tile along every axis, so the last tile of a row wraps around the periodic
+// cell). Tiles are ordered x fastest so that neighbouring CTAs share halos. The origin is not
+// wrapped: global indices of the tile's sites are.
+__device__ __forceinline__ void tile_origin(const Dims& d, unsigned b, int shift, int& x0, int& y0, int& z0) {
   const unsigned ntx = unsigned(d.nx / kTX), nty = unsigned(d.ny / kTY);
   const unsigned q = b / ntx;
-  x0 = int(b - q * ntx) * kTX;
-  y0 = int(q % nty) * kTY;
-  z0 = int(q / nty) * kTZ;
+  x0 = int(b - q * ntx) * kTX + shift * (kTX / 2);
+  y0 = int(q % nty) * kTY + shift * (kTY / 2);
+  z0 = int(q / nty) * kTZ + shift * (kTZ / 2);
 }
 
-// ---- the right-hand-side copy: TMA tensor load completing on an mbarrier ----------------------
+// Position of the right-hand side of tile vertex (x, y, z) (0-based inside the tile) of case 0 in
+// the staged boxes; case c is kFCase further: box (x / 8, y / 8, z / 4), inside it x, y, z, case.
+__device__ __forceinline__ int fpos(int x, int y, int z) {
+  return ((x >> 3) + 2 * (y >> 3) + 4 * (z >> 2)) * kFBox + ((z & 3) * kFBY + (y & 7)) * kFBX + (x & 7);
+}
+
+// ---- the right-hand-side copy: TMA tensor loads completing on an mbarrier ---------------------
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-// Thread 0 initialises the barrier and starts the copy of the tile's right-hand side; the barrier
-// initialisation is published to the other threads by the __syncthreads() that precedes the wait.
-__device__ __forceinline__ void tile_f_copy_start(const CUtensorMap* fmap, float* fsm, uint64_t* bar, int x0, int y0,
-                                                  int z0) {
+// Thread 0 initialises the barrier and starts the copies of the tile's right-hand side (eight
+// boxes, their periodic origins wrapped; an origin is a multiple of 8 (x, y) or 4 (z) and the
+// level's dimensions are multiples of 16 and 8, so no box crosses the periodic boundary). The
+// barrier initialisation is published to the other threads by the __syncthreads() that precedes
+// the wait.
+__device__ __forceinline__ void tile_f_copy_start(const CUtensorMap* fmap, float* fsm, uint64_t* bar, const Dims& d,
+                                                  int x0, int y0, int z0) {
   if (threadIdx.x == 0) {
     const uint32_t b = smem_addr(bar);
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(b), "r"(1) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(kFBytes) : "memory");
-    asm volatile(
-        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
-        "%5}], [%6];" ::"r"(smem_addr(fsm)),
-        "l"(reinterpret_cast<uint64_t>(fmap)), "r"(x0), "r"(y0), "r"(z0), "r"(0), "r"(b)
-        : "memory");
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const int X = wrapm(x0 + kFBX * (q & 1), d.nx), Y = wrapm(y0 + kFBY * ((q >> 1) & 1), d.ny),
+                Z = wrapm(z0 + kFBZ * (q >> 2), d.nz);
+      asm volatile(
+          "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, "
+          "%4, %5}], [%6];" ::"r"(smem_addr(fsm + q * kFBox)),
+          "l"(reinterpret_cast<uint64_t>(fmap)), "r"(X), "r"(Y), "r"(Z), "r"(0), "r"(b)
+          : "memory");
+    }
   }
 }
 
@@ -117,20 +145,26 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait for the copy. Returns false in every thread of the CTA if any thread ran out of
-// polls; then the solve is flagged (timeout + done) and the CTA waits once more, again bounded,
-// for the copy it issued before it returns.
+// Bounded wait for the copies. One thread polls the mbarrier (polls by every thread would compete
+// with the other CTA's passes for shared-memory bandwidth and issue slots); the others wait at the
+// barrier, which also makes the copied data visible to them. Returns false in every thread of the
+// CTA if the polls ran out; then the solve is flagged (timeout + done) and the polling thread waits
+// once more, again bounded, for the copies it issued before the CTA returns.
 __device__ __forceinline__ bool tile_f_copy_wait(uint64_t* bar, SolveScalars* sc) {
-  bool ok = false;
-  for (int i = 0; i < kTileWaitPolls && !ok; i++) ok = mbar_try_wait(bar, 0);
-  if (!__syncthreads_or(!ok)) return true;
-  if (threadIdx.x == 0 && sc) {
-    atomicExch(&sc->timeout, 1);
-    atomicExch(&sc->done, 1);
+  bool ok = true;
+  if (threadIdx.x == 0) {
+    ok = false;
+    for (int i = 0; i < kTileWaitPolls && !ok; i++) ok = mbar_try_wait(bar, 0);
+    if (!ok) {
+      if (sc) {
+        atomicExch(&sc->timeout, 1);
+        atomicExch(&sc->done, 1);
+      }
+      for (int i = 0; i < kTileWaitPolls && !ok; i++) ok = mbar_try_wait(bar, 0);
+      ok = false;
+    }
   }
-  for (int i = 0; i < kTileWaitPolls && !ok; i++) ok = mbar_try_wait(bar, 0);
-  __syncthreads();
-  return false;
+  return !__syncthreads_or(!ok);
 }
 
 // ---- vector loads and stores of 4 consecutive values in the storage types --------------------
@@ -213,8 +247,8 @@ __device__ __forceinline__ void sub_inplane(float (&acc)[3], const float (&Kb)[4
 }
 
 // One colour-pair pass (PX, PY) over the tile's interior: every thread updates the 4 vertices
-// (lx, ly, lz0 .. lz0 + 3) of its column segment, reading planes lz0 - 1 .. lz0 + 4. fsm is the
-// staged right-hand side (box order: x, y, z, case), fs the per-case scale applied to it.
+// (lx, ly, lz0 .. lz0 + 3) of its column segment, reading planes lz0 - 1 .. lz0 + 4. fsm holds the
+// staged right-hand side (see fpos), fs the per-case scale applied to it.
 template <int PX, int PY>
 __device__ __forceinline__ void tile_pass(float4* sm, const float* fsm, const FineOp& op, const float (&fs)[3]) {
   const int t = int(threadIdx.x);
@@ -223,7 +257,7 @@ __device__ __forceinline__ void tile_pass(float4* sm, const float* fsm, const Fi
   // positions of the left / right neighbour columns relative to the own site: the parity of lx
   // is fixed by the pass, so they are compile-time offsets in the parity-split row
   constexpr int oL = PX ? kSHalf - 1 : -kSHalf, oR = PX ? kSHalf : -kSHalf + 1;
-  const float* fcol = fsm + (ly - 1) * kTX + (lx - 1);
+  const float* fcol = fsm + fpos(lx - 1, ly - 1, lz0 - 1);  // vertex q of the segment: + q * 64
   float Kp[4] = {0.f, 0.f, 0.f, 0.f};  // conductivities of the previous plane
   PlaneCoef Cp;                        // coefficients of the previous plane
   float accA[3] = {0.f, 0.f, 0.f}, accB[3] = {0.f, 0.f, 0.f}, accC[3] = {0.f, 0.f, 0.f};  // P-1, P, P+1
@@ -233,14 +267,14 @@ __device__ __forceinline__ void tile_pass(float4* sm, const float* fsm, const Fi
     const int P = lz0 - 1 + s;
     const float4* b = sm + tsite(lx, ly, P);
     float4 nb[8];
-    nb[0] = b[oL - kSX];
-    nb[1] = b[-kSX];
-    nb[2] = b[oR - kSX];
+    nb[0] = b[oL - kSRow];
+    nb[1] = b[-kSRow];
+    nb[2] = b[oR - kSRow];
     nb[3] = b[oL];
     nb[4] = b[oR];
-    nb[5] = b[oL + kSX];
-    nb[6] = b[kSX];
-    nb[7] = b[oR + kSX];
+    nb[5] = b[oL + kSRow];
+    nb[6] = b[kSRow];
+    nb[7] = b[oR + kSRow];
     const float kown = reinterpret_cast<const float*>(b)[3];
     const float K[4] = {nb[0].w, nb[1].w, nb[3].w, kown};
     const float sK = (K[0] + K[1]) + (K[2] + K[3]);
@@ -249,9 +283,9 @@ __device__ __forceinline__ void tile_pass(float4* sm, const float* fsm, const Fi
     // vertex P + 1 (segment index s): its lower element plane is P
     float dC = 0.f;
     if (s < kSeg) {
-      const float* fv = fcol + (lz0 - 1 + s) * (kTX * kTY);
+      const float* fv = fcol + s * (kFBX * kFBY);
 #pragma unroll
-      for (int c = 0; c < 3; c++) accC[c] = fv[c * (kTX * kTY * kTZ)] * fs[c];
+      for (int c = 0; c < 3; c++) accC[c] = fv[c * kFCase] * fs[c];
       sub_plane(accC, C, nb);
       dC = sK;
     }
@@ -309,6 +343,41 @@ __device__ __forceinline__ float3 prolong_site(const float4* cb, int ux, int uy,
   return o;
 }
 
+// The prolongation at the 4 fine sites xs .. xs + 3 of a row (xs even, unwrapped), reading the 3
+// coarse columns under them once per coarse row instead of 8 coarse sites per fine site; the
+// per-site expression and weights are those of prolong_site.
+__device__ __forceinline__ void prolong_quad(const float4* cb, int xs, int uy, int uz, int c0x, int c0y, int c0z,
+                                             float3 (&o)[4]) {
+  const int ax = (xs >> 1) - c0x;  // coarse columns ax, ax + 1, ax + 2
+  const int ay0 = (uy >> 1) - c0y, az0 = (uz >> 1) - c0z;
+  const int ay1 = ay0 + (uy & 1), az1 = az0 + (uz & 1);
+  const float wy1 = (uy & 1) ? 0.5f : 0.f, wz1 = (uz & 1) ? 0.5f : 0.f;
+  const float wy0 = 1.f - wy1, wz0 = 1.f - wz1;
+  const float4* rows[4] = {cb + (ay0 + kCY * az0) * kCX + ax, cb + (ay1 + kCY * az0) * kCX + ax,
+                           cb + (ay0 + kCY * az1) * kCX + ax, cb + (ay1 + kCY * az1) * kCX + ax};
+  float4 v[4][3];
+#pragma unroll
+  for (int r = 0; r < 4; r++)
+#pragma unroll
+    for (int a = 0; a < 3; a++) v[r][a] = rows[r][a];
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    // site xs + e: coarse columns (e / 2) and (e / 2 + (e & 1)), weights 1/0 or 1/2, 1/2
+    const int a0 = e >> 1, a1 = (e >> 1) + (e & 1);
+    const float wx1 = (e & 1) ? 0.5f : 0.f, wx0 = 1.f - wx1;
+    float xr[4][3];
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      xr[r][0] = wx0 * v[r][a0].x + wx1 * v[r][a1].x;
+      xr[r][1] = wx0 * v[r][a0].y + wx1 * v[r][a1].y;
+      xr[r][2] = wx0 * v[r][a0].z + wx1 * v[r][a1].z;
+    }
+    o[e].x = wz0 * (wy0 * xr[0][0] + wy1 * xr[1][0]) + wz1 * (wy0 * xr[2][0] + wy1 * xr[3][0]);
+    o[e].y = wz0 * (wy0 * xr[0][1] + wy1 * xr[1][1]) + wz1 * (wy0 * xr[2][1] + wy1 * xr[3][1]);
+    o[e].z = wz0 * (wy0 * xr[0][2] + wy1 * xr[1][2]) + wz1 * (wy0 * xr[2][2] + wy1 * xr[3][2]);
+  }
+}
+
 // Stages the tile's sites {u_case0, u_case1, u_case2, k_e} in shared memory (parity-split order
 // when kSplit, natural order otherwise). With kWithU the values are u (and, when uc is given, plus
 // the trilinear prolongation of the coarse correction uc, whose block under the tile is staged in
@@ -349,7 +418,7 @@ __device__ __forceinline__ void stage_tile(const Dims& d, const Dims& dc, int x0
     if (w < kQuads) {
       const int q = w & 3, row = w >> 2;
       const int ly = row % kSY, lz = row / kSY;
-      const size_t g = size_t(x0 + 4 * q) +
+      const size_t g = size_t(wrapm(x0 + 4 * q, d.nx)) +
                        size_t(d.nx) * (size_t(wrapm(y0 - 1 + ly, d.ny)) + size_t(d.ny) * wrapm(z0 - 1 + lz, d.nz));
       ld4(ks + g, kq[it]);
       if (kWithU)
@@ -389,6 +458,8 @@ __device__ __forceinline__ void stage_tile(const Dims& d, const Dims& dc, int x0
     if (w < kQuads) {
       const int q = w & 3, row = w >> 2;
       const int ly = row % kSY, lz = row / kSY;
+      float3 p[4] = {};
+      if (prolong) prolong_quad(cb, x0 + 4 * q, y0 - 1 + ly, z0 - 1 + lz, c0x, c0y, c0z, p);
 #pragma unroll
       for (int e = 0; e < 4; e++) {
         const int lx = 1 + 4 * q + e;
@@ -398,10 +469,9 @@ __device__ __forceinline__ void stage_tile(const Dims& d, const Dims& dc, int x0
           v.y = uq[it][1][e];
           v.z = uq[it][2][e];
           if (prolong) {
-            const float3 p = prolong_site(cb, x0 + 4 * q + e, y0 - 1 + ly, z0 - 1 + lz, c0x, c0y, c0z);
-            v.x += p.x;
-            v.y += p.y;
-            v.z += p.z;
+            v.x += p[e].x;
+            v.y += p[e].y;
+            v.z += p[e].z;
           }
         }
         sm[kSplit ? tsite(lx, ly, lz) : rsite(lx, ly, lz)] = v;
@@ -439,19 +509,21 @@ __device__ __forceinline__ unsigned char* tile_smem_base() {
   return reinterpret_cast<unsigned char*>((a + 127) & ~uintptr_t(127));
 }
 
-// One smoothing leg of the fine level on a tile.
-//   kPost = false (pre-smoothing): the leg starts from u = 0 (the halo stays 0), runs `sweeps`
-//     sweeps in the pair order 0,1,2,3 and writes the interior to u_out.
-//   kPost = true (post-smoothing): the tile is staged from u_in + P u_c (trilinear prolongation of
-//     the coarse correction uc, homogenization/grid.cu:881-940), then `sweeps` sweeps in the order
-//     3,2,1,0; the interior goes to u_out, which must not alias u_in.
-// ks: fine conductivity (storage KT); fmap: TMA map of the right-hand side (FP32, 3 cases, scaled
-// per case by fscale when given); u_in / u_out in storage VT; arithmetic and shared memory FP32.
-template <bool kPost, typename KT, typename VT>
+// Start of a sweep: from zero (the first pre-smoothing sweep), from u_in, or from u_in plus the
+// trilinear prolongation of the coarse correction (the first post-smoothing sweep).
+enum TileStart { kFromZero = 0, kFromU = 1, kFromUProlong = 2 };
+
+// One Gauss-Seidel sweep of the fine level on the tiles of tiling `shift` (see above): the tile is
+// staged from the start values (kStart), the four colour-pair passes run in the order 0,1,2,3, or
+// 3,2,1,0 when `reverse`, and the interior goes to u_out, which must not alias u_in. ks: fine
+// conductivity (storage KT); fmap: TMA map of the right-hand side (FP32, 3 cases, scaled per case
+// by fscale when given); u_in / u_out in storage VT; uc: the coarse correction (FP32, kFromUProlong,
+// homogenization/grid.cu:881-940); arithmetic and shared memory FP32.
+template <int kStart, typename KT, typename VT>
 __global__ void __launch_bounds__(kSmoothThreads, 2)
-    k_tile_smooth(const __grid_constant__ CUtensorMap fmap, Dims d, Dims dc, const KT* __restrict__ ks, FineOp op,
-                  const VT* __restrict__ u_in, const float* __restrict__ uc, VT* __restrict__ u_out,
-                  const double* fscale, int sweeps, SolveScalars* sc) {
+    k_tile_sweep(const __grid_constant__ CUtensorMap fmap, Dims d, Dims dc, const KT* __restrict__ ks, FineOp op,
+                 const VT* __restrict__ u_in, const float* __restrict__ uc, VT* __restrict__ u_out,
+                 const double* fscale, int shift, int reverse, SolveScalars* sc) {
   unsigned char* base = tile_smem_base();
   float* fsm = reinterpret_cast<float*>(base);
   uint64_t* bar = reinterpret_cast<uint64_t*>(base + kOffBar);
@@ -460,38 +532,36 @@ __global__ void __launch_bounds__(kSmoothThreads, 2)
   pdl_wait();
   if (sc && solve_done(sc)) return;
   int x0, y0, z0;
-  tile_origin(d, blockIdx.x, x0, y0, z0);
+  tile_origin(d, blockIdx.x, shift, x0, y0, z0);
   const size_t nv = d.nv();
-  tile_f_copy_start(&fmap, fsm, bar, x0, y0, z0);
+  tile_f_copy_start(&fmap, fsm, bar, d, x0, y0, z0);
   float fs[3] = {1.f, 1.f, 1.f};
   if (fscale)
 #pragma unroll
     for (int c = 0; c < 3; c++) fs[c] = float(fscale[c]);
-  stage_tile<kPost, kSmoothThreads, true>(d, dc, x0, y0, z0, ks, u_in, uc, sm, cb);
+  stage_tile<kStart != kFromZero, kSmoothThreads, true>(d, dc, x0, y0, z0, ks, u_in,
+                                                        kStart == kFromUProlong ? uc : nullptr, sm, cb);
   __syncthreads();
   if (!tile_f_copy_wait(bar, sc)) return;
-  for (int sw = 0; sw < sweeps; sw++) {
-    if (!kPost) {
-      tile_pass<0, 0>(sm, fsm, op, fs);
-      __syncthreads();
-      tile_pass<1, 0>(sm, fsm, op, fs);
-      __syncthreads();
-      tile_pass<0, 1>(sm, fsm, op, fs);
-      __syncthreads();
-      tile_pass<1, 1>(sm, fsm, op, fs);
-      __syncthreads();
-    } else {
-      tile_pass<1, 1>(sm, fsm, op, fs);
-      __syncthreads();
-      tile_pass<0, 1>(sm, fsm, op, fs);
-      __syncthreads();
-      tile_pass<1, 0>(sm, fsm, op, fs);
-      __syncthreads();
-      tile_pass<0, 0>(sm, fsm, op, fs);
-      __syncthreads();
-    }
+  if (!reverse) {
+    tile_pass<0, 0>(sm, fsm, op, fs);
+    __syncthreads();
+    tile_pass<1, 0>(sm, fsm, op, fs);
+    __syncthreads();
+    tile_pass<0, 1>(sm, fsm, op, fs);
+    __syncthreads();
+    tile_pass<1, 1>(sm, fsm, op, fs);
+  } else {
+    tile_pass<1, 1>(sm, fsm, op, fs);
+    __syncthreads();
+    tile_pass<0, 1>(sm, fsm, op, fs);
+    __syncthreads();
+    tile_pass<1, 0>(sm, fsm, op, fs);
+    __syncthreads();
+    tile_pass<0, 0>(sm, fsm, op, fs);
   }
-  // interior back to global memory, 4 consecutive x at a time
+  __syncthreads();
+  // interior to global memory, 4 consecutive x at a time
   for (int w = int(threadIdx.x); w < kTX * kTY * kTZ / 4; w += kSmoothThreads) {
     const int q = w & 3, row = w >> 2;
     const int ly = 1 + row % kTY, lz = 1 + row / kTY;
@@ -501,16 +571,17 @@ __global__ void __launch_bounds__(kSmoothThreads, 2)
       const float4 v = sm[tsite(1 + 4 * q + e, ly, lz)];
       o0[e] = v.x, o1[e] = v.y, o2[e] = v.z;
     }
-    const size_t g = size_t(x0 + 4 * q) + size_t(d.nx) * (size_t(y0 + ly - 1) + size_t(d.ny) * size_t(z0 + lz - 1));
+    const size_t g = size_t(wrapm(x0 + 4 * q, d.nx)) +
+                     size_t(d.nx) * (size_t(wrapm(y0 + ly - 1, d.ny)) + size_t(d.ny) * size_t(wrapm(z0 + lz - 1, d.nz)));
     st4(u_out + g, o0);
     st4(u_out + nv + g, o1);
     st4(u_out + 2 * nv + g, o2);
   }
 }
 
-// r = f - A u on the fine level for every vertex of a tile, from a staged tile with its halo
-// (natural site order here: lanes take consecutive sites of a row). A thread owns one column of
-// the tile and streams its 10 planes.
+// r = f - A u on the fine level for every vertex of a tile (tiling 0), from a staged tile with its
+// halo (natural site order here: lanes take consecutive sites of a row). A thread owns one column
+// of the tile and streams its 10 planes.
 template <typename KT, typename VT>
 __global__ void __launch_bounds__(kResidThreads, 2)
     k_tile_resid(const __grid_constant__ CUtensorMap fmap, Dims d, const KT* __restrict__ ks, FineOp op,
@@ -522,9 +593,9 @@ __global__ void __launch_bounds__(kResidThreads, 2)
   pdl_wait();
   if (sc && solve_done(sc)) return;
   int x0, y0, z0;
-  tile_origin(d, blockIdx.x, x0, y0, z0);
+  tile_origin(d, blockIdx.x, 0, x0, y0, z0);
   const size_t nv = d.nv();
-  tile_f_copy_start(&fmap, fsm, bar, x0, y0, z0);
+  tile_f_copy_start(&fmap, fsm, bar, d, x0, y0, z0);
   float fs[3] = {1.f, 1.f, 1.f};
   if (fscale)
 #pragma unroll
@@ -535,7 +606,6 @@ __global__ void __launch_bounds__(kResidThreads, 2)
   const int lx = 1 + (int(threadIdx.x) & 15), ly = 1 + (int(threadIdx.x) >> 4);
   const size_t col = size_t(x0 + lx - 1) + size_t(d.nx) * size_t(y0 + ly - 1);
   const size_t pl = size_t(d.nx) * d.ny;
-  const float* fcol = fsm + (ly - 1) * kTX + (lx - 1);
   float Kp[4] = {0.f, 0.f, 0.f, 0.f};
   PlaneCoef Cp;
   float accA[3] = {0.f, 0.f, 0.f}, accB[3] = {0.f, 0.f, 0.f}, accC[3] = {0.f, 0.f, 0.f};
@@ -545,14 +615,14 @@ __global__ void __launch_bounds__(kResidThreads, 2)
   for (int P = 0; P < kSZ; P++) {
     const float4* b = sm + rsite(lx, ly, P);
     float4 nb[8];
-    nb[0] = b[-kSX - 1];
-    nb[1] = b[-kSX];
-    nb[2] = b[-kSX + 1];
+    nb[0] = b[-kSRow - 1];
+    nb[1] = b[-kSRow];
+    nb[2] = b[-kSRow + 1];
     nb[3] = b[-1];
     nb[4] = b[1];
-    nb[5] = b[kSX - 1];
-    nb[6] = b[kSX];
-    nb[7] = b[kSX + 1];
+    nb[5] = b[kSRow - 1];
+    nb[6] = b[kSRow];
+    nb[7] = b[kSRow + 1];
     const float4 own = b[0];
     const float K[4] = {nb[0].w, nb[1].w, nb[3].w, own.w};
     const float sK = (K[0] + K[1]) + (K[2] + K[3]);
@@ -561,9 +631,9 @@ __global__ void __launch_bounds__(kResidThreads, 2)
     float dC = 0.f;
     // vertex P + 1 (interior planes 1..8): lower element plane P
     if (P + 1 <= kTZ) {
-      const float* fv = fcol + P * (kTX * kTY);
+      const float* fv = fsm + fpos(lx - 1, ly - 1, P);
 #pragma unroll
-      for (int c = 0; c < 3; c++) accC[c] = fv[c * (kTX * kTY * kTZ)] * fs[c];
+      for (int c = 0; c < 3; c++) accC[c] = fv[c * kFCase] * fs[c];
       sub_plane(accC, C, nb);
       dC = sK;
     }

@@ -204,10 +204,10 @@ def test_profile_events_inside_graphs():
         H.heatMatrix()
         pr = H.profile()
         assert pr.sweeps == H.stats().iterations > 0
-        # the tiled smoother's timed region is its post-smoothing launch: u in and out, k, f (3 cases,
-        # FP32) and the coarse correction
-        assert pr.kernel_kind == 1 and pr.launches_per_sweep == 1
-        assert pr.sweep_ms > 0 and pr.sweep_bytes == 32 ** 3 * (12 + 12 + 4 + 12 + 1.5)
+        # the tiled smoother's timed region is its post-smoothing leg, one launch per sweep: each
+        # reads u, k, f and writes u (3 cases, FP32), the first also reads the coarse correction
+        assert pr.kernel_kind == 1 and pr.launches_per_sweep == 2
+        assert pr.sweep_ms > 0 and pr.sweep_bytes == 32 ** 3 * (2 * (12 + 4 + 12 + 12) + 1.5)
         # a following library call still works (no stale error from the event queries)
         H.heatMatrix_nosolve()
 

@@ -1,24 +1,31 @@
 """CPU emulation of the tile-staged fine smoother and residual (opentm_b200/csrc/otm_tile.cuh).
 
-The kernels' index arithmetic is restated here line by line (tile origins, the parity-split
-shared-memory site order, the thread -> column-segment mapping, the six-plane streaming of a
-pass, the staged coarse block of the prolongation, the write-back) and every shared-memory and
-global access is checked to stay in bounds before the kernels run on a GPU. Within a pass no
-thread may read the values (.xyz) of a site that another thread writes in the same pass, and the
-write-back must cover each interior vertex once. The emulated arithmetic is then compared with an
-independent block Gauss-Seidel (whole 27-point rows, colour pairs in order, halo frozen) and an
-independent residual, so the streaming algebra (which plane's conductivities feed which
-coefficient) is checked too."""
+The kernels' index arithmetic is restated here line by line (tile origins of both tilings, the
+periodic wrap of shifted tiles, the parity-split and padded shared-memory site order, the thread ->
+column-segment mapping, the six-plane streaming of a pass, the right-hand-side boxes the TMA copies
+deliver, the staged coarse block and the quad-wise prolongation, the write-back) and every
+shared-memory and global access is checked to stay in bounds before the kernels run on a GPU.
+Within a pass no thread may read the values (.xyz) of a site that another thread writes in the
+same pass, and the write-back must cover each vertex once. The emulated arithmetic is then compared
+with an independent block Gauss-Seidel (whole 27-point rows, colour pairs in order, halo frozen,
+tiles of either tiling) and an independent residual, so the streaming algebra (which plane's
+conductivities feed which coefficient) is checked too."""
 import numpy as np
 import pytest
 
-TX, TY, TZ = 16, 16, 8            # interior vertices of a tile
+TX, TY, TZ = 16, 16, 8  # interior vertices of a tile
 SX, SY, SZ = TX + 2, TY + 2, TZ + 2
-SHALF, SPLANE, SSITES = SX // 2, SX * SY, SX * SY * SZ
+SHALF = SX // 2
+SROW = SX + 1  # padded row pitch
+SPLANE, SSITES = SROW * SY, SROW * SY * SZ
 THREADS, SEG, RTHREADS = 128, 4, 256
 CX, CY, CZ = TX // 2 + 2, TY // 2 + 2, TZ // 2 + 2
 CSITES = CX * CY * CZ
+FBX, FBY, FBZ = 8, 8, 4
+FBOX = FBX * FBY * FBZ * 3
+FCASE = FBX * FBY * FBZ
 OP = dict(c0=0.35, c2=-0.08, c3=-0.095)  # distinct c2 / c3 so that a mix-up shows
+NBR = [(-1, -1), (0, -1), (1, -1), (-1, 0), (1, 0), (-1, 1), (0, 1), (1, 1)]
 
 
 def wrapm(a, n):
@@ -28,32 +35,12 @@ def wrapm(a, n):
 
 def tsite(lx, ly, lz):
     assert 0 <= lx < SX and 0 <= ly < SY and 0 <= lz < SZ
-    return lz * SPLANE + ly * SX + ((SHALF + (lx >> 1)) if (lx & 1) else (lx >> 1))
+    return lz * SPLANE + ly * SROW + ((SHALF + (lx >> 1)) if (lx & 1) else (lx >> 1))
 
 
 def rsite(lx, ly, lz):
     assert 0 <= lx < SX and 0 <= ly < SY and 0 <= lz < SZ
-    return lz * SPLANE + ly * SX + lx
-
-
-def tile_origin(d, b):
-    nx, ny, nz = d
-    ntx, nty = nx // TX, ny // TY
-    q = b // ntx
-    return (b - q * ntx) * TX, (q % nty) * TY, (q // nty) * TZ
-
-
-def f_box(d, f, x0, y0, z0):
-    """The TMA copy: box {16, 16, 8, 3} of the right-hand side at (x0, y0, z0, 0), x fastest."""
-    nx, ny, nz = d
-    nv = nx * ny * nz
-    box = np.zeros(3 * TX * TY * TZ)
-    for c in range(3):
-        for z in range(TZ):
-            for y in range(TY):
-                for x in range(TX):
-                    box[x + TX * (y + TY * (z + TZ * c))] = f[c * nv + gidx(d, x0 + x, y0 + y, z0 + z)]
-    return box
+    return lz * SPLANE + ly * SROW + lx
 
 
 def gidx(d, x, y, z):
@@ -62,13 +49,48 @@ def gidx(d, x, y, z):
     return x + nx * (y + ny * z)
 
 
+def tile_origin(d, b, shift):
+    nx, ny, nz = d
+    ntx, nty = nx // TX, ny // TY
+    q = b // ntx
+    return ((b - q * ntx) * TX + shift * (TX // 2), (q % nty) * TY + shift * (TY // 2),
+            (q // nty) * TZ + shift * (TZ // 2))
+
+
+def fpos(x, y, z):
+    assert 0 <= x < TX and 0 <= y < TY and 0 <= z < TZ
+    return ((x >> 3) + 2 * (y >> 3) + 4 * (z >> 2)) * FBOX + ((z & 3) * FBY + (y & 7)) * FBX + (x & 7)
+
+
+def f_box(d, f, x0, y0, z0):
+    """The eight TMA copies: box q = {8, 8, 4, 3} of the right-hand side at the wrapped origin
+    (x0 + 8 (q & 1), y0 + 8 ((q >> 1) & 1), z0 + 4 (q >> 2), 0), landing at q * 768, x fastest."""
+    nx, ny, nz = d
+    nv = nx * ny * nz
+    box = np.full(8 * FBOX, np.nan)
+    for q in range(8):
+        X, Y, Z = wrapm(x0 + FBX * (q & 1), nx), wrapm(y0 + FBY * ((q >> 1) & 1), ny), wrapm(z0 + FBZ * (q >> 2), nz)
+        assert X + FBX <= nx and Y + FBY <= ny and Z + FBZ <= nz, "a box never crosses the periodic boundary"
+        assert (X * 4) % 16 == 0, "TMA: the innermost coordinate times the element size is a multiple of 16 bytes"
+        for c in range(3):
+            for z in range(FBZ):
+                for y in range(FBY):
+                    for x in range(FBX):
+                        box[q * FBOX + ((c * FBZ + z) * FBY + y) * FBX + x] = f[c * nv + gidx(d, X + x, Y + y, Z + z)]
+    # the position function the passes use reads the values of the global array
+    for c in range(3):
+        for z in range(TZ):
+            for y in range(TY):
+                for x in range(TX):
+                    g = gidx(d, wrapm(x0 + x, nx), wrapm(y0 + y, ny), wrapm(z0 + z, nz))
+                    assert box[fpos(x, y, z) + c * FCASE] == f[c * nv + g]
+    return box
+
+
 def plane_coef(K):
     c2, c3 = OP["c2"], OP["c3"]
     return [c3 * K[0], c2 * (K[0] + K[1]), c3 * K[1], c2 * (K[0] + K[2]), c2 * (K[1] + K[3]), c3 * K[2],
             c2 * (K[2] + K[3]), c3 * K[3]]
-
-
-NBR = [(-1, -1), (0, -1), (1, -1), (-1, 0), (1, 0), (-1, 1), (0, 1), (1, 1)]
 
 
 class Smem:
@@ -108,14 +130,14 @@ def emulate_pass(sm, px, py, fsm, fs):
         assert 1 <= lx <= TX and 1 <= ly <= TY and 1 <= lz0 and lz0 + SEG - 1 <= TZ
         # the compile-time neighbour offsets equal the site order's
         assert tsite(lx - 1, ly, 1) - tsite(lx, ly, 1) == oL and tsite(lx + 1, ly, 1) - tsite(lx, ly, 1) == oR
-        fcol = (ly - 1) * TX + (lx - 1)
+        fcol = fpos(lx - 1, ly - 1, lz0 - 1)
         Kp, Cp = [0.0] * 4, None
         accA, accB, accC = [0.0] * 3, [0.0] * 3, [0.0] * 3
         dA = dB = 0.0
         for s in range(SEG + 2):
             P = lz0 - 1 + s
             b = tsite(lx, ly, P)
-            offs = [oL - SX, -SX, oR - SX, oL, oR, oL + SX, SX, oR + SX]
+            offs = [oL - SROW, -SROW, oR - SROW, oL, oR, oL + SROW, SROW, oR + SROW]
             for n, (ox, oy) in enumerate(NBR):
                 assert b + offs[n] == tsite(lx + ox, ly + oy, P)
             nb = [sm.rd(b + o, t) for o in offs]
@@ -125,10 +147,9 @@ def emulate_pass(sm, px, py, fsm, fs):
             C = plane_coef(K)
             dC = 0.0
             if s < SEG:
-                fv = fcol + (lz0 - 1 + s) * (TX * TY)
-                idx = [fv + c * TX * TY * TZ for c in range(3)]
-                assert all(0 <= q < 3 * TX * TY * TZ for q in idx)
-                accC = [fsm[idx[c]] * fs[c] for c in range(3)]
+                fv = fcol + s * (FBX * FBY)
+                assert fv == fpos(lx - 1, ly - 1, lz0 - 1 + s)
+                accC = [fsm[fv + c * FCASE] * fs[c] for c in range(3)]
                 for n in range(8):
                     for c in range(3):
                         accC[c] -= C[n] * nb[n][c]
@@ -171,42 +192,72 @@ def prolong_site(cb, ux, uy, uz, c0x, c0y, c0z):
     return out
 
 
-def emulate_smooth(d, dc, ks, u_in, uc, f, sweeps, post, fs=(1.0, 1.0, 1.0)):
-    """k_tile_smooth<post> over all tiles."""
+def prolong_quad(cb, xs, uy, uz, c0x, c0y, c0z):
+    """The quad-wise prolongation: 3 coarse columns per coarse row, 4 fine sites."""
+    assert xs % 2 == 0
+    ax = (xs >> 1) - c0x
+    ay0, az0 = (uy >> 1) - c0y, (uz >> 1) - c0z
+    ay1, az1 = ay0 + (uy & 1), az0 + (uz & 1)
+    wy1, wz1 = (0.5 if uy & 1 else 0.0), (0.5 if uz & 1 else 0.0)
+    wy0, wz0 = 1 - wy1, 1 - wz1
+    rows = [(ay0 + CY * az0) * CX + ax, (ay1 + CY * az0) * CX + ax, (ay0 + CY * az1) * CX + ax,
+            (ay1 + CY * az1) * CX + ax]
+    for r in rows:
+        assert 0 <= r and r + 2 < CSITES and (r % CX) + 2 < CX
+    v = [[cb[r + a] for a in range(3)] for r in rows]
+    out = []
+    for e in range(4):
+        a0, a1 = e >> 1, (e >> 1) + (e & 1)
+        wx1 = 0.5 if e & 1 else 0.0
+        wx0 = 1 - wx1
+        xr = [[wx0 * v[r][a0][c] + wx1 * v[r][a1][c] for c in range(3)] for r in range(4)]
+        out.append([wz0 * (wy0 * xr[0][c] + wy1 * xr[1][c]) + wz1 * (wy0 * xr[2][c] + wy1 * xr[3][c])
+                    for c in range(3)])
+    # the same values as the per-site prolongation
+    for e in range(4):
+        ref = prolong_site(cb, xs + e, uy, uz, c0x, c0y, c0z)
+        assert all(out[e][c] == ref[c] for c in range(3))
+    return out
+
+
+def emulate_sweep(d, dc, ks, u_in, uc, f, start, shift, reverse, fs=(1.0, 1.0, 1.0)):
+    """k_tile_sweep<start> over all tiles of tiling `shift`. start: 0 zero, 1 u_in, 2 u_in + P uc."""
     nx, ny, nz = d
     nv = nx * ny * nz
     ntiles = (nx // TX) * (ny // TY) * (nz // TZ)
     out = np.full(3 * nv, np.nan)
     written = np.zeros(nv, dtype=int)
-    perm = sorted(tsite(lx, ly, lz) for lz in range(SZ) for ly in range(SY) for lx in range(SX))
-    assert perm == list(range(SSITES)), "the site order is a bijection"
+    pos = sorted(tsite(lx, ly, lz) for lz in range(SZ) for ly in range(SY) for lx in range(SX))
+    assert len(set(pos)) == SX * SY * SZ and pos[-1] < SSITES, "the site order is one-to-one and in bounds"
     for b in range(ntiles):
-        x0, y0, z0 = tile_origin(d, b)
+        x0, y0, z0 = tile_origin(d, b, shift)
         fsm = f_box(d, f, x0, y0, z0)
         sm = Smem(SSITES)
         c0x, c0y, c0z = x0 // 2 - 1, y0 // 2 - 1, z0 // 2 - 1
         cb = np.zeros((CSITES, 4))
-        if post:
+        if start == 2:
             cnx, cny, cnz = dc
             nvc = cnx * cny * cnz
             for s in range(CSITES):
                 ax, ay, az = s % CX, (s // CX) % CY, s // (CX * CY)
                 g = gidx(dc, wrapm(c0x + ax, cnx), wrapm(c0y + ay, cny), wrapm(c0z + az, cnz))
                 cb[s] = [uc[g], uc[nvc + g], uc[2 * nvc + g], 0.0]
-        staged = np.zeros(SSITES, dtype=int)
+        staged = {}
         for w in range(SY * SZ * (TX // 4)):
             q, row = w & 3, w >> 2
             ly, lz = row % SY, row // SY
             uy, uz = y0 - 1 + ly, z0 - 1 + lz
-            g = gidx(d, x0 + 4 * q, wrapm(uy, ny), wrapm(uz, nz))
+            g = gidx(d, wrapm(x0 + 4 * q, nx), wrapm(uy, ny), wrapm(uz, nz))
             assert g % 4 == 0 and g + 3 < nv and (g + 3) // nx == g // nx  # one aligned 4-wide vector in a row
+            p = prolong_quad(cb, x0 + 4 * q, uy, uz, c0x, c0y, c0z) if start == 2 else None
             for e in range(4):
                 v = [0.0, 0.0, 0.0, ks[g + e]]
-                if post:
-                    p = prolong_site(cb, x0 + 4 * q + e, uy, uz, c0x, c0y, c0z)
-                    v = [u_in[c * nv + g + e] + p[c] for c in range(3)] + [ks[g + e]]
+                if start >= 1:
+                    v = [u_in[c * nv + g + e] for c in range(3)] + [ks[g + e]]
+                if start == 2:
+                    v = [v[c] + p[e][c] for c in range(3)] + [ks[g + e]]
                 i = tsite(1 + 4 * q + e, ly, lz)
-                staged[i] += 1
+                staged[i] = staged.get(i, 0) + 1
                 sm.wr(i, v, -1)
         for w in range(SY * SZ * 2):
             side, row = w & 1, w >> 1
@@ -215,22 +266,22 @@ def emulate_smooth(d, dc, ks, u_in, uc, f, sweeps, post, fs=(1.0, 1.0, 1.0)):
             ux, uy, uz = x0 - 1 + lx, y0 - 1 + ly, z0 - 1 + lz
             g = gidx(d, wrapm(ux, nx), wrapm(uy, ny), wrapm(uz, nz))
             v = [0.0, 0.0, 0.0, ks[g]]
-            if post:
+            if start >= 1:
+                v = [u_in[c * nv + g] for c in range(3)] + [ks[g]]
+            if start == 2:
                 p = prolong_site(cb, ux, uy, uz, c0x, c0y, c0z)
-                v = [u_in[c * nv + g] + p[c] for c in range(3)] + [ks[g]]
+                v = [v[c] + p[c] for c in range(3)] + [ks[g]]
             i = tsite(lx, ly, lz)
-            staged[i] += 1
+            staged[i] = staged.get(i, 0) + 1
             sm.wr(i, v, -1)
-        assert (staged == 1).all(), "every site staged once"
+        assert len(staged) == SX * SY * SZ and set(staged.values()) == {1}, "every site staged once"
         sm.writes, sm.reads = {}, {}
-        order = (3, 2, 1, 0) if post else (0, 1, 2, 3)
-        for _ in range(sweeps):
-            for p in order:
-                emulate_pass(sm, p & 1, p >> 1, fsm, fs)
+        for p in ((3, 2, 1, 0) if reverse else (0, 1, 2, 3)):
+            emulate_pass(sm, p & 1, p >> 1, fsm, fs)
         for w in range(TX * TY * TZ // 4):
             q, row = w & 3, w >> 2
             ly, lz = 1 + row % TY, 1 + row // TY
-            g = gidx(d, x0 + 4 * q, y0 + ly - 1, z0 + lz - 1)
+            g = gidx(d, wrapm(x0 + 4 * q, nx), wrapm(y0 + ly - 1, ny), wrapm(z0 + lz - 1, nz))
             assert g % 4 == 0
             for e in range(4):
                 o = sm.v[tsite(1 + 4 * q + e, ly, lz)]
@@ -242,19 +293,19 @@ def emulate_smooth(d, dc, ks, u_in, uc, f, sweeps, post, fs=(1.0, 1.0, 1.0)):
 
 
 def emulate_resid(d, ks, u, f, fs=(1.0, 1.0, 1.0)):
-    """k_tile_resid over all tiles: 256 threads, one column each, 10 planes streamed."""
+    """k_tile_resid over all tiles of tiling 0: 256 threads, one column each, 10 planes streamed."""
     nx, ny, nz = d
     nv = nx * ny * nz
     r = np.full(3 * nv, np.nan)
     written = np.zeros(nv, dtype=int)
     for b in range((nx // TX) * (ny // TY) * (nz // TZ)):
-        x0, y0, z0 = tile_origin(d, b)
+        x0, y0, z0 = tile_origin(d, b, 0)
         fsm = f_box(d, f, x0, y0, z0)
         sm = np.full((SSITES, 4), np.nan)
         for w in range(SY * SZ * (TX // 4)):
             q, row = w & 3, w >> 2
             ly, lz = row % SY, row // SY
-            g = gidx(d, x0 + 4 * q, wrapm(y0 - 1 + ly, ny), wrapm(z0 - 1 + lz, nz))
+            g = gidx(d, wrapm(x0 + 4 * q, nx), wrapm(y0 - 1 + ly, ny), wrapm(z0 - 1 + lz, nz))
             for e in range(4):
                 sm[rsite(1 + 4 * q + e, ly, lz)] = [u[g + e], u[nv + g + e], u[2 * nv + g + e], ks[g + e]]
         for w in range(SY * SZ * 2):
@@ -263,30 +314,29 @@ def emulate_resid(d, ks, u, f, fs=(1.0, 1.0, 1.0)):
             lx = SX - 1 if side else 0
             g = gidx(d, wrapm(x0 - 1 + lx, nx), wrapm(y0 - 1 + ly, ny), wrapm(z0 - 1 + lz, nz))
             sm[rsite(lx, ly, lz)] = [u[g], u[nv + g], u[2 * nv + g], ks[g]]
-        assert not np.isnan(sm).any(), "every site staged"
         for t in range(RTHREADS):
             lx, ly = 1 + (t & 15), 1 + (t >> 4)
             col = gidx(d, x0 + lx - 1, y0 + ly - 1, 0)
             pl = nx * ny
-            fcol = (ly - 1) * TX + (lx - 1)
             Kp, Cp = [0.0] * 4, None
             accA, accB, accC = [0.0] * 3, [0.0] * 3, [0.0] * 3
             dA = dB = 0.0
             uA, uB = [0.0] * 3, [0.0] * 3
             for P in range(SZ):
                 b0 = rsite(lx, ly, P)
-                offs = [-SX - 1, -SX, -SX + 1, -1, 1, SX - 1, SX, SX + 1]
+                offs = [-SROW - 1, -SROW, -SROW + 1, -1, 1, SROW - 1, SROW, SROW + 1]
                 for n, (ox, oy) in enumerate(NBR):
                     assert b0 + offs[n] == rsite(lx + ox, ly + oy, P)
                 nb = [sm[b0 + o] for o in offs]
                 own = sm[b0]
+                assert not np.isnan(own).any() and not any(np.isnan(x).any() for x in nb), "read a staged site"
                 K = [nb[0][3], nb[1][3], nb[3][3], own[3]]
                 sK = (K[0] + K[1]) + (K[2] + K[3])
                 C = plane_coef(K)
                 dC = 0.0
                 if P + 1 <= TZ:
-                    fv = fcol + P * TX * TY
-                    accC = [fsm[fv + c * TX * TY * TZ] * fs[c] for c in range(3)]
+                    fv = fpos(lx - 1, ly - 1, P)
+                    accC = [fsm[fv + c * FCASE] * fs[c] for c in range(3)]
                     for n in range(8):
                         for c in range(3):
                             accC[c] -= C[n] * nb[n][c]
@@ -341,40 +391,39 @@ def row_coefs(d, ks, x, y, z):
     return out
 
 
-def block_gs(d, ks, u0, f, sweeps, order):
-    """Colour-pair Gauss-Seidel per 16 x 16 x 8 block, the halo (every neighbour outside the block,
-    periodic images of the block's own vertices included) frozen at u0."""
+def block_gs(d, ks, u0, f, order, shift):
+    """One colour-pair Gauss-Seidel sweep per 16 x 16 x 8 block of tiling `shift` (blocks shifted by
+    half a block along every axis for shift 1, wrapping periodically), the halo (every neighbour
+    outside the block, periodic images of the block's own vertices included) frozen at u0."""
     nx, ny, nz = d
     nv = nx * ny * nz
-    u = u0.copy()
+    sx, sy, sz = shift * TX // 2, shift * TY // 2, shift * TZ // 2
     out = u0.copy()
-    for z0 in range(0, nz, TZ):
-        for y0 in range(0, ny, TY):
-            for x0 in range(0, nx, TX):
-                loc = u.copy()  # frozen halo for this block
-                for _ in range(sweeps):
-                    for p in order:
-                        px, py = p & 1, p >> 1
-                        for z in range(z0, z0 + TZ):
-                            for y in range(y0 + py, y0 + TY, 2):
-                                for x in range(x0 + px, x0 + TX, 2):
-                                    A = row_coefs(d, ks, x, y, z)
-                                    v = gidx(d, x, y, z)
-                                    for c in range(3):
-                                        s = f[c * nv + v]
-                                        for (ox, oy, oz), a in A.items():
-                                            if (ox, oy, oz) == (0, 0, 0):
-                                                continue
-                                            inside = (x0 <= x + ox < x0 + TX and y0 <= y + oy < y0 + TY
-                                                      and z0 <= z + oz < z0 + TZ)
-                                            src = loc if inside else u  # the halo stays at u0
-                                            s -= a * src[c * nv + gidx(d, (x + ox) % nx, (y + oy) % ny,
-                                                                         (z + oz) % nz)]
-                                        loc[c * nv + v] = s / A[(0, 0, 0)]
+    for z0 in range(sz, nz + sz, TZ):
+        for y0 in range(sy, ny + sy, TY):
+            for x0 in range(sx, nx + sx, TX):
+                loc = u0.copy()
+                for p in order:
+                    px, py = p & 1, p >> 1
+                    for z in range(z0, z0 + TZ):
+                        for y in range(y0 + py, y0 + TY, 2):
+                            for x in range(x0 + px, x0 + TX, 2):
+                                A = row_coefs(d, ks, x % nx, y % ny, z % nz)
+                                v = gidx(d, x % nx, y % ny, z % nz)
+                                for c in range(3):
+                                    s = f[c * nv + v]
+                                    for (ox, oy, oz), a in A.items():
+                                        if (ox, oy, oz) == (0, 0, 0):
+                                            continue
+                                        inside = (x0 <= x + ox < x0 + TX and y0 <= y + oy < y0 + TY
+                                                  and z0 <= z + oz < z0 + TZ)
+                                        src = loc if inside else u0  # the halo stays at u0
+                                        s -= a * src[c * nv + gidx(d, (x + ox) % nx, (y + oy) % ny, (z + oz) % nz)]
+                                    loc[c * nv + v] = s / A[(0, 0, 0)]
                 for z in range(z0, z0 + TZ):
                     for y in range(y0, y0 + TY):
                         for x in range(x0, x0 + TX):
-                            v = gidx(d, x, y, z)
+                            v = gidx(d, x % nx, y % ny, z % nz)
                             for c in range(3):
                                 out[c * nv + v] = loc[c * nv + v]
     return out
@@ -419,7 +468,7 @@ def prolong(d, dc, uc):
 @pytest.fixture(scope="module")
 def fields():
     rng = np.random.default_rng(7)
-    d = (32, 16, 16)  # two tiles along x and z: halos cross tile faces and wrap periodically
+    d = (32, 16, 16)  # two tiles along x and z: halos cross tile faces, shifted tiles wrap
     dc = (16, 8, 8)
     nv, nvc = 32 * 16 * 16, 16 * 8 * 8
     ks = 0.001 + rng.random(nv)
@@ -429,18 +478,24 @@ def fields():
     return d, dc, ks, f, u_in, uc
 
 
-def test_pre_leg_indices_and_block_gauss_seidel(fields):
+def test_sweep_from_zero_forward_tiling0(fields):
     d, dc, ks, f, u_in, uc = fields
-    got = emulate_smooth(d, dc, ks, None, None, f, sweeps=2, post=False)
-    ref = block_gs(d, ks, np.zeros_like(f), f, 2, (0, 1, 2, 3))
+    got = emulate_sweep(d, dc, ks, None, None, f, start=0, shift=0, reverse=False)
+    ref = block_gs(d, ks, np.zeros_like(f), f, (0, 1, 2, 3), 0)
     assert np.abs(got - ref).max() <= 1e-10 * np.abs(ref).max()
 
 
-def test_post_leg_indices_prolongation_and_reverse_order(fields):
+def test_sweep_from_u_forward_shifted_tiling(fields):
     d, dc, ks, f, u_in, uc = fields
-    got = emulate_smooth(d, dc, ks, u_in, uc, f, sweeps=1, post=True)
-    start = u_in + prolong(d, dc, uc)
-    ref = block_gs(d, ks, start, f, 1, (3, 2, 1, 0))
+    got = emulate_sweep(d, dc, ks, u_in, None, f, start=1, shift=1, reverse=False)
+    ref = block_gs(d, ks, u_in, f, (0, 1, 2, 3), 1)
+    assert np.abs(got - ref).max() <= 1e-10 * np.abs(ref).max()
+
+
+def test_sweep_with_prolongation_reverse_shifted_tiling(fields):
+    d, dc, ks, f, u_in, uc = fields
+    got = emulate_sweep(d, dc, ks, u_in, uc, f, start=2, shift=1, reverse=True)
+    ref = block_gs(d, ks, u_in + prolong(d, dc, uc), f, (3, 2, 1, 0), 1)
     assert np.abs(got - ref).max() <= 1e-10 * np.abs(ref).max()
 
 
