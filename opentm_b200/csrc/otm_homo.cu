@@ -320,6 +320,20 @@ otm_status Homo::build(const otm_config& c, cudaStream_t ext_stream, cudaMemPool
     OTM_TRY(alloc(&u2, 3 * lv[0].d.nv() * (mixed ? 2 : sizeof(float))));
     tiled = true;
   }
+  // coarse levels smoothed by the tile kernels: the levels between the fine level and the cluster
+  // or single-CTA cycle (or the coarsest level) whose axes are multiples of the coarse tile, under
+  // the same conditions as the fine level's tiles
+  if (cfg.smoother == OTM_SMOOTHER_TILED && cfg.solver == OTM_SOLVER_PCG && cfg.pre_smooth > 0 && cfg.post_smooth > 0) {
+    const int L = int(lv.size());
+    int last = L - 1;  // first level not smoothed by regular passes
+    if (cluster_l > 0) last = std::min(last, cluster_l);
+    if (tail_l > 0) last = std::min(last, tail_l);
+    for (int l = 1; l < last; l++) {
+      if (!ctile_fits(lv[l].d)) continue;
+      OTM_TRY(alloc((void**)&lv[l].u2, 3 * lv[l].d.nv() * sizeof(float)));
+      lv[l].ctiled = true;
+    }
+  }
   stats.levels = int(lv.size());
   stats.cluster_level = cluster_l;
   stats.smoother = tiled ? OTM_SMOOTHER_TILED : OTM_SMOOTHER_COLOR;
@@ -594,6 +608,10 @@ void Homo::vcycle(int l) {
       vcycle_fine_tiled<__half, __half>((const __half*)k16, (__half*)u16, (__half*)r16, op0, fs);
     return;
   }
+  if (l > 0 && L.ctiled) {
+    vcycle_coarse_tiled(l);
+    return;
+  }
   const bool m16 = (l == 0 && mixed);
   const bool bf = cfg.precision == OTM_PRECISION_MIXED_BF16;
   // the first pass of the first sweep starts from u = 0: one kernel writes the zero fill and the
@@ -712,6 +730,49 @@ void Homo::vcycle_fine_tiled(const KT* k, VT* u, VT* r, const FineOp& fop, const
     in = out;
   }
   if (timed) cudaEventRecordWithFlags(prof_ev[1][prof_slot], stream, evflag);
+  launched(npost);
+}
+
+// A coarse level of the V-cycle with the tile kernels: pre-smoothing sweeps from u = 0 on the
+// tilings 0, 1, 0, ..., ending in u2; the residual into r and its restriction; the coarser cycle;
+// post-smoothing on the mirrored tilings, the first sweep adding the prolongation of the coarser
+// correction, the last writing the level's result into u (which the finer level prolongs).
+void Homo::vcycle_coarse_tiled(int l) {
+  Level& L = lv[l];
+  Level& C = lv[l + 1];
+  const unsigned nt = ctile_count(L.d);
+  const int npre = cfg.pre_smooth, npost = cfg.post_smooth;
+  const float* none = nullptr;
+  float* in = nullptr;
+  for (int s = 0; s < npre; s++) {
+    float* out = ((npre - 1 - s) % 2 == 0) ? L.u2 : L.u;
+    if (s == 0)
+      launch_pdl(k_ctile_sweep<kFromZero>, dim3(nt), dim3(kCThreads), kCTileSmem, stream, L.d, C.d,
+                 (const float*)L.st, none, none, out, (const float*)L.f, 0, 0, (const SolveScalars*)sc);
+    else
+      launch_pdl(k_ctile_sweep<kFromU>, dim3(nt), dim3(kCThreads), kCTileSmem, stream, L.d, C.d, (const float*)L.st,
+                 (const float*)in, none, out, (const float*)L.f, s & 1, 0, (const SolveScalars*)sc);
+    in = out;
+  }
+  const float* pre = in;
+  launch_pdl(k_resid_coarse<3>, dim3(ceil_div(L.d.nv(), kBlock)), dim3(kBlock), 0, stream, L.d, (const float*)L.st, pre,
+             (const float*)L.f, L.r, (const SolveScalars*)sc);
+  launch_pdl(k_restrict<3, float>, dim3(ceil_div(C.d.nv(), kBlock)), dim3(kBlock), 0, stream, L.d, C.d,
+             (const float*)L.r, C.f, (const SolveScalars*)sc);
+  launched(npre + 2);
+  vcycle(l + 1);
+  const float* pin = pre;
+  for (int s = 0; s < npost; s++) {
+    float* out = (s == npost - 1) ? L.u : (pin == L.r ? L.u2 : L.r);
+    const int shift = (npost - 1 - s) & 1;
+    if (s == 0)
+      launch_pdl(k_ctile_sweep<kFromUProlong>, dim3(nt), dim3(kCThreads), kCTileSmemProlong, stream, L.d, C.d,
+                 (const float*)L.st, pin, (const float*)C.u, out, (const float*)L.f, shift, 1, (const SolveScalars*)sc);
+    else
+      launch_pdl(k_ctile_sweep<kFromU>, dim3(nt), dim3(kCThreads), kCTileSmem, stream, L.d, C.d, (const float*)L.st,
+                 pin, none, out, (const float*)L.f, shift, 1, (const SolveScalars*)sc);
+    pin = out;
+  }
   launched(npost);
 }
 

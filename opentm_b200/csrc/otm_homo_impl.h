@@ -10,6 +10,7 @@
 #include "otm_cluster.cuh"
 #include "otm_tail.cuh"
 #include "otm_tile.cuh"
+#include "otm_ctile.cuh"
 #include "otm_template.h"
 
 namespace otm {
@@ -22,6 +23,9 @@ struct Level {
   float* f = nullptr;
   float* r = nullptr;
   float* st = nullptr;
+  // coarse level smoothed by the tile kernels: second buffer of the sweep ping-pong
+  bool ctiled = false;
+  float* u2 = nullptr;
 };
 
 struct ChunkGraph {
@@ -120,6 +124,7 @@ struct Homo {
   template <typename T>
   void fine_ops16(int what, int color);
   void vcycle(int l);
+  void vcycle_coarse_tiled(int l);
   template <typename KT, typename VT>
   void vcycle_fine_tiled(const KT* k, VT* u, VT* r, const FineOp& fop, const double* fs);
   // the fine level's V-cycle result (the preconditioned residual / correction)

@@ -504,3 +504,184 @@ def test_residual_indices_and_values(fields):
     got = emulate_resid(d, ks, u_in, f)
     ref = residual(d, ks, u_in, f)
     assert np.abs(got - ref).max() <= 1e-10 * np.abs(ref).max()
+
+
+# ---- coarse levels: otm_ctile.cuh -----------------------------------------------------------
+CTX, CTY, CTZ = 16, 8, 8
+CSX, CSY, CSZ = CTX + 2, CTY + 2, CTZ + 2
+CSHALF, CSROW = CSX // 2, CSX + 1
+CSPLANE, CSSITES = CSROW * CSY, CSROW * CSY * CSZ
+CTHREADS = (CTX // 2) * (CTY // 2) * (CTZ // 2)
+CCX, CCY, CCZ = CTX // 2 + 2, CTY // 2 + 2, CTZ // 2 + 2
+CCSITES = CCX * CCY * CCZ
+
+
+def csite(lx, ly, lz):
+    assert 0 <= lx < CSX and 0 <= ly < CSY and 0 <= lz < CSZ
+    return lz * CSPLANE + ly * CSROW + ((CSHALF + (lx >> 1)) if (lx & 1) else (lx >> 1))
+
+
+def ctile_origin(d, b, shift):
+    nx, ny, nz = d
+    ntx, nty = nx // CTX, ny // CTY
+    q = b // ntx
+    return ((b - q * ntx) * CTX + shift * (CTX // 2), (q % nty) * CTY + shift * (CTY // 2),
+            (q // nty) * CTZ + shift * (CTZ // 2))
+
+
+def cb_index(d, x, y, z):
+    nx, ny, nz = d
+    hx, hy = nx // 2, ny // 2
+    colour = (x & 1) + 2 * (y & 1) + 4 * (z & 1)
+    return colour * (nx * ny * nz // 8) + (x >> 1) + hx * ((y >> 1) + hy * (z >> 1))
+
+
+def cprolong_site(cb, ux, uy, uz, c0x, c0y, c0z):
+    ax0, ay0, az0 = (ux >> 1) - c0x, (uy >> 1) - c0y, (uz >> 1) - c0z
+    ax1, ay1, az1 = ax0 + (ux & 1), ay0 + (uy & 1), az0 + (uz & 1)
+    for a, n in ((ax0, CCX), (ax1, CCX), (ay0, CCY), (ay1, CCY), (az0, CCZ), (az1, CCZ)):
+        assert 0 <= a < n
+    wx1, wy1, wz1 = [0.5 if (q & 1) else 0.0 for q in (ux, uy, uz)]
+    wx0, wy0, wz0 = 1 - wx1, 1 - wy1, 1 - wz1
+    r = lambda ay, az: (ay + CCY * az) * CCX
+    out = []
+    for c in range(3):
+        u = cb[:, c]
+        out.append(wz0 * (wy0 * (wx0 * u[r(ay0, az0) + ax0] + wx1 * u[r(ay0, az0) + ax1]) +
+                          wy1 * (wx0 * u[r(ay1, az0) + ax0] + wx1 * u[r(ay1, az0) + ax1])) +
+                   wz1 * (wy0 * (wx0 * u[r(ay0, az1) + ax0] + wx1 * u[r(ay0, az1) + ax1]) +
+                          wy1 * (wx0 * u[r(ay1, az1) + ax0] + wx1 * u[r(ay1, az1) + ax1])))
+    return out
+
+
+def emulate_csweep(d, dc, st, u_in, uc, f, start, shift, reverse):
+    """k_ctile_sweep<start> over all coarse tiles of tiling `shift`."""
+    nx, ny, nz = d
+    nv = nx * ny * nz
+    out = np.full(3 * nv, np.nan)
+    written = np.zeros(nv, dtype=int)
+    pos = [csite(lx, ly, lz) for lz in range(CSZ) for ly in range(CSY) for lx in range(CSX)]
+    assert len(set(pos)) == len(pos) and max(pos) < CSSITES
+    for b in range((nx // CTX) * (ny // CTY) * (nz // CTZ)):
+        x0, y0, z0 = ctile_origin(d, b, shift)
+        c0x, c0y, c0z = x0 // 2 - 1, y0 // 2 - 1, z0 // 2 - 1
+        cb = np.zeros((CCSITES, 4))
+        if start == 2:
+            cnx, cny, cnz = dc
+            nvc = cnx * cny * cnz
+            for q in range(CCSITES):
+                ax, ay, az = q % CCX, (q // CCX) % CCY, q // (CCX * CCY)
+                g = gidx(dc, wrapm(c0x + ax, cnx), wrapm(c0y + ay, cny), wrapm(c0z + az, cnz))
+                cb[q] = [uc[g], uc[nvc + g], uc[2 * nvc + g], 0.0]
+        sm = Smem(CSSITES)
+        for q in range(CSX * CSY * CSZ):
+            lx, ly, lz = q % CSX, (q // CSX) % CSY, q // (CSX * CSY)
+            ux, uy, uz = x0 - 1 + lx, y0 - 1 + ly, z0 - 1 + lz
+            v = [0.0, 0.0, 0.0, 0.0]
+            if start >= 1:
+                g = gidx(d, wrapm(ux, nx), wrapm(uy, ny), wrapm(uz, nz))
+                v = [u_in[c * nv + g] for c in range(3)] + [0.0]
+                if start == 2:
+                    p = cprolong_site(cb, ux, uy, uz, c0x, c0y, c0z)
+                    v = [v[c] + p[c] for c in range(3)] + [0.0]
+            sm.wr(csite(lx, ly, lz), v, -1)
+        sm.writes, sm.reads = {}, {}
+        order = list(range(8))[::-1] if reverse else list(range(8))
+        for col in order:
+            cx, cy, cz = col & 1, (col >> 1) & 1, col >> 2
+            oL, oR = (-CSHALF, -CSHALF + 1) if cx == 0 else (CSHALF - 1, CSHALF)
+            for t in range(CTHREADS):
+                i, j, k = t & 7, (t >> 3) & 3, t >> 5
+                lx, ly, lz = 1 + 2 * i + cx, 1 + 2 * j + cy, 1 + 2 * k + cz
+                X, Y, Z = wrapm(x0 + lx - 1, nx), wrapm(y0 + ly - 1, ny), wrapm(z0 + lz - 1, nz)
+                v = gidx(d, X, Y, Z)
+                sb = cb_index(d, X, Y, Z)
+                assert 0 <= sb < nv
+                s = [st[o * nv + sb] for o in range(27)]
+                acc = [f[c * nv + v] for c in range(3)]
+                base = csite(lx, ly, lz)
+                for o in range(27):
+                    if o == 13:
+                        continue
+                    ox, oy, oz = o % 3 - 1, (o // 3) % 3 - 1, o // 9 - 1
+                    off = (oL if ox < 0 else (oR if ox > 0 else 0)) + oy * CSROW + oz * CSPLANE
+                    assert base + off == csite(lx + ox, ly + oy, lz + oz)
+                    n = sm.rd(base + off, t)
+                    for c in range(3):
+                        acc[c] -= s[o] * n[c]
+                sm.wr(base, [acc[c] / s[13] for c in range(3)] + [0.0], t)
+            sm.check_pass()
+        for q in range(CTX * CTY * CTZ):
+            lx, ly, lz = 1 + q % CTX, 1 + (q // CTX) % CTY, 1 + q // (CTX * CTY)
+            g = gidx(d, wrapm(x0 + lx - 1, nx), wrapm(y0 + ly - 1, ny), wrapm(z0 + lz - 1, nz))
+            written[g] += 1
+            o = sm.v[csite(lx, ly, lz)]
+            for c in range(3):
+                out[c * nv + g] = o[c]
+    assert (written == 1).all()
+    return out
+
+
+def block_gs_stencil(d, st, u0, f, order, shift):
+    """Colour Gauss-Seidel with 27-point stencils per 16 x 8 x 8 block of tiling `shift`, halo frozen."""
+    nx, ny, nz = d
+    nv = nx * ny * nz
+    sx, sy, sz = shift * CTX // 2, shift * CTY // 2, shift * CTZ // 2
+    out = u0.copy()
+    for z0 in range(sz, nz + sz, CTZ):
+        for y0 in range(sy, ny + sy, CTY):
+            for x0 in range(sx, nx + sx, CTX):
+                loc = u0.copy()
+                for col in order:
+                    cx, cy, cz = col & 1, (col >> 1) & 1, col >> 2
+                    for z in range(z0 + cz, z0 + CTZ, 2):
+                        for y in range(y0 + cy, y0 + CTY, 2):
+                            for x in range(x0 + cx, x0 + CTX, 2):
+                                X, Y, Z = x % nx, y % ny, z % nz
+                                v, sb = gidx(d, X, Y, Z), cb_index(d, X, Y, Z)
+                                for c in range(3):
+                                    s = f[c * nv + v]
+                                    for o in range(27):
+                                        if o == 13:
+                                            continue
+                                        ox, oy, oz = o % 3 - 1, (o // 3) % 3 - 1, o // 9 - 1
+                                        inside = (x0 <= x + ox < x0 + CTX and y0 <= y + oy < y0 + CTY
+                                                  and z0 <= z + oz < z0 + CTZ)
+                                        src = loc if inside else u0
+                                        s -= st[o * nv + sb] * src[c * nv + gidx(d, (x + ox) % nx, (y + oy) % ny,
+                                                                                   (z + oz) % nz)]
+                                    loc[c * nv + v] = s / st[13 * nv + sb]
+                for z in range(z0, z0 + CTZ):
+                    for y in range(y0, y0 + CTY):
+                        for x in range(x0, x0 + CTX):
+                            v = gidx(d, x % nx, y % ny, z % nz)
+                            for c in range(3):
+                                out[c * nv + v] = loc[c * nv + v]
+    return out
+
+
+@pytest.fixture(scope="module")
+def cfields():
+    rng = np.random.default_rng(11)
+    d, dc = (32, 16, 16), (16, 8, 8)
+    nv, nvc = 32 * 16 * 16, 16 * 8 * 8
+    st = rng.random(27 * nv) - 0.5
+    st[13 * nv:14 * nv] = 20.0 + rng.random(nv)  # a dominant diagonal
+    f = rng.standard_normal(3 * nv)
+    u_in = rng.standard_normal(3 * nv)
+    uc = rng.standard_normal(3 * nvc)
+    return d, dc, st, f, u_in, uc
+
+
+def test_coarse_sweep_from_zero_tiling0(cfields):
+    d, dc, st, f, u_in, uc = cfields
+    got = emulate_csweep(d, dc, st, None, None, f, start=0, shift=0, reverse=False)
+    ref = block_gs_stencil(d, st, np.zeros_like(f), f, list(range(8)), 0)
+    assert np.abs(got - ref).max() <= 1e-10 * np.abs(ref).max()
+
+
+def test_coarse_sweep_with_prolongation_reverse_shifted(cfields):
+    d, dc, st, f, u_in, uc = cfields
+    got = emulate_csweep(d, dc, st, u_in, uc, f, start=2, shift=1, reverse=True)
+    ref = block_gs_stencil(d, st, u_in + prolong(d, dc, uc), f, list(range(8))[::-1], 1)
+    assert np.abs(got - ref).max() <= 1e-10 * np.abs(ref).max()
