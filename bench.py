@@ -14,10 +14,16 @@ collective); the timed region is bracketed by barrier + synchronize, the per-ran
 time is max-reduced, rank 0 prints one JSON line. The L2 cache (126 MB) is flushed by writing
 a 256 MB buffer before every timed step, outside the timed events.
 
+With N = 1 the line also carries the other configurations measured in the same run (--extra 1,
+the default): `solve32` (configuration 1), `solve256` (configuration 3, the FP32 and both 16-bit
+forms with their K^H and sensitivity errors against the FP64 oracle) and `serve`
+(configuration 5 at 1000 requests/s offered); `mixed` is the same OC loop in the BF16 form with
+its own K^H error.
+
 Reference arm (--impl reference): the reference cannot be built offline, so the FP64 CPU
-restatement of its algorithm (oracle/) runs the same loop on the host cores with all
-threads; each step is a bounded sample: the solve of one of the three load cases (cycling)
-plus the filter/OC work, so three steps make one OC iteration.
+restatement of its algorithm (oracle/) runs the same OC loop on the host cores with all
+threads, step for step: each step is one OC iteration whose 3 load cases are solved from the
+previous iteration's solutions, as our arm's are. Both arms report the same `config`.
 """
 from __future__ import annotations
 
@@ -44,6 +50,13 @@ FILTER_R = 2.0
 P_SIMP, K0, KMIN = 3.0, 1.0, 1e-3
 METRIC = "solves/s & p50/p99 latency, mixed vs FP32 MG on one B200 at K^H err<=1e-5"
 UNIT = "solves/s"
+
+
+def oc_config(n):
+    """The workload of the headline line, shared by both arms (so their configs compare equal)."""
+    return {"workload": f"OC loop, {n}^3 periodic cell, 3 load cases, V(2,2)-PCG to rel.res {TOL}, "
+                        "warm-started load cases", "reso": n, "tol": TOL,
+            "l2": "GPU arm: L2 flushed (256 MB write) before every timed step"}
 
 
 def load_peaks():
@@ -132,7 +145,8 @@ def run_ours(args, rank, world, local_rank):
 
     def make(precision, profile=False):
         H = Homogenization_H(HomoConfig(reso=n, femRelThres=TOL, pre_smooth=2, post_smooth=2, max_iter=200,
-                                        precision=precision, profile=profile, smoother=args.smoother))
+                                        precision=precision, profile=profile, smoother=args.smoother,
+                                        cluster_cycle=bool(args.cluster_cycle)))
         df = DensityFilter((n, n, n), FILTER_R, 1, True, P_SIMP, K0, KMIN)
         oc = OCOptimizer(ne, 0.001, MOVE, DAMP)
         return H, df, oc
@@ -247,9 +261,7 @@ def run_ours(args, rank, world, local_rank):
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(t_main * 1e3 / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"OC loop, {n}^3 periodic cell, 3 load cases, V(2,2)-PCG to rel.res {TOL}",
-                   "reso": n, "tol": TOL, "l2": "flushed (256 MB write) before every timed step",
-                   "replicas": world, "precision": "fp32", "smoother": args.smoother},
+        "config": oc_config(n), "replicas": world, "precision": "fp32", "smoother": args.smoother,
         "p50_ms": round(float(np.percentile(lat, 50)), 4), "p99_ms": round(float(np.percentile(lat, 99)), 4),
         "pcg_iterations_last_step": main["iters"],
         "e2e": {"value": round(args.steps * world / t_e2e, 3), "unit": UNIT, "h2d_bytes_per_step": 4 * ne,
@@ -258,83 +270,103 @@ def run_ours(args, rank, world, local_rank):
         "roofline": roofline,
     }
     if mixed is not None:
-        line["mixed"] = ({"value": round(args.steps * world / t_mixed, 3), "unit": UNIT, "precision": "bf16"}
-                         if t_mixed else mixed)
+        line["mixed"] = ({"value": round(args.steps * world / t_mixed, 3), "unit": UNIT, "precision": "bf16",
+                          "pcg_iterations_last_step": mixed["iters"]} if t_mixed else mixed)
     if clk:
         line["clocks"] = clk
     if world == 1 and not args.no_cpu:
-        line["cpu_baseline"], line["kh_err"] = cpu_baseline(main["k_last"], main["C"][-1])
+        line["cpu_baseline"], err = cpu_baseline(main["k_last"], main["C"][-1])
+        line["kh_err"], line["kh_err_entries"] = err
+        if mixed is not None and "lat_ms" in mixed:
+            _, (e, ee) = cpu_baseline(mixed["k_last"], mixed["C"][-1], timed=False)
+            line["mixed"]["kh_err"], line["mixed"]["kh_err_entries"] = e, ee
+    if world == 1 and args.extra:
+        # the other configurations on the same GPU, measured in the same run
+        line["solve32"] = run_solve32(args, emit=False)
+        line["solve256"] = run_solve256(args, emit=False)
+        line["serve"] = serve_summary(args)
     print(json.dumps(line), flush=True)
     return line
 
 
-def cpu_baseline(k_last, C_gpu):
-    """FP64 oracle (the reference algorithm restated) timed on the host cores for one solve of
-    the same workload (the density the GPU saw in its last timed step), and the K^H error of the
-    GPU result against it."""
+def kh_errors(C_gpu, C_ref):
+    """Largest K^H error relative to max |K|, and every entry's error on its own scale
+    |dK_ij| / sqrt(|K_ii K_jj|)."""
+    C_gpu, C_ref = np.asarray(C_gpu, dtype=np.float64), np.asarray(C_ref, dtype=np.float64)
+    scale = np.sqrt(np.abs(np.outer(np.diag(C_ref), np.diag(C_ref))))
+    ent = np.abs(C_gpu - C_ref) / scale
+    return float(np.abs(C_gpu - C_ref).max() / np.abs(C_ref).max()), [[float(f"{v:.3e}") for v in row] for row in ent]
+
+
+def cpu_baseline(k_last, C_gpu, timed=True):
+    """FP64 oracle (the reference algorithm restated) timed on the host cores for one solve of the
+    same workload (the density the GPU saw in its last timed step), and the K^H errors of the GPU
+    result against it (the oracle converged to 1e-10)."""
     import oracle as ora
     ora.build()
     k = k_last.astype(np.float64)
-    t = time.perf_counter()
-    r = ora.homogenize(k, tol=TOL, want_energy=True)
-    s = ora.sensitivity(r["energy"], k, -np.eye(3))
-    t_solve = time.perf_counter() - t
+    base = None
+    if timed:
+        t = time.perf_counter()
+        r = ora.homogenize(k, tol=TOL, want_energy=True)
+        s = ora.sensitivity(r["energy"], k, -np.eye(3))
+        t_solve = time.perf_counter() - t
+        base = {"value": round(1.0 / t_solve, 5), "unit": UNIT, "cores": ora.num_threads(), "kind": "port",
+                "sample": f"one {k.shape[0]}^3 homogenization solve from a zero initial guess (3 load cases to "
+                          f"{TOL}, K^H, sensitivity) in FP64 with the multigrid-PCG restatement, {t_solve:.2f} s"}
+        del s
     ref = ora.homogenize(k, tol=1e-10)
-    kh_err = float(np.abs(np.asarray(C_gpu) - ref["C"]).max() / np.abs(ref["C"]).max())
-    base = {"value": round(1.0 / t_solve, 5), "unit": UNIT, "cores": ora.num_threads(), "kind": "port",
-            "sample": f"one {k.shape[0]}^3 homogenization solve (3 load cases to {TOL}, K^H, sensitivity) in FP64 "
-                      f"with the multigrid-PCG restatement, {t_solve:.2f} s"}
-    del s
-    return base, kh_err
+    return base, kh_errors(C_gpu, ref["C"])
 
 
 # ---------------------------------------------------------------------------------------
 # Reference arm: the FP64 CPU restatement of the reference algorithm
 # ---------------------------------------------------------------------------------------
 def run_reference(args, rank, world):
+    """The same OC loop as our arm, step for step, in the FP64 restatement on the host cores: each
+    step is one OC iteration (density filter, conductivity, the 3 load cases solved from the
+    previous iteration's solutions with the hierarchy built once, K^H, sensitivity, filter
+    adjoint, OC update)."""
     if rank != 0:
         return None
     import oracle as ora
     from opentm_b200 import workloads as wl
 
     ora.build()
+    ora.set_num_threads(os.cpu_count() or 1)
     n = args.n
     rho = wl.config2_density(n, seed=1).astype(np.float64)
-    state = {"k": None, "wsum": None, "rho_f": None, "energy": np.zeros((6,) + rho.shape)}
+    chi = np.zeros((3, n, n, n))
+    iters = []
 
-    def sample(i):
-        c = i % 3
-        if c == 0:
-            rho_f, ws = ora.conv_forward(rho, 1, FILTER_R, True)
-            state["rho_f"], state["wsum"] = rho_f, ws
-            state["k"] = KMIN + rho_f ** P_SIMP * (K0 - KMIN)
-        r = ora.homogenize(state["k"], tol=TOL, want_energy=True, case_mask=1 << c)
-        state["energy"] += r["energy"]
-        if c == 2:
-            sk = ora.sensitivity(state["energy"], state["k"], -np.eye(3))
-            g = ora.conv_backward(sk * P_SIMP * state["rho_f"] ** (P_SIMP - 1) * (K0 - KMIN), state["wsum"], 1,
-                                  FILTER_R, True)
-            new, _ = ora.oc_update(g, rho, VOLFRAC, 0.001, MOVE, DAMP)
-            rho[...] = new
-            state["energy"][...] = 0.0
+    def step():
+        rho_f, ws = ora.conv_forward(rho, 1, FILTER_R, True)
+        k = KMIN + rho_f ** P_SIMP * (K0 - KMIN)
+        r = ora.homogenize_warm(k, chi, tol=TOL, want_energy=True)
+        iters.append(max(r["iters"]))
+        sk = ora.sensitivity(r["energy"], k, -np.eye(3))
+        g = ora.conv_backward(sk * P_SIMP * rho_f ** (P_SIMP - 1) * (K0 - KMIN), ws, 1, FILTER_R, True)
+        new, _ = ora.oc_update(g, rho, VOLFRAC, 0.001, MOVE, DAMP)
+        rho[...] = new
 
-    for i in range(args.warmup):
-        sample(i)
+    for _ in range(args.warmup):
+        step()
     lat = []
-    for i in range(args.steps):
+    for _ in range(args.steps):
         t = time.perf_counter()
-        sample(args.warmup + i)
+        step()
         lat.append(time.perf_counter() - t)
     total = sum(lat)
-    value = (args.steps / 3.0) / total
+    value = args.steps / total
     line = {"impl": "reference", "metric": METRIC, "value": round(value, 5), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total * 1e3 / args.steps, 3),
+            "p50_ms": round(float(np.percentile(np.array(lat) * 1e3, 50)), 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"OC loop, {n}^3 periodic cell, 3 load cases, V(2,2)-PCG to rel.res {TOL}",
-                       "reso": n, "tol": TOL},
+            "config": oc_config(n), "pcg_iterations_last_step": iters[-1] if iters else None,
             "cpu_baseline": {"value": round(value, 5), "unit": UNIT, "cores": ora.num_threads(), "kind": "port",
-                             "sample": "each step solves one of the 3 load cases (cycling) plus the filter/OC work "
-                                       "of the FP64 multigrid-PCG restatement; 3 steps = 1 solve"},
+                             "sample": "each step is one OC iteration of the FP64 multigrid-PCG restatement: filter, "
+                                       "3 load cases solved from the previous solutions (hierarchy built once per "
+                                       "iteration), K^H, sensitivity, filter adjoint, OC update"},
             "e2e": {"value": round(value, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return line
@@ -359,7 +391,7 @@ def serve_fields(seed=4, per_reso=4):
     return out
 
 
-def run_serve(args):
+def run_serve(args, emit=True):
     import torch
 
     from opentm_b200 import HomoConfig, Homogenization_H, copy_to_device, pinned_empty
@@ -404,7 +436,23 @@ def run_serve(args):
         line.update({k: best[k] for k in ("value", "p50_ms", "p99_ms", "ms_per_step", "steps", "gpu_launches")})
         line["config"]["rate"] = best["rate"]
     line.pop("rate", None)
-    print(json.dumps(line), flush=True)
+    if emit:
+        print(json.dumps(line), flush=True)
+    return line
+
+
+def serve_summary(args, rate=1000.0, requests=2000):
+    """Configuration 5 at one offered rate for the default line: solves/s, p50/p99 latency and the
+    speed-up over serial single-request solves."""
+    a = argparse.Namespace(**vars(args))
+    a.rate, a.requests = rate, requests
+    line = run_serve(a, emit=False)
+    keep = ("value", "unit", "p50_ms", "p99_ms", "serial_fp32_solves_per_s", "speedup_vs_serial", "steps",
+            "gpu_launches")
+    out = {k: line[k] for k in keep if k in line}
+    out["config"] = line["config"]
+    out["config"]["rate"] = rate
+    return out
 
 
 def serve_once(args, fields, rate, serial_rate):
@@ -471,22 +519,27 @@ def serve_once(args, fields, rate, serial_rate):
 # ---------------------------------------------------------------------------------------
 # Configuration 3: one 256^3 solve in FP32 and in the two 16-bit forms, against the FP64 oracle
 # ---------------------------------------------------------------------------------------
-def run_solve256(args):
+def run_solve256(args, emit=True):
     from opentm_b200 import workloads as wl
-    n = 256 if args.n == N_CELL else args.n
-    run_solve(args, n, wl.simp(wl.config3_density(n, seed=2)), "configuration 3",
-              f"{n}^3 thresholded smoothed Gaussian field (seed 2), SIMP p=3", headline="bf16")
+    n = 256 if (args.n == N_CELL or not emit) else args.n
+    return run_solve(args, n, wl.simp(wl.config3_density(n, seed=2)), "configuration 3",
+                     f"{n}^3 thresholded smoothed Gaussian field (seed 2), SIMP p=3", headline="bf16", emit=emit)
 
 
-def run_solve32(args):
+def run_solve32(args, emit=True):
     """Configuration 1: one plain solve of a 32^3 cell with rho ~ U(0.001, 1) (seed 0)."""
     from opentm_b200 import workloads as wl
-    n = 32 if args.n == N_CELL else args.n
-    run_solve(args, n, wl.simp(wl.config1_density(n, seed=0)), "configuration 1",
-              f"{n}^3 rho ~ U(0.001, 1) i.i.d. (seed 0), SIMP p=3", headline="fp32")
+    n = 32 if (args.n == N_CELL or not emit) else args.n
+    return run_solve(args, n, wl.simp(wl.config1_density(n, seed=0)), "configuration 1",
+                     f"{n}^3 rho ~ U(0.001, 1) i.i.d. (seed 0), SIMP p=3", headline="fp32", emit=emit)
 
 
-def run_solve(args, n, k, label, field, headline):
+def run_solve(args, n, k, label, field, headline, emit=True):
+    """One cold solve (update, 3 load cases from zero, K^H, sensitivity) per step in the FP32 and
+    both 16-bit forms, with their K^H (per entry) and sensitivity errors against the FP64 oracle.
+    The oracle reference is converged to 1e-10 from the FP32 solution (the FP64 solution does not
+    depend on the initial guess); run as its own workload, the oracle is also timed cold on the
+    host cores as the CPU baseline."""
     import torch
 
     import oracle as ora
@@ -496,6 +549,7 @@ def run_solve(args, n, k, label, field, headline):
     kd = torch.from_numpy(k).cuda()
     dC = -np.eye(3)
     res = {}
+    chi32 = None
     for prec in ("fp32", "bf16", "fp16"):
         H = Homogenization_H(HomoConfig(reso=n, femRelThres=TOL, pre_smooth=2, post_smooth=2, precision=prec,
                                         warm_start=False, max_iter=200, smoother=args.smoother))
@@ -515,19 +569,31 @@ def run_solve(args, n, k, label, field, headline):
             lat.append(e0.elapsed_time(e1))
         st = H.stats()
         res[prec] = {"ms": float(np.median(lat)), "C": C, "sens": sens.cpu().numpy(), "iterations": st.iterations,
-                     "rel_res": max(st.rel_res)}
+                     "refinements": st.refinements, "rel_res": max(st.rel_res)}
+        if prec == "fp32":
+            chi32 = np.stack([H.solution(c).cpu().numpy() for c in range(3)]).astype(np.float64)
         del H
     ora.build()
-    t = time.perf_counter()
-    ref = ora.homogenize(k.astype(np.float64), tol=1e-10, want_energy=True)
-    s_ref = ora.sensitivity(ref["energy"], k.astype(np.float64), dC)
-    t_ora = time.perf_counter() - t
+    k64 = k.astype(np.float64)
+    base = None
+    if emit:
+        t = time.perf_counter()
+        r0 = ora.homogenize(k64, tol=TOL, want_energy=True)
+        ora.sensitivity(r0["energy"], k64, dC)
+        t_ora = time.perf_counter() - t
+        base = {"value": round(1.0 / t_ora, 4), "unit": "solves/s", "cores": ora.num_threads(), "kind": "port",
+                "sample": f"one {n}^3 cold solve (3 load cases to {TOL}) + sensitivity of the FP64 restatement, "
+                          f"{t_ora:.1f} s"}
+    ref = ora.homogenize_warm(k64, np.ascontiguousarray(chi32), tol=1e-10, want_energy=True)
+    s_ref = ora.sensitivity(ref["energy"], k64, dC)
     out = {}
     for prec, r in res.items():
-        kh = float(np.abs(r["C"] - ref["C"]).max() / np.abs(ref["C"]).max())
+        kh, kh_ent = kh_errors(r["C"], ref["C"])
         se = float(np.abs(r["sens"] - s_ref).max() / np.abs(s_ref).max())
+        se2 = float(np.linalg.norm(r["sens"] - s_ref) / np.linalg.norm(s_ref))
         out[prec] = {"solve_ms": round(r["ms"], 3), "solves_per_s": round(1e3 / r["ms"], 3), "kh_err": kh,
-                     "sens_err": se, "iterations": r["iterations"], "rel_res": r["rel_res"]}
+                     "kh_err_entries": kh_ent, "sens_err": se, "sens_err_l2": se2, "iterations": r["iterations"],
+                     "refinements": r["refinements"], "rel_res": r["rel_res"]}
     line = {"metric": f"{n}^3 solve: solves/s (update + 3 load cases from zero + K^H + sensitivity), error vs "
                       "FP64 oracle",
             "value": out[headline]["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "steps": args.steps,
@@ -535,11 +601,12 @@ def run_solve(args, n, k, label, field, headline):
             "data": "synthetic",
             "config": {"workload": f"{label}: {field}, cold solve to rel.res {TOL}, V(2,2), coarsest FP64 direct",
                        "reso": n},
-            "forms": out, "oracle_seconds": round(t_ora, 2),
-            "cpu_baseline": {"value": round(1.0 / t_ora, 4), "unit": "solves/s", "cores": ora.num_threads(),
-                             "kind": "port", "sample": f"one {n}^3 solve (3 load cases to 1e-10) + sensitivity of "
-                                                       "the FP64 restatement"}}
-    print(json.dumps(line), flush=True)
+            "forms": out}
+    if base:
+        line["cpu_baseline"] = base
+    if emit:
+        print(json.dumps(line), flush=True)
+    return line
 
 
 # ---------------------------------------------------------------------------------------
@@ -665,6 +732,10 @@ def main():
     ap.add_argument("--iters-per-step", type=int, default=2)
     ap.add_argument("--batched", action="store_true", help="serve: batched form instead of handles on streams")
     ap.add_argument("--streams", type=int, default=8, help="serve: requests running at once in the handle form")
+    ap.add_argument("--extra", type=int, default=1,
+                    help="add the 32^3 and 256^3 solves and one serving rate to the default line (N = 1 only)")
+    ap.add_argument("--cluster-cycle", type=int, default=1,
+                    help="run the levels with <= 32^3 unknowns as one thread-block-cluster launch (1) or not (0)")
     ap.add_argument("--smoother", default="tiled", choices=["tiled", "color"],
                     help="fine-level smoother: shared-memory tiles (default) or global colour-pair passes")
     args = ap.parse_args()

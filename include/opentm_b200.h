@@ -180,6 +180,10 @@ OTM_API otm_status otm_homo_get_profile(otm_homo* h, otm_profile* prof, int rese
 
 /* Kernels this library has launched in the process (graph replays count their kernel nodes). */
 OTM_API uint64_t otm_launch_count(void);
+/* Temporary device buffers the handle-free entry points (OC update and filter, MMA subsolver,
+ * server task tables) have taken from the library's scratch memory pool in this process; no
+ * reference counterpart (a diagnostic: an entry point that allocates nothing leaves it unchanged). */
+OTM_API uint64_t otm_scratch_alloc_count(void);
 
 /* Page-locked host memory for the arrays a caller moves to and from the device every step
  * (the densities and sensitivities of an optimisation loop): allocated with cudaHostAlloc, so

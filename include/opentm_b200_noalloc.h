@@ -27,7 +27,12 @@ extern "C" {
  * temporary lives in the library's static device array, so the call allocates nothing.
  * Returns OTM_ERR_UNSUPPORTED for a cell of more than OTM_NOALLOC_MAX_CELLS voxels.
  * The first call on a device looks up the array's device address (cudaGetSymbolAddress); make
- * that first call before any stream capture. All calls share the one array: calls whose GPU
+ * that first call before any stream capture. With lazy module loading (the CUDA default) that
+ * first call is also when the library's device code is loaded and the 8 MiB array is reserved on
+ * the device, so make it (a warm-up call on a small cell will do) before the caller's own
+ * allocator takes the device's memory. The address is kept per device for the life of the
+ * process: do not use this entry point across a cudaDeviceReset of that device. All calls share
+ * the one array: calls whose GPU
  * work overlaps (several streams or host threads at once) race on it, so order them on one
  * stream. The array keeps the last call's contents; nothing in it needs to start at zero,
  * because every element a call reads was written earlier in the same call. */

@@ -145,6 +145,7 @@ SIGNATURES = {
     "otm_homo_get_stats": (_S, [_P, ctypes.POINTER(SolveStats)]),
     "otm_homo_get_profile": (_S, [_P, ctypes.POINTER(Profile), ctypes.c_int]),
     "otm_launch_count": (ctypes.c_uint64, []),
+    "otm_scratch_alloc_count": (ctypes.c_uint64, []),
     "otm_host_alloc": (_S, [ctypes.c_size_t, ctypes.POINTER(_P)]),
     "otm_host_free": (_S, [_P]),
     "otm_copy_to_device": (_S, [_P, _P, ctypes.c_size_t, _P]),

@@ -8,6 +8,7 @@
 // then pay for a fresh allocation).
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <mutex>
 
@@ -19,9 +20,11 @@ namespace {
 constexpr int kPoolMaxDevices = 64;
 cudaMemPool_t g_pools[kPoolMaxDevices] = {};
 std::mutex g_pool_mu;
+std::atomic<uint64_t> g_scratch_allocs{0};
 }  // namespace
 
 cudaError_t scratch_malloc(void** p, size_t bytes, cudaStream_t s) {
+  g_scratch_allocs.fetch_add(1, std::memory_order_relaxed);
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
@@ -51,6 +54,8 @@ cudaError_t scratch_malloc(void** p, size_t bytes, cudaStream_t s) {
 }  // namespace otm
 
 extern "C" {
+
+uint64_t otm_scratch_alloc_count(void) { return otm::g_scratch_allocs.load(); }
 
 otm_status otm_host_alloc(size_t bytes, void** out) {
   if (!out || bytes == 0) return OTM_ERR_INVALID_ARGUMENT;

@@ -50,6 +50,9 @@ def lib():
         L.ora_homogenize_cases.argtypes = [_I, _D, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                            ctypes.c_int, ctypes.c_int, _D, _D, _D, _D]
         L.ora_homogenize_cases.restype = ctypes.c_int
+        L.ora_homogenize_warm.argtypes = [_I, _D, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_int, _D, _D, _D, _D, ctypes.POINTER(ctypes.c_int)]
+        L.ora_homogenize_warm.restype = ctypes.c_int
         L.ora_element_energy.argtypes = [_I, _D, _D]
         L.ora_sensitivity.argtypes = [_I, _D, _D, ctypes.c_double, _D, _D]
         L.ora_conv_forward.argtypes = [_I, _D, _D, _D, ctypes.c_int, ctypes.c_double, ctypes.c_int]
@@ -129,6 +132,23 @@ def homogenize(k: np.ndarray, power_penal: float = 1.0, tol: float = 1e-12, max_
                                     _dp(chi) if chi is not None else None, _dp(en) if en is not None else None,
                                     _dp(rr))
     return {"C": C.reshape(3, 3), "chi": chi, "energy": en, "iters": it, "relres": rr}
+
+
+def homogenize_warm(k: np.ndarray, chi: np.ndarray, power_penal: float = 1.0, tol: float = 1e-12,
+                    max_iter: int = 2000, coarsest_max_dof: int = 64, want_energy: bool = False):
+    """The 3 load cases solved from the initial guess ``chi`` (3, nz, ny, nx; float64, updated in
+    place with the solutions), as the warm-started solve of an optimisation loop. Returns a dict
+    with keys C, energy, iters (per case), relres."""
+    kk = _f64(k)
+    assert chi.dtype == np.float64 and chi.flags["C_CONTIGUOUS"] and chi.shape == (3,) + kk.shape
+    C = np.zeros(9)
+    en = np.zeros((6,) + kk.shape) if want_energy else None
+    rr = np.zeros(3)
+    its = (ctypes.c_int * 3)()
+    lib().ora_homogenize_warm(_dims(kk.shape), _dp(kk), float(power_penal), float(tol), int(max_iter), 1,
+                              int(coarsest_max_dof), _dp(chi), _dp(C), _dp(en) if en is not None else None, _dp(rr),
+                              its)
+    return {"C": C.reshape(3, 3), "energy": en, "iters": list(its), "relres": rr}
 
 
 def element_energy(chi: np.ndarray) -> np.ndarray:

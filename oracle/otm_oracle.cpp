@@ -655,6 +655,62 @@ int ora_homogenize_cases(const int* n, const double* k_in, double power_penal, d
   return worst;
 }
 
+// As ora_homogenize for the 3 load cases, with chi_inout (3 * nv) as the initial guess of every
+// case and the solutions written back to it: the warm-started solve of an optimisation loop
+// (homogenization/homogenization.cu:182-188 keeps each case's last solution as its next initial
+// guess). One hierarchy build per call. iters_out (3, optional) gets each case's PCG iterations.
+int ora_homogenize_warm(const int* n, const double* k_in, double power_penal, double tol, int max_iter, int precond,
+                        int coarsest_max_dof, double* chi_inout, double* C, double* energy_out, double* relres_out,
+                        int* iters_out) {
+  Dims d{{n[0], n[1], n[2]}};
+  const size_t nv = d.nv();
+  std::vector<double> ks(nv);
+  for (size_t e = 0; e < nv; e++) ks[e] = kRhoPenalMin + std::pow(k_in[e], power_penal);
+  double KE[64], fe[24], dp[24];
+  template_matrix(1.0 / n[0] / 2.0, KE, fe, dp);
+  Hierarchy H;
+  H.build(n, ks.data(), KE, coarsest_max_dof > 0 ? coarsest_max_dof : 64);
+  std::vector<double> f(3 * nv);
+  ora_rhs(n, ks.data(), f.data());
+  int worst = 0;
+  for (int c = 0; c < 3; c++) {
+    std::vector<double> fc(f.begin() + c * nv, f.begin() + (c + 1) * nv);
+    remove_mean(fc);
+    std::vector<double> x(chi_inout + c * nv, chi_inout + (c + 1) * nv);
+    double rr = 0.0;
+    int it = pcg(H, fc, x, tol, max_iter, precond, &rr);
+    if (relres_out) relres_out[c] = rr;
+    if (iters_out) iters_out[c] = it;
+    if (rr > tol) worst = -1;
+    if (worst >= 0) worst = std::max(worst, it);
+    std::copy(x.begin(), x.end(), chi_inout + c * nv);
+  }
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  const long long ne = (long long)nv;
+#pragma omp parallel
+  {
+    double loc[6] = {0, 0, 0, 0, 0, 0};
+#pragma omp for schedule(static)
+    for (long long e = 0; e < ne; e++) {
+      double E[6];
+      element_energy(d, KE, dp, chi_inout, size_t(e), E);
+      if (energy_out)
+        for (int q = 0; q < 6; q++) energy_out[q * nv + e] = E[q];
+      for (int q = 0; q < 6; q++) loc[q] += ks[e] * E[q];
+    }
+#pragma omp critical
+    for (int q = 0; q < 6; q++) acc[q] += loc[q];
+  }
+  int cnt = 0;
+  for (int a = 0; a < 3; a++)
+    for (int b = a; b < 3; b++) {
+      C[a * 3 + b] = acc[cnt];
+      C[b * 3 + a] = acc[cnt];
+      cnt++;
+    }
+  return worst;
+}
+
 // Element energies for a given chi (3 * nv), pairs 00 01 02 11 12 22.
 void ora_element_energy(const int* n, const double* chi, double* energy_out) {
   Dims d{{n[0], n[1], n[2]}};

@@ -5,6 +5,7 @@ import pytest
 
 import oracle as ora
 from opentm_b200 import workloads as wl
+from tests.helpers import random_k
 
 
 def test_template_matrix_structure():
@@ -128,3 +129,16 @@ def test_mma_solves_small_convex_problem():
             hi = mu
     x_star = np.clip(t - hi / 2, 0, 1)
     assert np.abs(x - x_star).max() < 1e-3
+
+
+def test_warm_started_solve_matches_cold_and_reuses_the_guess():
+    """homogenize_warm (the reference arm's OC-loop solve) converges to the same K^H as a cold solve
+    and needs no iteration when started from that solution."""
+    k, _ = random_k((16, 16, 16), seed=9)
+    cold = ora.homogenize(k, tol=1e-12)
+    chi = np.zeros((3, 16, 16, 16))
+    warm = ora.homogenize_warm(k, chi, tol=1e-12)
+    assert np.abs(warm["C"] - cold["C"]).max() <= 1e-12 * np.abs(cold["C"]).max()
+    again = ora.homogenize_warm(k, chi, tol=1e-12)
+    assert again["iters"] == [0, 0, 0]
+    assert np.abs(again["C"] - cold["C"]).max() <= 1e-12 * np.abs(cold["C"]).max()
