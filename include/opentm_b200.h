@@ -168,6 +168,23 @@ OTM_API otm_status otm_homo_sensitivity(otm_homo* h, const float dC[9], float* s
 /* dK^H_ij / dk_e for the 6 unique pairs (00 01 02 11 12 22), 6 unpitched fields of ne floats. */
 OTM_API otm_status otm_homo_element_energy(otm_homo* h, float* energy_dev);
 
+/* MG_H::v_cycle(w_SOR, pre, post) (homogenization/MG.cpp:46-71): one V(pre, post) cycle of the
+ * handle's hierarchy (built by the last otm_homo_update) applied to the right-hand sides f_dev of
+ * the 3 load cases (3 * nv device floats, case-major, x fastest) from a zero correction; the
+ * correction is written to u_dev (3 * nv floats). FP32 form only (OTM_ERR_UNSUPPORTED for the
+ * 16-bit forms, whose cycle works on scaled residuals); the smoother is Gauss-Seidel (w_SOR = 1). */
+OTM_API otm_status otm_homo_v_cycle(otm_homo* h, const float* f_dev, float* u_dev, int pre, int post);
+
+/* One level of the hierarchy (Grid_H, homogenization/grid.h:104-421): level 0 is the root. */
+typedef struct otm_level_info {
+  int levels;      /* levels of the hierarchy */
+  int reso[3];     /* cells (= periodic vertices) per axis of this level */
+  int stencil;     /* 1: the level holds assembled 27-point Galerkin stencils; 0: matrix-free */
+  int smoother;    /* otm_smoother of the level (the tile kernels or colour passes); -1: solved
+                      directly, in one cluster launch or in the single-CTA cycle */
+} otm_level_info;
+OTM_API otm_status otm_homo_level(const otm_homo* h, int level, otm_level_info* info);
+
 /* The periodic fluctuation chi of load case c (nv floats, x fastest), as kept in
  * Grid_H::uchar_h (homogenization/grid.cpp:200-211). */
 OTM_API otm_status otm_homo_get_solution(otm_homo* h, int lcase, float* dst_dev);

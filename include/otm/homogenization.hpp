@@ -2,7 +2,11 @@
 // the C ABI of libopentm_b200.so. Class names, constructor arguments and method signatures
 // follow the reference so existing callers compile unchanged:
 //   homo::Homogenization_H   homogenization/homogenization.h:15-30
-//   homo::MG_H (subset)      homogenization/MG.h:14-32
+//   homo::MG_H, MGConfig     homogenization/MG.h:8-32
+//   homo::Grid_H (subset)    homogenization/grid.h:104-421
+//   homo::heat_tensor_t      homogenization/homoExpression.h:69-150, over homo::DensityChain, the
+//                            density expression rho.conv(ker).pow(p) * (k0 - kmin) + kmin that
+//                            runCustom builds (Framework.cu:163)
 //   homo::OCOptimizer        optimization/OCOptimizer.h:7-20
 //   homo::MMAOptimizer       optimization/mmaOptimizer.h:12-35
 //   mmasubDevice             optimization/mmaOpt.h:14-19
@@ -17,7 +21,9 @@
 
 #include <cuda_runtime.h>
 
+#include <array>
 #include <cstdio>
+#include <fstream>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -91,6 +97,7 @@ struct Homogenization_H {
     if (h_) otm_homo_destroy(h_);
     h_ = nullptr;
     config = homconfig;
+    opt_ = opt;
     otm_config c;
     otm_config_init(&c);
     for (int i = 0; i < 3; i++) c.reso[i] = config.reso[i];
@@ -147,6 +154,7 @@ struct Homogenization_H {
     return st;
   }
   otm_homo* handle() { return h_; }
+  const SolverOptions& options() const { return opt_; }
 
   float power_penal = 1;
   float diag_strength = 1e6;
@@ -154,14 +162,69 @@ struct Homogenization_H {
 
  private:
   otm_homo* h_ = nullptr;
+  SolverOptions opt_;
   float* last_rho_ = nullptr;
   int last_pitch_ = -1;
 };
 
-// MG_H view of a Homogenization_H (homogenization/MG.h:14-32): the hierarchy lives inside the
-// handle, so only the solve-level entry points are exposed.
+// MGConfig (homogenization/MG.h:8-12).
+struct MGConfig {
+  int reso[3] = {128, 128, 128};
+  bool enableManagedMem = true;
+  std::string namePrefix;
+};
+
+// One level of the hierarchy (homogenization/grid.h:104-421): its sizes and neighbours. The
+// level's vectors live inside the library's handle; the root grid's right-hand sides and
+// correction (3 load cases, case-major, x fastest) are device buffers owned by the MG_H view, so
+// that v_cycle() works on them as the reference's does on f_g / u_g.
+struct Grid_H {
+  Grid_H* fine = nullptr;
+  Grid_H* Coarse = nullptr;
+  bool is_root = false;
+  bool assemb_otf = false;  // matrix-free (the fine level)
+  std::array<int, 3> cellReso = {};
+  int smoother = 0;  // otm_smoother of the level, -1 when it is solved in one direct / cluster launch
+  float* f_g[3] = {nullptr, nullptr, nullptr};
+  float* u_g[3] = {nullptr, nullptr, nullptr};
+  int n_cells(void) const { return cellReso[0] * cellReso[1] * cellReso[2]; }
+  std::string getName(void) const {
+    return "Grid_" + std::to_string(cellReso[0]) + "x" + std::to_string(cellReso[1]) + "x" +
+           std::to_string(cellReso[2]);
+  }
+  float* getDisplacement(void) { return u_g[0]; }
+};
+
+// MG_H (homogenization/MG.h:14-32) as a view of a Homogenization_H, whose handle holds the
+// hierarchy.
 struct MG_H {
-  explicit MG_H(Homogenization_H& hom) : hom_(hom) {}
+  explicit MG_H(Homogenization_H& hom) : hom_(hom) { sync_grids(); }
+  MG_H(const MG_H&) = delete;
+  MG_H& operator=(const MG_H&) = delete;
+  ~MG_H() { free_root(); }
+
+  std::vector<std::shared_ptr<Grid_H>> grids;  // fine to coarse
+  MGConfig mgConfig;
+
+  std::shared_ptr<Grid_H> getRootGrid(void) { return grids.empty() ? nullptr : grids[0]; }
+
+  // build(MGConfig) (MG.cpp:13-44): rebuild the hierarchy for the configuration's resolution.
+  void build(MGConfig config) {
+    mgConfig = config;
+    cfg::HomoConfig hc = hom_.config;
+    for (int i = 0; i < 3; i++) hc.reso[i] = config.reso[i];
+    hom_.build(hc, hom_.options());
+    sync_grids();
+  }
+
+  // v_cycle(w_SOR, pre, post) (MG.cpp:46-71): one V-cycle on the root grid's f_g, correction into
+  // its u_g. Needs the hierarchy's operators, i.e. a Homogenization_H::update() first.
+  void v_cycle(float w_SOR = 1.f, int pre = 1, int post = 1) {
+    if (w_SOR != 1.f) throw Error(OTM_ERR_UNSUPPORTED, "MG_H::v_cycle: the smoother is Gauss-Seidel (w_SOR = 1)");
+    check(otm_homo_v_cycle(hom_.handle(), root_f_, root_u_, pre, post), "MG_H::v_cycle");
+    cudaDeviceSynchronize();
+  }
+
   // solveEquation(tol, with_guess) (MG.cpp:80-142): solves all 3 load cases, returns the
   // largest relative residual.
   double solveEquation(double tol = 1e-2, bool with_guess = true) {
@@ -181,7 +244,180 @@ struct MG_H {
   void updateStencils() { hom_.update(); }
 
  private:
+  void free_root() {
+    if (root_f_) cudaFree(root_f_);
+    if (root_u_) cudaFree(root_u_);
+    root_f_ = root_u_ = nullptr;
+  }
+  void sync_grids() {
+    grids.clear();
+    free_root();
+    otm_level_info info;
+    check(otm_homo_level(hom_.handle(), 0, &info), "MG_H::grids");
+    for (int l = 0; l < info.levels; l++) {
+      otm_level_info li;
+      check(otm_homo_level(hom_.handle(), l, &li), "MG_H::grids");
+      auto g = std::make_shared<Grid_H>();
+      g->is_root = (l == 0);
+      g->assemb_otf = !li.stencil;
+      g->cellReso = {li.reso[0], li.reso[1], li.reso[2]};
+      g->smoother = li.smoother;
+      grids.push_back(g);
+    }
+    for (size_t l = 0; l < grids.size(); l++) {
+      if (l > 0) grids[l]->fine = grids[l - 1].get();
+      if (l + 1 < grids.size()) grids[l]->Coarse = grids[l + 1].get();
+    }
+    const size_t nv = size_t(grids[0]->n_cells());
+    if (cudaMalloc(&root_f_, 3 * nv * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&root_u_, 3 * nv * sizeof(float)) != cudaSuccess)
+      throw Error(OTM_ERR_OUT_OF_MEMORY, "MG_H: root grid vectors");
+    cudaMemset(root_f_, 0, 3 * nv * sizeof(float));
+    cudaMemset(root_u_, 0, 3 * nv * sizeof(float));
+    for (int c = 0; c < 3; c++) {
+      grids[0]->f_g[c] = root_f_ + c * nv;
+      grids[0]->u_g[c] = root_u_ + c * nv;
+    }
+  }
   Homogenization_H& hom_;
+  float* root_f_ = nullptr;
+  float* root_u_ = nullptr;
+};
+
+// The density expression of runCustom (Framework.cu:163): rho.conv(ker).pow(p) * (k0 - kmin) + kmin
+// (the filter of AutoDiff/TensorExpression.h:1095-1185, pow_umker_t :816-843, the affine map), as
+// a value type with the interface heat_tensor_t uses: eval(), value(), diff(), backward(diff()).
+// rho is the caller's device field (x fastest, element (x,y,z) at x + (y + z*ny)*rho_pitchT);
+// grad() receives d objective / d rho after backward(), with the same pitch.
+struct DensityChain {
+  struct View {
+    int pitchT;
+    int getPitchT() const { return pitchT; }
+  };
+  struct TensorRef {
+    float* ptr;
+    int pitchT;
+    float* data() const { return ptr; }
+    View view() const { return View{pitchT}; }
+  };
+
+  DensityChain(const int reso[3], float* rho, int rho_pitchT, float* grad_rho, float radius = 2.f,
+               int weight = OTM_WEIGHT_LINEAR, bool periodic = true, float p = 3.f, float k0 = 1.f, float kmin = 1e-3f)
+      : rho_(rho), grad_(grad_rho), pitch_(rho_pitchT > 0 ? rho_pitchT : reso[0]), radius_(radius), weight_(weight),
+        periodic_(periodic), p_(p), k0_(k0), kmin_(kmin) {
+    for (int i = 0; i < 3; i++) reso_[i] = reso[i];
+    const size_t ne = size_t(reso[0]) * reso[1] * reso[2];
+    float* bufs[5];
+    for (auto& b : bufs)
+      if (cudaMalloc(&b, ne * sizeof(float)) != cudaSuccess) throw Error(OTM_ERR_OUT_OF_MEMORY, "DensityChain");
+    rho_f_ = bufs[0], k_ = bufs[1], dk_ = bufs[2], wsum_ = bufs[3], diff_ = bufs[4];
+  }
+  DensityChain(const DensityChain&) = delete;
+  DensityChain& operator=(const DensityChain&) = delete;
+  ~DensityChain() {
+    for (float* b : {rho_f_, k_, dk_, wsum_, diff_}) cudaFree(b);
+  }
+
+  void eval() {
+    check(otm_density_forward(reso_, rho_, pitch_, rho_f_, k_, dk_, wsum_, weight_, radius_, periodic_ ? 1 : 0, p_,
+                              k0_, kmin_, nullptr),
+          "DensityChain::eval");
+  }
+  TensorRef value() { return TensorRef{k_, reso_[0]}; }  // the conductivity field k
+  TensorRef diff() { return TensorRef{diff_, reso_[0]}; }  // d objective / d k (written by Sensitivity)
+  // chain rule back to rho: grad = filter^T(diff * dk/drho_f)
+  void backward(TensorRef g) {
+    check(otm_density_backward(reso_, g.data(), dk_, wsum_, grad_, pitch_, weight_, radius_, periodic_ ? 1 : 0,
+                               nullptr),
+          "DensityChain::backward");
+  }
+  float* grad() { return grad_; }
+
+ private:
+  int reso_[3];
+  float* rho_;
+  float* grad_;
+  int pitch_;
+  float radius_;
+  int weight_;
+  bool periodic_;
+  float p_, k0_, kmin_;
+  float *rho_f_ = nullptr, *k_ = nullptr, *dk_ = nullptr, *wsum_ = nullptr, *diff_ = nullptr;
+};
+
+// Reference counting of the expression graph (each user's eval counts once; backward runs when
+// every user has propagated its gradient).
+struct RefCounter {
+  int n_eval = 0, n_backward = 0;
+  void c_eval() { n_eval++; }
+  void c_backward() { n_backward++; }
+  bool finishedBackward() const { return n_backward >= n_eval; }
+  void reset() { n_eval = n_backward = 0; }
+};
+
+// heat_tensor_t (homogenization/homoExpression.h:69-150): eval() evaluates the density expression,
+// updates the homogenization domain with it and stores K^H in H_; the caller writes the gradient
+// of its objective with respect to K^H into gradH_ (the reference's scalar autodiff does that
+// through operator()(i, j)); backward() turns it into the element sensitivity (Sensitivity,
+// pitched lexicographic) and back-propagates it through the density expression.
+template <typename Scalar, typename DensityExp_t>
+struct heat_tensor_t {
+  Scalar H_[3][3] = {};
+  Scalar gradH_[3][3] = {};
+  DensityExp_t& densityField;
+  RefCounter counter;
+  Homogenization_H& domain_;
+  bool hold_on = false;
+  bool expired = true;
+
+  heat_tensor_t(Homogenization_H& dom, DensityExp_t& rho) : densityField(rho), domain_(dom), expired(true) {}
+
+  Scalar& value(int i, int j) { return H_[i][j]; }
+  Scalar& grad(int i, int j) { return gradH_[i][j]; }
+  void reset(void) { counter.reset(); }
+  void holdOn(void) { hold_on = true; }
+  void holdOff(void) { hold_on = false; }
+
+  void eval(void) {
+    counter.c_eval();
+    if (expired && !hold_on) {
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) gradH_[i][j] = 0;
+      densityField.eval();
+      domain_.update(densityField.value().data(), densityField.value().view().getPitchT());
+      domain_.heatMatrix(H_);
+      expired = false;
+    }
+    if (hold_on)
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) gradH_[i][j] = 0;
+  }
+
+  void backward() {
+    counter.c_backward();
+    if (counter.finishedBackward() && (!expired || hold_on)) {
+      expired = true;
+      counter.reset();
+      float g[3][3];
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) g[i][j] = float(gradH_[i][j]);
+      domain_.Sensitivity(g, densityField.diff().data(), densityField.diff().view().getPitchT(), true);
+      densityField.backward(densityField.diff());
+    }
+  }
+
+  void writeTo(const std::string& filename) {
+    std::ofstream ofs(filename, std::ios::binary);
+    ofs.write((const char*)(&H_[0][0]), sizeof(H_));
+  }
+  void writeToTxt(const std::string& filename) {
+    std::ofstream ofs(filename);
+    for (int i = 0; i < 3; i++) {
+      for (int j = 0; j < 3; j++) ofs << H_[i][j] << "  ";
+      ofs << "\n";
+    }
+  }
+  const Scalar* data(void) { return &H_[0][0]; }
 };
 
 struct OCOptimizer {

@@ -207,6 +207,23 @@ class Homogenization_H:
         check(lib().otm_homo_element_energy(self._h, ctypes.c_void_p(_ptr(out))), "otm_homo_element_energy")
         return out
 
+    def v_cycle(self, f, u=None, pre: int = 1, post: int = 1):
+        """MG_H::v_cycle (homogenization/MG.cpp:46-71): one V(pre, post) cycle of the handle's
+        hierarchy on the right-hand sides f (3, nz, ny, nx) from a zero correction -> u."""
+        import torch
+        if u is None:
+            u = torch.empty_like(f)
+        self._sync_stream()
+        check(lib().otm_homo_v_cycle(self._h, ctypes.c_void_p(_ptr(f)), ctypes.c_void_p(_ptr(u)), int(pre), int(post)),
+              "otm_homo_v_cycle")
+        return u
+
+    def level(self, level: int) -> _lib.LevelInfo:
+        """Grid_H of one level (homogenization/grid.h:104-421): sizes, stencil or matrix-free, smoother."""
+        info = _lib.LevelInfo()
+        check(lib().otm_homo_level(self._h, int(level), ctypes.byref(info)), "otm_homo_level")
+        return info
+
     def solution(self, lcase: int, out=None):
         import torch
         nx, ny, nz = self.reso

@@ -57,6 +57,11 @@ class Config(ctypes.Structure):
     ]
 
 
+class LevelInfo(ctypes.Structure):
+    _fields_ = [("levels", ctypes.c_int), ("reso", ctypes.c_int * 3), ("stencil", ctypes.c_int),
+                ("smoother", ctypes.c_int)]
+
+
 class SolveStats(ctypes.Structure):
     _fields_ = [
         ("iterations", ctypes.c_int),
@@ -140,6 +145,8 @@ SIGNATURES = {
     "otm_homo_sensitivity": (_S, [_P, _F, _P, ctypes.c_int, ctypes.c_int]),
     "otm_homo_element_energy": (_S, [_P, _P]),
     "otm_homo_get_solution": (_S, [_P, ctypes.c_int, _P]),
+    "otm_homo_v_cycle": (_S, [_P, _P, _P, ctypes.c_int, ctypes.c_int]),
+    "otm_homo_level": (_S, [_P, ctypes.c_int, ctypes.POINTER(LevelInfo)]),
     "otm_homo_set_solution": (_S, [_P, ctypes.c_int, _P]),
     "otm_homo_reset_displacement": (_S, [_P]),
     "otm_homo_get_stats": (_S, [_P, ctypes.POINTER(SolveStats)]),

@@ -567,6 +567,8 @@ void Homo::vcycle(int l) {
     ClDesc cd = cl_desc;
     cd.f_in = L.f;
     cd.u_out = L.u;
+    cd.pre = cfg.pre_smooth;
+    cd.post = cfg.post_smooth;
     launch_pdl(k_vcycle_cluster, dim3(kCl), dim3(kClThreads), cluster_smem, stream, cd, sc);
     launched(1);
     return;
@@ -1124,6 +1126,38 @@ otm_status Homo::solve_impl(bool with_heat) {
   return st;
 }
 
+// One V(pre, post) cycle on caller-given right-hand sides (MG_H::v_cycle, MG.cpp:46-71), with
+// direct launches: the right-hand sides go into the fine level's f, the cycle runs from a zero
+// correction with the handle's smoother, the correction is copied out. The cycle's kernels skip
+// their work once a solve has set the done flag, so it is cleared first.
+otm_status Homo::v_cycle_once(const float* f, float* u, int pre, int post) {
+  if (mixed) {
+    set_error("a single V-cycle is available in the FP32 form only");
+    return OTM_ERR_UNSUPPORTED;
+  }
+  if (!updated) {
+    set_error("update() must be called before a V-cycle");
+    return OTM_ERR_STATE;
+  }
+  if (pre < 0 || post < 0 || pre + post == 0 || pre > 16 || post > 16) return invalid("need 1..16 smoothing sweeps");
+  if (tiled && (pre == 0 || post == 0)) return invalid("the tiled smoother needs at least one sweep in each leg");
+  const size_t nv = lv[0].d.nv();
+  OTM_TRY(enter());
+  OTM_TRY(join_coarse());
+  OTM_CUDA(cudaMemcpyAsync(lv[0].f, f, 3 * nv * sizeof(float), cudaMemcpyDeviceToDevice, stream));
+  OTM_CUDA(cudaMemsetAsync(&sc->done, 0, sizeof(int), stream));
+  const int keep_pre = cfg.pre_smooth, keep_post = cfg.post_smooth;
+  cfg.pre_smooth = pre;
+  cfg.post_smooth = post;
+  prof_slot = -1;
+  vcycle(0);
+  cfg.pre_smooth = keep_pre;
+  cfg.post_smooth = keep_post;
+  OTM_CHECK_LAUNCH("v_cycle");
+  OTM_CUDA(cudaMemcpyAsync(u, fine_z(), 3 * nv * sizeof(float), cudaMemcpyDeviceToDevice, stream));
+  return leave();
+}
+
 otm_status Homo::solve(otm_solve_stats* out) {
   if (!updated) {
     set_error("update() must be called before solving");
@@ -1333,6 +1367,33 @@ otm_status otm_homo_sensitivity(otm_homo* h, const float dC[9], float* sens_dev,
 otm_status otm_homo_element_energy(otm_homo* h, float* energy_dev) {
   if (!h) return OTM_ERR_INVALID_ARGUMENT;
   return h->impl.element_energy(energy_dev);
+}
+
+otm_status otm_homo_v_cycle(otm_homo* h, const float* f_dev, float* u_dev, int pre, int post) {
+  if (!h || !f_dev || !u_dev) return OTM_ERR_INVALID_ARGUMENT;
+  return h->impl.v_cycle_once(f_dev, u_dev, pre, post);
+}
+
+otm_status otm_homo_level(const otm_homo* h, int level, otm_level_info* info) {
+  if (!h || !info) return OTM_ERR_INVALID_ARGUMENT;
+  const Homo& H = h->impl;
+  const int L = int(H.lv.size());
+  if (level < 0 || level >= L) return OTM_ERR_INVALID_ARGUMENT;
+  const otm::Level& lv = H.lv[level];
+  info->levels = L;
+  info->reso[0] = lv.d.nx;
+  info->reso[1] = lv.d.ny;
+  info->reso[2] = lv.d.nz;
+  info->stencil = level > 0 || L == 1;
+  const bool direct = level == L - 1 || (H.cluster_l >= 0 && level >= H.cluster_l) ||
+                      (H.tail_l >= 0 && level >= H.tail_l);
+  if (direct)
+    info->smoother = -1;
+  else if (level == 0)
+    info->smoother = H.tiled ? OTM_SMOOTHER_TILED : OTM_SMOOTHER_COLOR;
+  else
+    info->smoother = lv.ctiled ? OTM_SMOOTHER_TILED : OTM_SMOOTHER_COLOR;
+  return OTM_OK;
 }
 
 otm_status otm_homo_get_solution(otm_homo* h, int lcase, float* dst_dev) {

@@ -146,6 +146,7 @@ struct Homo {
   otm_status heat_matrix(double C[9], bool do_solve);
   otm_status sensitivity(const float dC[9], float* sens, int pitchT, int lexi);
   otm_status element_energy(float* out);
+  otm_status v_cycle_once(const float* f, float* u, int pre, int post);
 };
 
 }  // namespace otm

@@ -1,7 +1,8 @@
 // Drop-in check of the C++ wrapper: the reference's call sequence (Homogenization_H::update,
 // heatMatrix, Sensitivity; OCOptimizer::filterSens/update; MMAOptimizer::update; mmasubDevice)
 // compiled unchanged against include/otm/homogenization.hpp, then runCustom / ConvergeChecker /
-// VolumeGovernor of the driver layer. Prints K^H and checksums; the
+// VolumeGovernor of the driver layer, heat_tensor_t's eval / backward over the density chain, and
+// MG_H's grids and v_cycle. Prints K^H and checksums; the
 // pytest driver compares them with the Python path.
 #include <cmath>
 #include <cstdio>
@@ -116,6 +117,45 @@ int main() {
     VolumeGovernor vg;
     vg.volume_check(-1e-3f, 0.25f, 0.5f, 0);
     std::printf("governor %.7f %d\n", vg.get_volume_bound(), int(cc.is_converge(0, 1.0)));
+  }
+  // heat_tensor_t over the density chain of runCustom (homoExpression.h:69-150), used as a design
+  // step uses it: eval() gives K^H, the objective's gradient goes into gradH_, backward() gives
+  // d objective / d rho
+  {
+    const int reso[3] = {n, n, n};
+    std::vector<float> hr(ne);
+    for (int e = 0; e < ne; e++) hr[e] = u01(5 * ne + e);
+    float *rho_e = nullptr, *grad_e = nullptr;
+    cudaMalloc(&rho_e, ne * sizeof(float));
+    cudaMalloc(&grad_e, ne * sizeof(float));
+    cudaMemcpy(rho_e, hr.data(), ne * sizeof(float), cudaMemcpyHostToDevice);
+    homo::Homogenization_H hom2(config, opt);
+    homo::DensityChain dens(reso, rho_e, n, grad_e);
+    homo::heat_tensor_t<float, homo::DensityChain> Hh(hom2, dens);
+    Hh.eval();
+    for (int i = 0; i < 3; i++) Hh.gradH_[i][i] = -1.f;  // objective -trace(K^H)
+    Hh.backward();
+    std::vector<float> g(ne);
+    cudaMemcpy(g.data(), dens.grad(), ne * sizeof(float), cudaMemcpyDeviceToHost);
+    double gs = 0;
+    for (float v : g) gs += v;
+    std::printf("ht_C %.9e %.9e %.9e %.9e %.9e %.9e\n", Hh.H_[0][0], Hh.H_[0][1], Hh.H_[0][2], Hh.H_[1][1],
+                Hh.H_[1][2], Hh.H_[2][2]);
+    std::printf("ht_grad_sum %.9e\n", gs);
+    // MG_H: the grids and one V(2,2) cycle on the root grid's right-hand sides
+    homo::MG_H mg2(hom2);
+    auto root = mg2.getRootGrid();
+    std::printf("mg_levels %d %d %d\n", int(mg2.grids.size()), root->cellReso[0], int(root->Coarse != nullptr));
+    std::vector<float> fr(3 * size_t(ne));
+    for (int i = 0; i < 3 * ne; i++) fr[i] = u01(7 * ne + i) - 0.5f;
+    cudaMemcpy(root->f_g[0], fr.data(), fr.size() * sizeof(float), cudaMemcpyHostToDevice);
+    mg2.v_cycle(1.f, 2, 2);
+    cudaMemcpy(fr.data(), root->u_g[0], fr.size() * sizeof(float), cudaMemcpyDeviceToHost);
+    double un = 0;
+    for (float v : fr) un += double(v) * v;
+    std::printf("vc_norm %.9e\n", std::sqrt(un));
+    cudaFree(rho_e);
+    cudaFree(grad_e);
   }
   std::printf("ok\n");
   return 0;

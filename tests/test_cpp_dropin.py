@@ -62,3 +62,23 @@ def test_dropin_program_matches_python_path(tmp_path):
     rho, _ = run_custom(DesignConfig(reso=16, max_iter=2, heatRatio=(1.0, 1e-4), winit=InitWay.IWP, model=Model.oc))
     assert vals["design_sum"][0] == pytest.approx(float(rho.astype(np.float64).sum()), rel=1e-9)
     assert vals["governor"] == [pytest.approx(0.25, abs=1e-7), 0.0]
+    # heat_tensor_t eval / backward = density filter -> update -> heatMatrix -> Sensitivity -> filter
+    # adjoint through the Python path on the same density (the same library calls)
+    from opentm_b200 import DensityFilter
+    rho_h = wl.uniform(0, 6 * n3)[5 * n3:].astype(np.float32).reshape(n, n, n)
+    df = DensityFilter((n, n, n), 2.0, 1, True, 3.0, 1.0, 1e-3)
+    H2 = Homogenization_H(HomoConfig(reso=n, femRelThres=1e-6, pre_smooth=2, post_smooth=2))
+    H2.update(df.forward(torch.from_numpy(rho_h).cuda()))
+    C2 = H2.heatMatrix()
+    g_k = torch.empty((n, n, n), dtype=torch.float32, device="cuda")
+    H2.Sensitivity(-np.eye(3), g_k)
+    g_rho = df.backward(g_k)
+    want = [C2[0, 0], C2[0, 1], C2[0, 2], C2[1, 1], C2[1, 2], C2[2, 2]]
+    assert np.allclose(vals["ht_C"], want, rtol=1e-7, atol=1e-12)
+    assert vals["ht_grad_sum"][0] == pytest.approx(float(g_rho.double().sum()), rel=1e-6)
+    # MG_H: one V(2,2) cycle on the same right-hand sides
+    lv = [H2.level(l) for l in range(H2.level(0).levels)]
+    assert vals["mg_levels"] == [len(lv), n, 1.0]
+    f = (wl.uniform(0, 10 * n3)[7 * n3:].astype(np.float32) - np.float32(0.5)).reshape(3, n, n, n)
+    u = H2.v_cycle(torch.from_numpy(f).cuda(), pre=2, post=2)
+    assert vals["vc_norm"][0] == pytest.approx(float(u.double().norm()), rel=1e-6)

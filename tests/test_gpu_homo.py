@@ -5,6 +5,7 @@ import numpy as np
 import pytest
 
 import oracle as ora
+from opentm_b200 import workloads as wl
 from tests.helpers import (DC_TEST, KH_TOL, SENS_TOL, oracle_solution, random_k, rel_c, rel_diag, rel_entries,
                            rel_field)
 
@@ -317,3 +318,25 @@ def test_tiled_graphs_and_repeat_bitwise():
     _, C3, E3, s3 = gpu_run(k, use_graphs=True, smoother="tiled")
     assert np.array_equal(C1, C2) and np.array_equal(E1, E2) and np.array_equal(s1, s2)
     assert np.array_equal(C1, C3) and np.array_equal(s1, s3)
+
+
+@pytest.mark.parametrize("smoother", ["tiled", "color"])
+def test_single_v_cycle_reduces_the_residual(smoother):
+    """MG_H::v_cycle through otm_homo_v_cycle: one V(2,2) cycle from a zero correction on random
+    mean-free right-hand sides leaves a residual f - A u (FP64 operator of the oracle) of at most a
+    third of f, for both fine smoothers; the level description names the smoother."""
+    from opentm_b200 import HomoConfig, Homogenization_H
+    n = 32
+    k = (0.5 + 0.5 * wl.uniform(81, n ** 3)).astype(np.float32).reshape(n, n, n)
+    H = Homogenization_H(HomoConfig(reso=n, femRelThres=1e-6, pre_smooth=2, post_smooth=2, smoother=smoother))
+    H.update(torch.from_numpy(k).cuda())
+    f = np.random.default_rng(1).standard_normal((3, n, n, n)).astype(np.float32)
+    f -= f.mean(axis=(1, 2, 3), keepdims=True)
+    u = H.v_cycle(torch.from_numpy(f).cuda(), pre=2, post=2).cpu().numpy().astype(np.float64)
+    ks = 1e-9 + k.astype(np.float64)
+    for c in range(3):
+        r = f[c] - ora.apply(ks, u[c])
+        assert np.linalg.norm(r) <= np.linalg.norm(f[c]) / 3.0, (c, np.linalg.norm(r) / np.linalg.norm(f[c]))
+    info = H.level(0)
+    assert info.levels == H.stats().levels and list(info.reso) == [n, n, n] and info.stencil == 0
+    assert info.smoother == (1 if smoother == "tiled" else 0)
