@@ -146,7 +146,7 @@ def run_ours(args, rank, world, local_rank):
     def make(precision, profile=False):
         H = Homogenization_H(HomoConfig(reso=n, femRelThres=TOL, pre_smooth=2, post_smooth=2, max_iter=200,
                                         precision=precision, profile=profile, smoother=args.smoother,
-                                        cluster_cycle=bool(args.cluster_cycle)))
+                                        cluster_cycle=int(args.cluster_cycle)))
         df = DensityFilter((n, n, n), FILTER_R, 1, True, P_SIMP, K0, KMIN)
         oc = OCOptimizer(ne, 0.001, MOVE, DAMP)
         return H, df, oc
@@ -735,7 +735,7 @@ def main():
     ap.add_argument("--extra", type=int, default=1,
                     help="add the 32^3 and 256^3 solves and one serving rate to the default line (N = 1 only)")
     ap.add_argument("--cluster-cycle", type=int, default=1,
-                    help="run the levels with <= 32^3 unknowns as one thread-block-cluster launch (1) or not (0)")
+                    help="lower levels as one thread-block-cluster launch: automatic (1), from 16^3 (2), from 32^3 (3), off (0)")
     ap.add_argument("--smoother", default="tiled", choices=["tiled", "color"],
                     help="fine-level smoother: shared-memory tiles (default) or global colour-pair passes")
     args = ap.parse_args()

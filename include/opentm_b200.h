@@ -82,8 +82,10 @@ typedef struct otm_config {
   int use_graphs;        /* capture the iteration loop in a CUDA graph; default 1 */
   int profile;           /* time the first fine-level post-smoothing sweep of every iteration with CUDA
                             events recorded inside the graph; default 0 */
-  int cluster_cycle;     /* run the levels with <= 32^3 unknowns and the coarsest solve in one
-                            thread-block-cluster launch when they fit; default 1 */
+  int cluster_cycle;     /* run the lower levels and the coarsest solve in one thread-block-cluster
+                            launch when they fit, from the first level with <= 16^3 unknowns (2) or
+                            <= 32^3 (3); 1: 16^3 when the level above it is tile-smoothed, else
+                            32^3; 0: per-level kernels only; default 1 */
   int smoother;          /* otm_smoother of the fine level; default OTM_SMOOTHER_TILED */
 } otm_config;
 

@@ -113,7 +113,7 @@ class HomoConfig:
     check_every: int = 4
     use_graphs: bool = True
     profile: bool = False
-    cluster_cycle: bool = True
+    cluster_cycle: int = 1  # 0 off, 1 automatic, 2 from 16^3, 3 from 32^3
     smoother: str = "tiled"
 
     def to_c(self) -> _lib.Config:
@@ -124,7 +124,7 @@ class HomoConfig:
             precision=self.precision, coarsest_max_dof=int(self.coarsest_max_dof),
             power_penal=float(self.power_penal), warm_start=int(bool(self.warm_start)),
             check_every=int(self.check_every), use_graphs=int(bool(self.use_graphs)),
-            profile=int(bool(self.profile)), cluster_cycle=int(bool(self.cluster_cycle)),
+            profile=int(bool(self.profile)), cluster_cycle=int(self.cluster_cycle),
             smoother=self.smoother)
 
 

@@ -3,13 +3,16 @@
 // The levels with at most kClMaxNv unknowns, down to and including the coarsest direct solve,
 // run in kCl CTAs of one cluster. Every level is split into slabs of z-planes, one slab per
 // CTA; each CTA keeps u of its planes plus ghost copies of the two neighbouring planes, and f,
-// r and the 27-point stencils of its planes (the first level's stencils, right-hand side and
-// residual stay in global memory, L2-resident), in its own shared memory. A CTA that writes
+// r and the 27-point stencils of its planes (a first level too large for that keeps its stencils,
+// right-hand side and residual in global memory, L2-resident), in its own shared memory. A CTA that writes
 // an edge plane of u also stores the values into its neighbours' ghost copies (distributed
 // shared memory), so colour passes and residuals read only local shared memory; restriction,
 // prolongation and the coarsest gather read other CTAs' planes directly. The phases are
 // separated by cluster barriers (barrier.cluster arrive/wait, release/acquire) instead of
-// kernel boundaries, so the whole lower cycle costs one launch. The arithmetic is that of the
+// kernel boundaries, so the whole lower cycle costs one launch. A cluster barrier costs about
+// as much as a small level's colour pass, so a sweep takes two: colours 0-3 update only the
+// even planes and colours 4-7 only the odd ones, and within each half a vertex's changing
+// neighbours lie in its own plane, held by its own CTA (CTA barriers between those passes). The arithmetic is that of the
 // per-level kernels in otm_mg_kernels.cuh except for the summation order of the 27-point
 // products; the coarsest solve is u = Ainv (f - mean f) as in k_coarsest_solve.
 #pragma once
@@ -36,7 +39,7 @@ struct ClLevel {
   int ups;     // u plane stride (ny * urs, padded)
   int ucs;     // u case stride: two more planes (ghost copies of the neighbouring slabs' edge planes)
   int u_off;   // float offsets in shared memory
-  int f_off;   // < 0: right-hand side read from f_in (global; first level only)
+  int f_off;   // < 0: right-hand side read from f_in (global; first level only, when not staged)
   int r_off;   // < 0: residual in rg (global, lexicographic, case-major)
   int st_off;  // < 0: stencils read from st (global, colour-blocked); else [vertex][27]
   int inv_off; // inverse diagonal per own vertex (with st_off >= 0)
@@ -388,6 +391,20 @@ __device__ __forceinline__ void cl_prolong(const ClLevel& F, const ClLevel& C, f
   }
 }
 
+// One colour pass (cl_gs) followed by the barrier that its successor in the sweep needs:
+// colours 0-3 update the even planes, 4-7 the odd ones, and a pass's changing neighbours are in
+// its own plane unless it ends a half (colour 3 or 4 last, going up or down), after which the
+// neighbouring CTAs' planes must be visible.
+template <typename Cluster>
+__device__ __forceinline__ void cl_gs_sync(const ClLevel& L, const float* f_glob, float* sm, const int* tab,
+                                           float* const* rb, int rank, int color, bool half_end, Cluster& cluster) {
+  cl_gs(L, f_glob, sm, tab, rb, rank, color);
+  if (half_end)
+    cluster.sync();
+  else
+    __syncthreads();
+}
+
 static __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads)
     k_vcycle_cluster(ClDesc cdp, const SolveScalars* sc) {
   pdl_wait();
@@ -407,7 +424,8 @@ static __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads)
   __syncthreads();
   cooperative_groups::cluster_group cluster = cooperative_groups::this_cluster();
   const int rank = int(cluster.block_rank());
-  if (threadIdx.x < kCl) rb[threadIdx.x] = cluster.map_shared_rank(sm, int(threadIdx.x));
+  // other CTAs' shared memory through the cluster window, this CTA's own directly
+  if (threadIdx.x < kCl) rb[threadIdx.x] = int(threadIdx.x) == rank ? sm : cluster.map_shared_rank(sm, int(threadIdx.x));
   int* tab = reinterpret_cast<int*>(sm + cd.tab_base);
   const int L = cd.nlev;
   // plane tables: owner and local plane of every plane; the ghost copies every plane feeds
@@ -429,30 +447,49 @@ static __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads)
       }
     }
   }
-  // first level: zero correction (ghosts included); stencils of the other smoothed levels
+  // the coarsest inverse is read once, late in the cycle: bring it into L2 now
+  l2_prefetch_share(cd.Ainv, size_t(cd.nc) * size_t(cd.nc) * sizeof(double));
+  // first level: zero correction (ghosts included) and, where it is staged, its right-hand side;
+  // stencils of the other smoothed levels. One thread per own vertex, all of its loads in flight
+  // before its stores (a copy of one element per round trip made this a chain of L2 latencies).
   cl_zero_u(cd.lv[0], sm, rank);
+  if (cd.lv[0].f_off >= 0) {
+    const ClLevel& V = cd.lv[0];
+    const int pl = V.d.nx * V.d.ny, z0 = V.zstart[rank];
+    const int n = (V.zstart[rank + 1] - z0) * pl;
+    const size_t nv = V.d.nv();
+    const float* fz = cd.f_in + size_t(z0) * pl;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+      float v[3];
+#pragma unroll
+      for (int c = 0; c < 3; c++) v[c] = __ldg(fz + c * nv + t);
+#pragma unroll
+      for (int c = 0; c < 3; c++) sm[V.f_off + c * V.cs + t] = v[c];
+    }
+  }
   for (int l = 0; l < L - 1; l++) {
     const ClLevel& V = cd.lv[l];
     if (V.st_off < 0) continue;
     const int nx = V.d.nx, pl = nx * V.d.ny, z0 = V.zstart[rank];
     const int n = (V.zstart[rank + 1] - z0) * pl;
     const size_t nv = V.d.nv();
-    for (int idx = threadIdx.x; idx < 27 * n; idx += blockDim.x) {
-      const int o = idx / n, t = idx - o * n;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
       const int zl = t / pl, rem = t - zl * pl, y = rem / nx, x = rem - y * nx;
-      const float a = __ldg(V.st + size_t(o) * nv + cb_index(V.d, x, y, z0 + zl));
-      sm[V.st_off + t * 27 + o] = a;
-      if (o == 13) sm[V.inv_off + t] = 1.0f / a;
+      const float* src = V.st + cb_index(V.d, x, y, z0 + zl);
+      float a[27];
+#pragma unroll
+      for (int o = 0; o < 27; o++) a[o] = __ldg(src + size_t(o) * nv);
+      float* dst = sm + V.st_off + t * 27;
+#pragma unroll
+      for (int o = 0; o < 27; o++) dst[o] = a[o];
+      sm[V.inv_off + t] = 1.0f / a[13];
     }
   }
   cluster.sync();
   for (int l = 0; l < L - 1; l++) {
     const ClLevel& F = cd.lv[l];
     for (int s = 0; s < cd.pre; s++)
-      for (int c = 0; c < 8; c++) {
-        cl_gs(F, cd.f_in, sm, tab, rb, rank, c);
-        cluster.sync();
-      }
+      for (int c = 0; c < 8; c++) cl_gs_sync(F, cd.f_in, sm, tab, rb, rank, c, c == 3 || c == 7, cluster);
     cl_resid(F, cd.f_in, sm, rank);
     cluster.sync();
     cl_restrict(F, cd.lv[l + 1], sm, tab, rb, rank);
@@ -465,10 +502,7 @@ static __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads)
     cl_prolong(F, cd.lv[l + 1], sm, tab, rb, rank);
     cluster.sync();
     for (int s = 0; s < cd.post; s++)
-      for (int c = 7; c >= 0; c--) {
-        cl_gs(F, cd.f_in, sm, tab, rb, rank, c);
-        cluster.sync();
-      }
+      for (int c = 7; c >= 0; c--) cl_gs_sync(F, cd.f_in, sm, tab, rb, rank, c, c == 4 || c == 0, cluster);
   }
   // no distributed access after the last barrier: write this CTA's planes of the correction
   {
@@ -519,7 +553,7 @@ inline int cl_log2_ceil(int v) {
   return l;
 }
 
-// first_smem: the first level's stencils and residual also live in shared memory.
+// first_smem: the first level's stencils, right-hand side and residual also live in shared memory.
 inline size_t cl_plan_try(const Dims* dims, int n, ClDesc* cd, bool first_smem) {
   if (n < 2 || n > kClMaxLevels) return 0;
   if (dims[0].nv() > size_t(kClMaxNv)) return 0;
@@ -557,8 +591,8 @@ inline size_t cl_plan_try(const Dims* dims, int n, ClDesc* cd, bool first_smem) 
     V.ucs = (maxpl + 2) * V.ups;
     V.u_off = off;
     off += 3 * V.ucs;
-    V.f_off = -1;  // the first level reads its right-hand side from global memory
-    if (l > 0) {
+    V.f_off = -1;  // the first level reads its right-hand side from global memory unless staged
+    if (l > 0 || smem_st) {
       V.f_off = off;
       off += 3 * V.cs;
     }

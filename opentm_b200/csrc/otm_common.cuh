@@ -57,6 +57,23 @@ struct Dims {
 // predecessor writes; for a launch without the attribute it returns at once.
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
+// This CTA's share of an L2 prefetch of [base, base + bytes) (base 16-byte aligned, or null for
+// none), issued by thread 0 as bulk prefetches of at most 32 KB (cp.async.bulk.prefetch.L2: a
+// hint that moves the lines into L2 through the copy engine and holds no registers or shared
+// memory). Used by a kernel to bring the data of the kernel after it into L2 while it runs.
+__device__ __forceinline__ void l2_prefetch_share(const void* base, size_t bytes) {
+  if (base == nullptr || threadIdx.x != 0) return;
+  const size_t per = ((bytes + gridDim.x - 1) / gridDim.x + 15) & ~size_t(15);
+  size_t lo = size_t(blockIdx.x) * per;
+  const size_t hi = lo + per < bytes ? lo + per : bytes;
+  for (; lo + 16 <= hi; lo += 32768) {
+    const size_t rest = hi - lo;
+    const unsigned n = unsigned(rest < 32768 ? rest : 32768) & ~15u;
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(static_cast<const char*>(base) + lo), "r"(n)
+                 : "memory");
+  }
+}
+
 // (x, y, z) of lexicographic index v (x fastest) on a grid with rows of nx and planes of
 // nx * ny points. Grids hold at most 1024^3 = 2^30 points, so 32-bit division is exact and
 // several times cheaper than 64-bit.

@@ -268,12 +268,25 @@ otm_status Homo::build(const otm_config& c, cudaStream_t ext_stream, cudaMemPool
       }
     }
   }
-  // levels with <= 32^3 unknowns and the coarsest solve in one thread-block-cluster launch
+  // the levels from the first with <= 32^3 unknowns (cluster_cycle 3) or <= 16^3 (cluster_cycle 2)
+  // and the coarsest solve in one thread-block-cluster launch; cluster_cycle 1 takes <= 16^3 when
+  // the level above that is smoothed by the coarse tile kernels (a sweep there is one launch, and
+  // the cluster's passes cost a cluster barrier per half sweep), else <= 32^3
   if (cfg.cluster_cycle) {
     const int L = int(lv.size());
+    size_t cl_max = cfg.cluster_cycle == 2 ? size_t(kClMaxNv / 8) : size_t(kClMaxNv);
+    if (cfg.cluster_cycle == 1) {
+      const bool ctiles = cfg.smoother == OTM_SMOOTHER_TILED && cfg.solver == OTM_SOLVER_PCG && cfg.pre_smooth > 0 &&
+                          cfg.post_smooth > 0;
+      for (int l = 2; l < L - 1; l++)
+        if (lv[l].d.nv() <= size_t(kClMaxNv / 8)) {
+          if (ctiles && lv[l - 1].d.nv() <= size_t(kClMaxNv) && ctile_fits(lv[l - 1].d)) cl_max = kClMaxNv / 8;
+          break;
+        }
+    }
     int t = -1;
     for (int l = 1; l < L - 1; l++)
-      if (lv[l].d.nv() <= size_t(kClMaxNv)) {
+      if (lv[l].d.nv() <= cl_max) {
         t = l;
         break;
       }
@@ -505,7 +518,8 @@ void Homo::fine_ops16(int what, int color) {
         k_resid_fine<false, 3, T, T><<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(L.d, kk, op0, u, L.f, r, sc, fs);
       break;
     case 2:
-      k_restrict<3, T><<<ceil_div(lv[1].d.nv(), kBlock), kBlock, 0, stream>>>(L.d, lv[1].d, r, lv[1].f, sc);
+      k_restrict<3, T><<<ceil_div(lv[1].d.nv(), kBlock), kBlock, 0, stream>>>(L.d, lv[1].d, r, lv[1].f, sc,
+                                                                            nullptr, size_t(0));
       break;
     case 4:  // zero fill + first colour-pair pass (paired colours only)
       k_gs_fine_pair_first<3, T, T><<<ceil_div(nv >> 3, kBlock), kBlock, 0, stream>>>(L.d, kk, op0, u, L.f, sc, fs);
@@ -654,7 +668,8 @@ void Homo::vcycle(int l) {
     } else {
       launch_pdl(k_resid_coarse<3>, dim3(ceil_div(nv, kBlock)), dim3(kBlock), 0, stream, L.d, L.st, L.u, L.f, L.r, sc);
     }
-    launch_pdl(k_restrict<3>, dim3(ceil_div(C.d.nv(), kBlock)), dim3(kBlock), 0, stream, L.d, C.d, L.r, C.f, sc);
+    launch_pdl(k_restrict<3>, dim3(ceil_div(C.d.nv(), kBlock)), dim3(kBlock), 0, stream, L.d, C.d, L.r, C.f, sc,
+               st_prefetch(l + 1), st_prefetch_bytes(l + 1));
     launched(2);  // residual + restriction
   }
   if (l == 0 && join_in_cycle) {
@@ -706,7 +721,7 @@ void Homo::vcycle_fine_tiled(const KT* k, VT* u, VT* r, const FineOp& fop, const
   launch_pdl(k_tile_resid<KT, VT>, dim3(nt), dim3(kResidThreads), kTileSmemResid, stream, fmap, L.d, k, fop,
              (const VT*)pre, r, fs, sc);
   launch_pdl(k_restrict<3, VT>, dim3(ceil_div(C.d.nv(), kBlock)), dim3(kBlock), 0, stream, L.d, C.d, (const VT*)r,
-             C.f, (const SolveScalars*)sc);
+             C.f, (const SolveScalars*)sc, st_prefetch(1), st_prefetch_bytes(1));
   launched(npre + 2);
   if (join_in_cycle) {
     // the coarse levels need the operators of the side stream's chain from here on
@@ -760,7 +775,7 @@ void Homo::vcycle_coarse_tiled(int l) {
   launch_pdl(k_resid_coarse<3>, dim3(ceil_div(L.d.nv(), kBlock)), dim3(kBlock), 0, stream, L.d, (const float*)L.st, pre,
              (const float*)L.f, L.r, (const SolveScalars*)sc);
   launch_pdl(k_restrict<3, float>, dim3(ceil_div(C.d.nv(), kBlock)), dim3(kBlock), 0, stream, L.d, C.d,
-             (const float*)L.r, C.f, (const SolveScalars*)sc);
+             (const float*)L.r, C.f, (const SolveScalars*)sc, st_prefetch(l + 1), st_prefetch_bytes(l + 1));
   launched(npre + 2);
   vcycle(l + 1);
   const float* pin = pre;

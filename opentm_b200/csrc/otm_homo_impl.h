@@ -129,6 +129,15 @@ struct Homo {
   void vcycle_fine_tiled(const KT* k, VT* u, VT* r, const FineOp& fop, const double* fs);
   // the fine level's V-cycle result (the preconditioned residual / correction)
   void* fine_z() const { return tiled ? (mixed ? r16 : (void*)lv[0].r) : (mixed ? u16 : (void*)lv[0].u); }
+  // the stencils of coarse level l for the L2 prefetch of the restriction into it: null while the
+  // side stream may still be writing them, on the coarsest level and for an unaligned buffer
+  const void* st_prefetch(int l) const {
+    if (coarse_pending || l <= 0 || l >= int(lv.size()) - 1 || !lv[l].st ||
+        (reinterpret_cast<uintptr_t>(lv[l].st) & 15))
+      return nullptr;
+    return lv[l].st;
+  }
+  size_t st_prefetch_bytes(int l) const { return st_prefetch(l) ? 27 * lv[l].d.nv() * sizeof(float) : 0; }
   template <typename VT>
   void pcg_direction(const VT* z, const float* r, bool face, int nb);
   void gs_first(int l);

@@ -548,9 +548,13 @@ __device__ __forceinline__ void restrict_body(const Dims& df, const Dims& dc, co
   for (int c = 0; c < NC; c++) fc[c * nvc + V] = acc[c];
 }
 
+// pf / pf_bytes: data of a later kernel to bring into L2 (the coarse level's stencils, which the
+// fine level's work evicts between two V-cycles), or null.
 template <int NC, typename VT = float>
 __global__ void __launch_bounds__(kBlock) k_restrict(Dims df, Dims dc, const VT* __restrict__ r,
-                                                      float* __restrict__ fc, const SolveScalars* sc) {
+                                                      float* __restrict__ fc, const SolveScalars* sc,
+                                                      const void* pf, size_t pf_bytes) {
+  l2_prefetch_share(pf, pf_bytes);  // data not written by the preceding kernels
   pdl_wait();
   if (sc && solve_done(sc)) return;
   restrict_body<NC, VT>(df, dc, r, fc, size_t(blockIdx.x) * blockDim.x + threadIdx.x);

@@ -258,6 +258,23 @@ def test_cluster_cycle_matches_per_level_kernels(shape):
     check_against_oracle(k, C1, E1, s1)
 
 
+@pytest.mark.parametrize("shape,auto_level", [((64, 64, 64), 2), ((48, 48, 48), 1)])
+def test_cluster_from_16_cubed(shape, auto_level):
+    """cluster_cycle 2: the cluster launch starts at the level with <= 16^3 unknowns and the
+    level above it is smoothed by the coarse tile kernels (64^3) or colour passes (48^3). The
+    automatic choice (cluster_cycle 1) takes that level only where the level above is tiled."""
+    nz, ny, nx = shape
+    k, _ = random_k(shape, seed=50 + nx)
+    H1, C1, E1, s1 = gpu_run(k, tol=1e-7, cluster_cycle=2)
+    H2, C2, E2, s2 = gpu_run(k, tol=1e-7, cluster_cycle=0)
+    H3, C3, E3, s3 = gpu_run(k, tol=1e-7, cluster_cycle=1)
+    assert H1.stats().cluster_level == 2 and H2.stats().cluster_level == -1
+    assert H3.stats().cluster_level == auto_level
+    assert rel_c(C1, C2) <= 1e-6 and rel_c(C3, C2) <= 1e-6
+    assert abs(H1.stats().iterations - H2.stats().iterations) <= 1
+    check_against_oracle(k, C1, E1, s1)
+
+
 def test_mixed_precision_stationary_refinement():
     """The stationary form (solver "vcycle"): FP64 refinement around one 16-bit V-cycle per step."""
     k, _ = random_k((32, 32, 32), seed=33)
