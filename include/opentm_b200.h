@@ -149,6 +149,15 @@ OTM_API otm_status otm_homo_set_tolerance(otm_homo* h, double fem_rel_thres);
  * (MG_H::updateStencils, homogenization/MG.cpp:144-151). */
 OTM_API otm_status otm_homo_update(otm_homo* h, const float* k_dev, int pitchT);
 
+/* otm_density_forward followed by otm_homo_update with its k, in fewer passes: the density chain's
+ * forward pass (filter, SIMP map; arguments as otm_density_forward, on the handle's stream) writes
+ * the conductivities straight into the handle (the conductivity import of Grid_H::update folded
+ * into the pow/affine epilogue of the filter, TensorExpression.h:816-843), then the coarse
+ * operators are rebuilt. rho_f may be NULL; dk and wsum are written for otm_density_backward. */
+OTM_API otm_status otm_homo_update_density(otm_homo* h, const int reso[3], const float* rho, int rho_pitchT,
+                                           float* rho_f, float* dk, float* wsum, int weight_type, float radius,
+                                           int periodic, float p, float k0, float kmin);
+
 /* MG_H::solveEquation for the 3 load cases at once (homogenization/MG.cpp:80-142 called per
  * case at homogenization/homogenization.cu:182-188); warm-started unless disabled. */
 OTM_API otm_status otm_homo_solve(otm_homo* h, otm_solve_stats* stats);
@@ -166,6 +175,13 @@ OTM_API otm_status otm_homo_heat_matrix_nosolve(otm_homo* h, double C[9]);
  * (dC_ij + [i!=j] dC_ji). lexi != 0 writes element (x,y,z) at x + (y + z*ny)*pitchT (the
  * reference's lexiOrder = true layout); lexi == 0 writes it unpitched. */
 OTM_API otm_status otm_homo_sensitivity(otm_homo* h, const float dC[9], float* sens_dev, int pitchT, int lexi);
+
+/* otm_homo_heat_matrix and otm_homo_sensitivity(dC) in one element pass (the sensitivity kernel
+ * Sensitivity_kernel_opt_2_H fused with the K^H kernel, homogenization/homogenization.cu:13-153,
+ * 255-412) for a dC that does not depend on C (a linear objective such as the OC loop's
+ * -trace K^H): solves, then one kernel emits C and sens_dev exactly as the two calls would. */
+OTM_API otm_status otm_homo_heat_matrix_sensitivity(otm_homo* h, double C[9], const float dC[9], float* sens_dev,
+                                                    int pitchT, int lexi);
 
 /* dK^H_ij / dk_e for the 6 unique pairs (00 01 02 11 12 22), 6 unpitched fields of ne floats. */
 OTM_API otm_status otm_homo_element_energy(otm_homo* h, float* energy_dev);

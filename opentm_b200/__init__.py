@@ -169,6 +169,17 @@ class Homogenization_H:
         self._sync_stream()
         check(lib().otm_homo_update(self._h, ctypes.c_void_p(_ptr(rho)), int(pitchT)), "otm_homo_update")
 
+    def update_density(self, df: "DensityFilter", rho, pitchT: int = -1):
+        """df.forward(rho) followed by update(k) with the conductivity import folded into the
+        filter's forward pass (otm_homo_update_density): df.rho_f, df.dk and df.wsum are written as
+        by df.forward, for df.backward; the conductivities go straight into this handle (df.k is
+        left as it was)."""
+        self._sync_stream()
+        check(lib().otm_homo_update_density(self._h, i3(df.reso), ctypes.c_void_p(_ptr(rho)), int(pitchT),
+                                            ctypes.c_void_p(_ptr(df.rho_f)), ctypes.c_void_p(_ptr(df.dk)),
+                                            ctypes.c_void_p(_ptr(df.wsum)), df.weight, df.radius, int(df.periodic),
+                                            df.p, df.k0, df.kmin), "otm_homo_update_density")
+
     def solve(self, allow_not_converged: bool = False) -> _lib.SolveStats:
         self._sync_stream()
         st = _lib.SolveStats()
@@ -196,6 +207,18 @@ class Homogenization_H:
         d = (ctypes.c_float * 9)(*[float(v) for v in np.asarray(dC, dtype=np.float64).reshape(9)])
         check(lib().otm_homo_sensitivity(self._h, d, ctypes.c_void_p(_ptr(sens)), int(pitchT), int(bool(lexiOrder))),
               "otm_homo_sensitivity")
+
+    def heatMatrixSensitivity(self, dC, sens, pitchT: int = -1, lexiOrder: bool = False,
+                              allow_not_converged: bool = False) -> np.ndarray:
+        """heatMatrix() and Sensitivity(dC, sens, pitchT, lexiOrder) in one element pass, for a dC
+        that does not depend on C (a linear objective); returns C."""
+        self._sync_stream()
+        C = (ctypes.c_double * 9)()
+        d = (ctypes.c_float * 9)(*[float(v) for v in np.asarray(dC, dtype=np.float64).reshape(9)])
+        allow = (0, _lib.OTM_ERR_NOT_CONVERGED) if allow_not_converged else (0,)
+        check(lib().otm_homo_heat_matrix_sensitivity(self._h, C, d, ctypes.c_void_p(_ptr(sens)), int(pitchT),
+                                                     int(bool(lexiOrder))), "otm_homo_heat_matrix_sensitivity", allow)
+        return np.array(C[:], dtype=np.float64).reshape(3, 3)
 
     def element_energy(self, out=None):
         """dK^H_ab/dk_e for the pairs 00 01 02 11 12 22 as a (6, nz, ny, nx) tensor."""

@@ -139,10 +139,13 @@ SIGNATURES = {
     "otm_homo_get_config": (_S, [_P, ctypes.POINTER(Config)]),
     "otm_homo_set_tolerance": (_S, [_P, ctypes.c_double]),
     "otm_homo_update": (_S, [_P, _P, ctypes.c_int]),
+    "otm_homo_update_density": (_S, [_P, _I3, _P, ctypes.c_int, _P, _P, _P, ctypes.c_int, ctypes.c_float,
+                                     ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float]),
     "otm_homo_solve": (_S, [_P, ctypes.POINTER(SolveStats)]),
     "otm_homo_heat_matrix": (_S, [_P, _D]),
     "otm_homo_heat_matrix_nosolve": (_S, [_P, _D]),
     "otm_homo_sensitivity": (_S, [_P, _F, _P, ctypes.c_int, ctypes.c_int]),
+    "otm_homo_heat_matrix_sensitivity": (_S, [_P, _D, _F, _P, ctypes.c_int, ctypes.c_int]),
     "otm_homo_element_energy": (_S, [_P, _P]),
     "otm_homo_get_solution": (_S, [_P, ctypes.c_int, _P]),
     "otm_homo_v_cycle": (_S, [_P, _P, _P, ctypes.c_int, ctypes.c_int]),

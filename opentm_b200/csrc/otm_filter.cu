@@ -65,6 +65,9 @@ static otm_status make_weights(int type, float radius, ConvWeights* cw) {
 //   MODE 1: forward + SIMP     also k = (k0 - kmin) out^p + kmin and dk = dk/dout
 //   MODE 2: adjoint            out = sum_off w g(i - off) / ws(i - off)
 //   MODE 3: adjoint chain      as 2 with g = g_k * dk
+//   MODE 4: forward + SIMP + conductivity import: as 1, with k written as the solver's raw
+//           conductivity and ks = 1e-9 + k^pp beside it (k_import's arithmetic), a negative,
+//           NaN or Inf k flagged in *bad
 constexpr int kTX = 32, kTY = 8, kTZ = 4;
 
 template <int H>
@@ -100,9 +103,10 @@ __global__ void __launch_bounds__(256) k_conv_tiled(Dims d, const float* __restr
                                                     float* __restrict__ dst, int dst_pitch,
                                                     float* __restrict__ ws_out, int periodic, TapList tl,
                                                     float wsum_all, float p, float k0, float kmin,
-                                                    float* __restrict__ kout, float* __restrict__ dkout) {
+                                                    float* __restrict__ kout, float* __restrict__ dkout,
+                                                    float* __restrict__ ksout, float pp, int* bad) {
   constexpr int SX = kTX + 2 * H, SY = kTY + 2 * H, SZ = kTZ + 2 * H;
-  constexpr bool kFwd = MODE < 2;
+  constexpr bool kFwd = MODE < 2 || MODE == 4;
   extern __shared__ float sm[];
   float* val = sm;
   float* msk = sm + SX * SY * SZ;  // only used without periodicity
@@ -175,11 +179,16 @@ __global__ void __launch_bounds__(256) k_conv_tiled(Dims d, const float* __restr
       const float out = sumv / ws;
       if (dst) dst[row * dst_pitch + gx] = out;
       if (ws_out) ws_out[row * d.nx + gx] = ws;
-      if (MODE == 1) {
+      if (MODE == 1 || MODE == 4) {
         const float pw = (p == 3.f) ? out * out * out : powf(out, p);
-        kout[row * d.nx + gx] = (k0 - kmin) * pw + kmin;
+        const float k = (k0 - kmin) * pw + kmin;
+        kout[row * d.nx + gx] = k;
         const float dpw = (p == 3.f) ? 3.f * out * out : p * powf(out, p - 1.f);
         dkout[row * d.nx + gx] = (k0 - kmin) * dpw;
+        if (MODE == 4) {
+          if (!(k >= 0.f) || !isfinite(k)) atomicOr(bad, 1);
+          ksout[row * d.nx + gx] = kRhoPenalMin + (pp == 1.f ? k : powf(k, pp));
+        }
       }
     } else {
       dst[row * dst_pitch + gx] = sumv;
@@ -191,7 +200,7 @@ template <int H, int MODE>
 static otm_status launch_tiled(const Dims& d, const float* src, int src_pitch, const float* dk_in,
                                const float* ws_in, float* dst, int dst_pitch, float* ws_out, int periodic,
                                const ConvWeights& cw, float wsum_all, float p, float k0, float kmin, float* kout,
-                               float* dkout, cudaStream_t s) {
+                               float* dkout, float* ksout, float pp, int* bad, cudaStream_t s) {
   const size_t smem = size_t(tile_elems<H>()) * sizeof(float) * (periodic ? 1 : 2);
   static bool attr = false;  // the attribute is per function and process-wide
   if (!attr) {
@@ -202,7 +211,8 @@ static otm_status launch_tiled(const Dims& d, const float* src, int src_pitch, c
   TapList tl;
   make_taps<H>(cw, &tl);
   k_conv_tiled<H, MODE><<<grid, dim3(kTX, kTY), smem, s>>>(d, src, src_pitch, dk_in, ws_in, dst, dst_pitch, ws_out,
-                                                          periodic, tl, wsum_all, p, k0, kmin, kout, dkout);
+                                                          periodic, tl, wsum_all, p, k0, kmin, kout, dkout, ksout,
+                                                          pp, bad);
   OTM_CHECK_LAUNCH("k_conv_tiled");
   count_launches(1);
   return OTM_OK;
@@ -212,7 +222,7 @@ template <int MODE>
 static otm_status conv_dispatch(const Dims& d, const float* src, int src_pitch, const float* dk_in,
                                 const float* ws_in, float* dst, int dst_pitch, float* ws_out, int periodic,
                                 const ConvWeights& cw, float p, float k0, float kmin, float* kout, float* dkout,
-                                cudaStream_t s) {
+                                cudaStream_t s, float* ksout = nullptr, float pp = 1.f, int* bad = nullptr) {
   // sum of the normalised weights in the reference's tap order (the in-bounds weight of a
   // periodic filter)
   float wsum_all = 0.f;
@@ -221,12 +231,27 @@ static otm_status conv_dispatch(const Dims& d, const float* src, int src_pitch, 
 #define OTM_H(HH) \
   case HH:        \
     return launch_tiled<HH, MODE>(d, src, src_pitch, dk_in, ws_in, dst, dst_pitch, ws_out, periodic, cw, wsum_all, \
-                                  p, k0, kmin, kout, dkout, s);
+                                  p, k0, kmin, kout, dkout, ksout, pp, bad, s);
     OTM_H(0) OTM_H(1) OTM_H(2) OTM_H(3) OTM_H(4) OTM_H(5) OTM_H(6)
 #undef OTM_H
   }
   set_error("unsupported filter half width");
   return OTM_ERR_UNSUPPORTED;
+}
+
+// The density chain's forward pass writing straight into a homogenization handle's conductivity
+// buffers (otm_homo_update_density): rho_f, dk and wsum as otm_density_forward, k as kraw and
+// ks = 1e-9 + k^pp, invalid values flagged in *bad.
+otm_status density_forward_import(const Dims& d, const float* rho, int rho_pitchT, float* rho_f, float* dk,
+                                  float* wsum, int weight_type, float radius, int periodic, float p, float k0,
+                                  float kmin, float* kraw, float* ks, float pp, int* bad, cudaStream_t s) {
+  if (!rho || !dk || !wsum) return OTM_ERR_INVALID_ARGUMENT;
+  if (rho_pitchT <= 0) rho_pitchT = d.nx;
+  if (rho_pitchT < d.nx) return OTM_ERR_INVALID_ARGUMENT;
+  ConvWeights cw;
+  OTM_TRY(make_weights(weight_type, radius, &cw));
+  return conv_dispatch<4>(d, rho, rho_pitchT, nullptr, nullptr, rho_f, d.nx, wsum, periodic, cw, p, k0, kmin, kraw,
+                          dk, s, ks, pp, bad);
 }
 
 static otm_status check_reso(const int reso[3]) {

@@ -437,6 +437,28 @@ otm_status Homo::update(const float* kin, int pitchT) {
   k_import<<<ceil_div(nv, kBlock), kBlock, 0, stream>>>(d0, kin, pitchT, cfg.power_penal, ks, kraw, flags);
   OTM_CHECK_LAUNCH("k_import");
   launched(1);
+  return update_operators();
+}
+
+// update() from a density field: the density chain's forward pass (filter, SIMP map) writes the
+// conductivities straight into this handle (no k field, no import pass), then the operators are
+// built as in update().
+otm_status Homo::update_density(const DensityArgs& a) {
+  const Dims d0 = lv[0].d;
+  OTM_TRY(enter());
+  OTM_TRY(join_coarse());
+  OTM_CUDA(cudaMemsetAsync(flags, 0, 2 * sizeof(int), stream));
+  OTM_TRY(density_forward_import(d0, a.rho, a.rho_pitchT, a.rho_f, a.dk, a.wsum, a.weight_type, a.radius, a.periodic,
+                                 a.p, a.k0, a.kmin, kraw, ks, cfg.power_penal, flags, stream));
+  launched(1);
+  return update_operators();
+}
+
+// Galerkin stencils of every coarse level and the dense coarsest inverse for the imported ks (the
+// coarse chain on a side stream), then leave().
+otm_status Homo::update_operators() {
+  const Dims d0 = lv[0].d;
+  const size_t nv = d0.nv();
   const int L = int(lv.size());
   const unsigned int* kmax_bits = (const unsigned int*)(flags + 2);
   if (mixed) {
@@ -914,10 +936,26 @@ void Homo::launch_solve_init() {
   launched(2);
 }
 
+// K^H of the current solutions (-> sc->kh), with the sensitivity of a pending
+// heat_matrix_sensitivity call in the same element pass.
 void Homo::launch_heat_matrix() {
   const Dims d0 = lv[0].d;
-  k_heat_matrix<<<reduce_blocks(d0.nv()), kBlock, 0, stream>>>(d0, ks, x, op, ef, partials, sc);
+  const int nb = reduce_blocks(d0.nv());
+  if (sens_req.on)
+    k_elem_pass<true, true><<<nb, kBlock, 0, stream>>>(d0, ks, kraw, x, op, ef, sens_req.sw, cfg.power_penal,
+                                                        sens_req.sens, sens_req.pitchT, partials, sc);
+  else
+    k_elem_pass<true, false><<<nb, kBlock, 0, stream>>>(d0, ks, kraw, x, op, ef, SensWeights{}, cfg.power_penal,
+                                                         nullptr, 0, partials, sc);
   launched(1);
+}
+
+static SensWeights sens_weights(const float dC[9]) {
+  SensWeights sw;
+  int cnt = 0;
+  for (int a = 0; a < 3; a++)
+    for (int bq = a; bq < 3; bq++) sw.w[cnt++] = dC[a * 3 + bq] + (a != bq ? dC[bq * 3 + a] : 0.f);
+  return sw;
 }
 
 // Solve the 3 load cases to the tolerance (MG_H::solveEquation, homogenization/MG.cpp:80-142;
@@ -1207,7 +1245,7 @@ otm_status Homo::heat_matrix(double C[9], bool do_solve) {
   }
   if (!heat_ready) {
     launch_heat_matrix();
-    OTM_CHECK_LAUNCH("k_heat_matrix");
+    OTM_CHECK_LAUNCH("k_elem_pass");
     OTM_CUDA(cudaMemcpyAsync(sc_host->kh, sc->kh, 6 * sizeof(double), cudaMemcpyDeviceToHost, stream));
     OTM_CUDA(cudaStreamSynchronize(stream));
   }
@@ -1231,17 +1269,31 @@ otm_status Homo::sensitivity(const float dC[9], float* sens, int pitchT, int lex
   const Dims d0 = lv[0].d;
   if (!lexi || pitchT <= 0) pitchT = d0.nx;
   if (pitchT < d0.nx) return invalid("pitchT smaller than the x resolution");
-  SensWeights sw;
-  int cnt = 0;
-  for (int a = 0; a < 3; a++)
-    for (int bq = a; bq < 3; bq++) sw.w[cnt++] = dC[a * 3 + bq] + (a != bq ? dC[bq * 3 + a] : 0.f);
+  const SensWeights sw = sens_weights(dC);
   OTM_TRY(enter());
-  const size_t total = size_t(pitchT) * d0.ny * d0.nz;
-  k_sensitivity<<<ceil_div(total, kBlock), kBlock, 0, stream>>>(d0, kraw, x, op, ef, sw, cfg.power_penal, sens,
-                                                                pitchT);
-  OTM_CHECK_LAUNCH("k_sensitivity");
+  const size_t nruns = size_t((d0.nx + kRun - 1) / kRun) * d0.ny * d0.nz;
+  k_elem_pass<false, true><<<ceil_div(nruns, kBlock), kBlock, 0, stream>>>(d0, ks, kraw, x, op, ef, sw,
+                                                                           cfg.power_penal, sens, pitchT, nullptr,
+                                                                           nullptr);
+  OTM_CHECK_LAUNCH("k_elem_pass");
   launched(1);
   return leave();
+}
+
+// heat_matrix and sensitivity(dC) in one element pass, for a dC known before K^H (a linear
+// objective): the solve, then one kernel that emits both.
+otm_status Homo::heat_matrix_sensitivity(double C[9], const float dC[9], float* sens, int pitchT, int lexi) {
+  if (!C || !dC || !sens) return invalid("NULL argument");
+  const Dims d0 = lv[0].d;
+  if (!lexi || pitchT <= 0) pitchT = d0.nx;
+  if (pitchT < d0.nx) return invalid("pitchT smaller than the x resolution");
+  sens_req.on = true;
+  sens_req.sw = sens_weights(dC);
+  sens_req.sens = sens;
+  sens_req.pitchT = pitchT;
+  const otm_status st = heat_matrix(C, true);
+  sens_req.on = false;
+  return st;
 }
 
 otm_status Homo::element_energy(float* out) {
@@ -1377,6 +1429,25 @@ otm_status otm_homo_heat_matrix_nosolve(otm_homo* h, double C[9]) {
 otm_status otm_homo_sensitivity(otm_homo* h, const float dC[9], float* sens_dev, int pitchT, int lexi) {
   if (!h) return OTM_ERR_INVALID_ARGUMENT;
   return h->impl.sensitivity(dC, sens_dev, pitchT, lexi);
+}
+
+otm_status otm_homo_update_density(otm_homo* h, const int reso[3], const float* rho, int rho_pitchT, float* rho_f,
+                                   float* dk, float* wsum, int weight_type, float radius, int periodic, float p,
+                                   float k0, float kmin) {
+  if (!h) return OTM_ERR_INVALID_ARGUMENT;
+  const otm::Dims d = h->impl.lv[0].d;
+  if (!reso || reso[0] != d.nx || reso[1] != d.ny || reso[2] != d.nz) {
+    otm::set_error("reso differs from the handle's resolution");
+    return OTM_ERR_INVALID_ARGUMENT;
+  }
+  otm::Homo::DensityArgs a{rho, rho_pitchT, rho_f, dk, wsum, weight_type, radius, periodic, p, k0, kmin};
+  return h->impl.update_density(a);
+}
+
+otm_status otm_homo_heat_matrix_sensitivity(otm_homo* h, double C[9], const float dC[9], float* sens_dev, int pitchT,
+                                            int lexi) {
+  if (!h) return OTM_ERR_INVALID_ARGUMENT;
+  return h->impl.heat_matrix_sensitivity(C, dC, sens_dev, pitchT, lexi);
 }
 
 otm_status otm_homo_element_energy(otm_homo* h, float* energy_dev) {

@@ -37,6 +37,11 @@ struct ChunkGraph {
 
 constexpr int kMaxChunk = 64;
 
+// otm_filter.cu: the density chain's forward pass into a handle's conductivity buffers.
+otm_status density_forward_import(const Dims& d, const float* rho, int rho_pitchT, float* rho_f, float* dk,
+                                  float* wsum, int weight_type, float radius, int periodic, float p, float k0,
+                                  float kmin, float* kraw, float* ks, float pp, int* bad, cudaStream_t s);
+
 struct Homo {
   otm_config cfg{};
   cudaStream_t stream = nullptr;       // private stream (graph capture needs a non-legacy stream)
@@ -114,7 +119,27 @@ struct Homo {
   otm_status build(const otm_config& c, cudaStream_t ext_stream = nullptr, cudaMemPool_t ext_pool = nullptr,
                    bool external_mode = false);
   void launch_solve_init();
+  // arguments of otm_homo_update_density (the density chain's forward pass, otm_density_forward)
+  struct DensityArgs {
+    const float* rho;
+    int rho_pitchT;
+    float *rho_f, *dk, *wsum;
+    int weight_type;
+    float radius;
+    int periodic;
+    float p, k0, kmin;
+  };
+  otm_status update_density(const DensityArgs& a);
+  otm_status update_operators();
   void launch_heat_matrix();
+  // the sensitivity that launch_heat_matrix emits in the same element pass (heat_matrix_sensitivity)
+  struct SensRequest {
+    bool on = false;
+    SensWeights sw{};
+    float* sens = nullptr;
+    int pitchT = 0;
+  } sens_req;
+  otm_status heat_matrix_sensitivity(double C[9], const float dC[9], float* sens, int pitchT, int lexi);
   otm_status tile_attributes();
   otm_status join_coarse();
   otm_status enter();

@@ -993,63 +993,143 @@ __device__ __forceinline__ void elem_energy(const Dims& d, size_t e, const float
     }
 }
 
-// K^H_ab = sum_e k_e E_ab(e) / vol with FP64 accumulation (vol = 1), -> sc->kh.
-static __global__ void __launch_bounds__(kBlock) k_heat_matrix(Dims d, const float* __restrict__ ks,
-                                                        const float* __restrict__ chi, FineOp op, ElemFields ef,
-                                                        double* partials, SolveScalars* sc) {
-  __shared__ double smem[32 * 6];
-  const size_t nv = d.nv();
-  double v[6] = {0, 0, 0, 0, 0, 0};
-  for (size_t e = size_t(blockIdx.x) * blockDim.x + threadIdx.x; e < nv; e += size_t(gridDim.x) * blockDim.x) {
-    float E[6];
-    elem_energy(d, e, chi, op, ef, E);
-    const double k = __ldg(ks + e);
-#pragma unroll
-    for (int i = 0; i < 6; i++) v[i] += k * double(E[i]);
-  }
-  block_reduce_f64<6>(v, smem);
-  if (threadIdx.x == 0)
-#pragma unroll
-    for (int i = 0; i < 6; i++) partials[blockIdx.x * 6 + i] = v[i];
-  if (last_block(&sc->counter[T_KH])) {
-    double t[6];
-    reduce_partials<6>(partials, gridDim.x, t, smem);
-    if (threadIdx.x == 0) {
-#pragma unroll
-      for (int i = 0; i < 6; i++) sc->kh[i] = t[i];
-      sc->counter[T_KH] = 0;
-    }
-  }
-}
-
+// K^H_ab = sum_e k_e E_ab(e) / vol with FP64 accumulation (vol = 1), -> sc->kh;
 // sens_e = p k^(p-1) sum_{a<=b} E_ab (dC_ab + [a != b] dC_ba); pitched lexicographic output
 // with zeroed pitch padding (Sensitivity_kernel_opt_2_H + init_array, homogenization.cu:415-479).
 struct SensWeights {
   float w[6];
 };
 
-static __global__ void __launch_bounds__(kBlock) k_sensitivity(Dims d, const float* __restrict__ kraw,
-                                                        const float* __restrict__ chi, FineOp op, ElemFields ef,
-                                                        SensWeights sw, float p, float* __restrict__ sens,
-                                                        int pitchT) {
-  const size_t total = size_t(pitchT) * d.ny * d.nz;
-  const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (t >= total) return;
-  const unsigned yz32 = unsigned(t) / unsigned(pitchT);
-  const int x = int(unsigned(t) - yz32 * unsigned(pitchT));
-  const size_t yz = yz32;
-  if (x >= d.nx) {
-    sens[t] = 0.f;
-    return;
-  }
-  const size_t e = yz * d.nx + x;
-  float E[6];
-  elem_energy(d, e, chi, op, ef, E);
-  float s = 0.f;
+// The element pass of K^H and of the sensitivity, either or both at once (the sensitivity kernel
+// fused with the K^H kernel: one pass computes the element energies once and emits the FP64 K^H
+// partials and sens_e). One thread takes a run of kRun consecutive elements along x: the faces
+// x0 .. x0 + kRun of the run are gathered once (4 corners x 3 cases) and transformed over (y, z)
+// once, and each element combines two neighbouring faces with the x stage of the Walsh-Hadamard
+// transform, so neighbouring elements share a face's loads and butterflies (about a third of
+// the instructions of elem_energy per element). The transform is linear, so W (disp - chi) =
+// W disp - W chi with W disp a per-thread constant. sens: written when kSens, pitched by pitchT
+// with the padding zeroed.
+constexpr int kRun = 8;
+
+__device__ __forceinline__ void face_wht(const float* __restrict__ chi, size_t nv, size_t i00, size_t i10, size_t i01,
+                                         size_t i11, float (&F)[3][4]) {
 #pragma unroll
-  for (int i = 0; i < 6; i++) s += E[i] * sw.w[i];
-  const float pr = (p == 1.f) ? 1.f : p * powf(__ldg(kraw + e), p - 1.f);
-  sens[t] = s * pr;
+  for (int c = 0; c < 3; c++) {
+    const float* q = chi + c * nv;
+    const float a = __ldg(q + i00), b = __ldg(q + i10), cc = __ldg(q + i01), e = __ldg(q + i11);
+    const float p0 = a + b, p1 = a - b, p2 = cc + e, p3 = cc - e;  // y stage
+    F[c][0] = p0 + p2;                                                // z stage
+    F[c][1] = p1 + p3;
+    F[c][2] = p0 - p2;
+    F[c][3] = p1 - p3;
+  }
+}
+
+template <bool kKH, bool kSens>
+__global__ void __launch_bounds__(kBlock) k_elem_pass(Dims d, const float* __restrict__ ks,
+                                                     const float* __restrict__ kraw, const float* __restrict__ chi,
+                                                     FineOp op, ElemFields ef, SensWeights sw, float p,
+                                                     float* __restrict__ sens, int pitchT, double* partials,
+                                                     SolveScalars* sc) {
+  __shared__ double smem[32 * 6];
+  const size_t nv = d.nv();
+  const int nx = d.nx, ny = d.ny, nrow = (nx + kRun - 1) / kRun;
+  const size_t nruns = size_t(nrow) * ny * d.nz;
+  // W disp per case (same butterflies, index bits x, y, z = 1, 2, 4)
+  float dw[3][8];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+#pragma unroll
+    for (int j = 0; j < 8; j++) dw[c][j] = ef.disp[j][c];
+#pragma unroll
+    for (int st = 1; st < 8; st <<= 1)
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+        if (!(i & st)) {
+          const float a = dw[c][i], b = dw[c][i | st];
+          dw[c][i] = a + b;
+          dw[c][i | st] = a - b;
+        }
+  }
+  const float l0 = 0.125f * (op.c0 + 3.f * op.c1 + 3.f * op.c2 + op.c3);
+  const float l1 = 0.125f * (op.c0 + op.c1 - op.c2 - op.c3);
+  const float l2 = 0.125f * (op.c0 - op.c1 - op.c2 + op.c3);
+  const float l3 = 0.125f * (op.c0 - 3.f * op.c1 + 3.f * op.c2 - op.c3);
+  double v[6] = {0, 0, 0, 0, 0, 0};
+  for (size_t r = size_t(blockIdx.x) * blockDim.x + threadIdx.x; r < nruns; r += size_t(gridDim.x) * blockDim.x) {
+    const unsigned yz = unsigned(r / unsigned(nrow));
+    const int x0 = int(r - size_t(yz) * nrow) * kRun;
+    const int y = int(yz % unsigned(ny)), z = int(yz / unsigned(ny));
+    const int y1 = wrapm(y + 1, ny), z1 = wrapm(z + 1, d.nz);
+    const size_t r00 = (size_t(y) + size_t(ny) * z) * nx, r10 = (size_t(y1) + size_t(ny) * z) * nx;
+    const size_t r01 = (size_t(y) + size_t(ny) * z1) * nx, r11 = (size_t(y1) + size_t(ny) * z1) * nx;
+    float F[3][4];
+    face_wht(chi, nv, r00 + x0, r10 + x0, r01 + x0, r11 + x0, F);
+#pragma unroll
+    for (int i = 0; i < kRun; i++) {
+      const int x = x0 + i;
+      if (x < nx) {
+        const int xn = x + 1 < nx ? x + 1 : 0;
+        float G[3][4];
+        face_wht(chi, nv, r00 + xn, r10 + xn, r01 + xn, r11 + xn, G);
+        float w[3][8];
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            w[c][2 * q] = dw[c][2 * q] - (F[c][q] + G[c][q]);
+            w[c][2 * q + 1] = dw[c][2 * q + 1] - (F[c][q] - G[c][q]);
+          }
+        float E[6];
+        int cnt = 0;
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+#pragma unroll
+          for (int bq = a; bq < 3; bq++) {
+            const float* u = w[a];
+            const float* t = w[bq];
+            const float s1 = u[1] * t[1] + u[2] * t[2] + u[4] * t[4];
+            const float s2 = u[3] * t[3] + u[5] * t[5] + u[6] * t[6];
+            E[cnt++] = l0 * (u[0] * t[0]) + l1 * s1 + l2 * s2 + l3 * (u[7] * t[7]);
+          }
+        const size_t e = size_t(yz) * nx + x;
+        if (kKH) {
+          const double k = __ldg(ks + e);
+#pragma unroll
+          for (int j = 0; j < 6; j++) v[j] += k * double(E[j]);
+        }
+        if (kSens) {
+          float sv = 0.f;
+#pragma unroll
+          for (int j = 0; j < 6; j++) sv += E[j] * sw.w[j];
+          const float pr = (p == 1.f) ? 1.f : p * powf(__ldg(kraw + e), p - 1.f);
+          sens[size_t(yz) * pitchT + x] = sv * pr;
+        }
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+#pragma unroll
+          for (int q = 0; q < 4; q++) F[c][q] = G[c][q];
+      }
+    }
+    // the pitch padding of the row, by the thread of its last run
+    if (kSens && x0 + kRun >= nx)
+      for (int x = nx; x < pitchT; x++) sens[size_t(yz) * pitchT + x] = 0.f;
+  }
+  if (kKH) {
+    block_reduce_f64<6>(v, smem);
+    if (threadIdx.x == 0)
+#pragma unroll
+      for (int i = 0; i < 6; i++) partials[blockIdx.x * 6 + i] = v[i];
+    if (last_block(&sc->counter[T_KH])) {
+      double t[6];
+      reduce_partials<6>(partials, gridDim.x, t, smem);
+      if (threadIdx.x == 0) {
+#pragma unroll
+        for (int i = 0; i < 6; i++) sc->kh[i] = t[i];
+        sc->counter[T_KH] = 0;
+      }
+    }
+  }
 }
 
 // 6 unpitched fields of dK^H_ab / dk_e.

@@ -56,6 +56,39 @@ def test_density_chain_forward_backward():
     assert rel_field(g, g_ref)[0] <= FILTER_TOL
 
 
+@pytest.mark.parametrize("power_penal", [1.0, 2.0])
+def test_update_density_equals_forward_then_update(power_penal):
+    """Homogenization_H.update_density (the filter's forward pass writing the handle's
+    conductivities, no import pass) gives what df.forward + H.update give, bit for bit: the
+    filter outputs, K^H and the sensitivity (power_penal 2 checks the import's k^p and the
+    sensitivity's k^(p-1) on the folded path); an invalid density is reported the same way."""
+    from opentm_b200 import DensityFilter, HomoConfig, Homogenization_H
+    n = 24
+    rho = torch.from_numpy(wl.config2_density(n, seed=3)).cuda()
+    dC = -np.eye(3)
+    res = []
+    for folded in (False, True):
+        df = DensityFilter((n, n, n), radius=2.0, weight=1, periodic=True, p=3.0, k0=1.0, kmin=1e-3)
+        H = Homogenization_H(HomoConfig(reso=n, femRelThres=1e-7, pre_smooth=2, post_smooth=2,
+                                        power_penal=power_penal))
+        if folded:
+            H.update_density(df, rho)
+        else:
+            H.update(df.forward(rho))
+        sens = torch.empty((n, n, n), dtype=torch.float32, device="cuda")
+        C = H.heatMatrixSensitivity(dC, sens)
+        torch.cuda.synchronize()
+        res.append((C, sens.cpu().numpy(), df.rho_f.cpu().numpy(), df.dk.cpu().numpy(), df.wsum.cpu().numpy()))
+    for a, b in zip(res[0], res[1]):
+        assert np.array_equal(a, b)
+    bad = rho.clone()
+    bad[1, 2, 3] = float("nan")
+    H = Homogenization_H(HomoConfig(reso=n))
+    H.update_density(DensityFilter((n, n, n), radius=2.0, weight=1), bad)
+    with pytest.raises(Exception):
+        H.heatMatrix()
+
+
 def test_oc_filter_sens():
     from opentm_b200 import OCOptimizer
     shape = (12, 12, 12)

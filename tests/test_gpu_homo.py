@@ -275,6 +275,38 @@ def test_cluster_from_16_cubed(shape, auto_level):
     check_against_oracle(k, C1, E1, s1)
 
 
+@pytest.mark.parametrize("precision", ["fp32", "bf16"])
+def test_heat_matrix_sensitivity_one_pass(precision):
+    """heatMatrixSensitivity (K^H and the sensitivity in one element pass) returns what
+    heatMatrix + Sensitivity return, bit for bit, pitched output with zeroed padding included; x
+    not a multiple of the 8-element runs of the element pass."""
+    from opentm_b200 import HomoConfig, Homogenization_H
+    shape = (16, 12, 20)
+    nz, ny, nx = shape
+    k, _ = random_k(shape, seed=77)
+    kd = torch.from_numpy(k).cuda()
+    out = []
+    for fused in (False, True):
+        H = Homogenization_H(HomoConfig(reso=(nx, ny, nz), femRelThres=1e-7, pre_smooth=2, post_smooth=2,
+                                        precision=precision))
+        H.update(kd)
+        s = torch.full((nz, ny, nx + 5), 7.0, dtype=torch.float32, device="cuda")
+        if fused:
+            C = H.heatMatrixSensitivity(DC_TEST, s, nx + 5, True)
+        else:
+            C = H.heatMatrix()
+            H.Sensitivity(DC_TEST, s, nx + 5, True)
+        torch.cuda.synchronize()
+        out.append((C, s.cpu().numpy()))
+    (C1, s1), (C2, s2) = out
+    assert np.array_equal(C1, C2) and np.array_equal(s1, s2)
+    assert np.all(s2[:, :, nx:] == 0)
+    ref = oracle_solution(k)
+    assert rel_entries(C2, ref["C"]).max() <= KH_TOL
+    mx, l2 = rel_field(s2[:, :, :nx], ora.sensitivity(ref["energy"], k, DC_TEST))
+    assert mx <= SENS_TOL and l2 <= SENS_TOL, (mx, l2)
+
+
 def test_mixed_precision_stationary_refinement():
     """The stationary form (solver "vcycle"): FP64 refinement around one 16-bit V-cycle per step."""
     k, _ = random_k((32, 32, 32), seed=33)
