@@ -201,9 +201,14 @@ def run_ours(args, rank, world, local_rank):
             torch.distributed.barrier()
         torch.cuda.synchronize()
         prof = H.profile(reset=True)
-        k_last = df.k.detach().cpu().numpy()
-        return {"lat_ms": lat, "C": Cs, "launches": launches, "prof": prof, "k_last": k_last,
-                "iters": H.stats().iterations}
+        iters = H.stats().iterations
+        # one more (untimed) step for the error check: the step writes the conductivities straight
+        # into the handle, so the field it used is formed again from the density it started from
+        rho_chk = rho.clone()
+        C_chk = step(H, df, oc, rho)
+        k_last = df.forward(rho_chk).detach().cpu().numpy()
+        return {"lat_ms": lat, "C": Cs, "launches": launches, "prof": prof, "k_last": k_last, "C_chk": C_chk,
+                "iters": iters}
 
     clocks = ClockSampler(local_rank)
     clocks.start()
@@ -273,10 +278,10 @@ def run_ours(args, rank, world, local_rank):
     if clk:
         line["clocks"] = clk
     if world == 1 and not args.no_cpu:
-        line["cpu_baseline"], err = cpu_baseline(main["k_last"], main["C"][-1])
+        line["cpu_baseline"], err = cpu_baseline(main["k_last"], main["C_chk"])
         line["kh_err"], line["kh_err_entries"] = err
         if mixed is not None and "lat_ms" in mixed:
-            _, (e, ee) = cpu_baseline(mixed["k_last"], mixed["C"][-1], timed=False)
+            _, (e, ee) = cpu_baseline(mixed["k_last"], mixed["C_chk"], timed=False)
             line["mixed"]["kh_err"], line["mixed"]["kh_err_entries"] = e, ee
     if world == 1 and args.extra:
         # the other configurations on the same GPU, measured in the same run
@@ -298,7 +303,7 @@ def kh_errors(C_gpu, C_ref):
 
 def cpu_baseline(k_last, C_gpu, timed=True):
     """FP64 oracle (the reference algorithm restated) timed on the host cores for one solve of the
-    same workload (the density the GPU saw in its last timed step), and the K^H errors of the GPU
+    same workload (the field of one more step after the timed ones), and the K^H errors of the GPU
     result against it (the oracle converged to 1e-10)."""
     import oracle as ora
     ora.build()
@@ -524,6 +529,35 @@ def run_solve256(args, emit=True):
                      f"{n}^3 thresholded smoothed Gaussian field (seed 2), SIMP p=3", headline="bf16", emit=emit)
 
 
+def fine_sweep_roofline(args, n, kd):
+    """HBM roofline of the fine-level sweep kernel at a cell whose working set exceeds L2: CUDA
+    events around the first fine-level post-smoothing leg of every PCG iteration of a few FP32
+    solves (the profiled solve runs the iterations as chunked graphs with event nodes)."""
+    import torch
+    from opentm_b200 import HomoConfig, Homogenization_H
+    H = Homogenization_H(HomoConfig(reso=n, femRelThres=TOL, pre_smooth=2, post_smooth=2, warm_start=False,
+                                    max_iter=200, smoother=args.smoother, profile=True))
+    H.update(kd)
+    H.heatMatrix()
+    H.profile(reset=True)
+    for _ in range(2):
+        H.update(kd)
+        H.heatMatrix()
+    torch.cuda.synchronize()
+    pr = H.profile(reset=True)
+    del H
+    if pr.sweeps <= 0:
+        return None
+    hbm, peak_kind = load_peaks()
+    launch_ms = pr.sweep_ms / pr.sweeps / pr.launches_per_sweep
+    bytes_launch = pr.sweep_bytes / pr.launches_per_sweep
+    achieved = bytes_launch / (launch_ms * 1e-3) / 1e9
+    return {"bound": "hbm", "kernel": "k_tile_sweep (post-smoothing leg)" if pr.kernel_kind == 1 else "k_gs_fine_pair",
+            "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
+            "peak_kind": f"{peak_kind} hbm_gbs", "launch_us": round(launch_ms * 1e3, 3),
+            "algorithmic_bytes_per_launch": bytes_launch, "launches_timed": pr.sweeps * pr.launches_per_sweep}
+
+
 def run_solve32(args, emit=True):
     """Configuration 1: one plain solve of a 32^3 cell with rho ~ U(0.001, 1) (seed 0)."""
     from opentm_b200 import workloads as wl
@@ -570,6 +604,7 @@ def run_solve(args, n, k, label, field, headline, emit=True):
         if prec == "fp32":
             chi32 = np.stack([H.solution(c).cpu().numpy() for c in range(3)]).astype(np.float64)
         del H
+    sweep_roofline = fine_sweep_roofline(args, n, kd) if n * n * n * 40 > 126 * 2 ** 20 else None
     ora.build()
     k64 = k.astype(np.float64)
     base = None
@@ -591,6 +626,8 @@ def run_solve(args, n, k, label, field, headline, emit=True):
         out[prec] = {"solve_ms": round(r["ms"], 3), "solves_per_s": round(1e3 / r["ms"], 3), "kh_err": kh,
                      "kh_err_entries": kh_ent, "sens_err": se, "sens_err_l2": se2, "iterations": r["iterations"],
                      "refinements": r["refinements"], "rel_res": r["rel_res"]}
+    if sweep_roofline:
+        out["fp32"]["roofline"] = sweep_roofline
     line = {"metric": f"{n}^3 solve: solves/s (update + 3 load cases from zero + K^H + sensitivity), error vs "
                       "FP64 oracle",
             "value": out[headline]["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "steps": args.steps,

@@ -144,6 +144,19 @@ struct Homogenization_H {
     check(otm_homo_sensitivity(h_, &dC[0][0], sens, pitchT, lexiOrder ? 1 : 0), "Homogenization_H::Sensitivity");
   }
 
+  // Not in the reference: heatMatrix(C) and Sensitivity(dC, sens, pitchT, lexiOrder) in one
+  // element pass, for a dC that does not depend on C (a linear objective).
+  void heatMatrix(double C[3][3], float dC[3][3], float* sens, int pitchT, bool lexiOrder = false) {
+    double c[9];
+    otm_status s = otm_homo_heat_matrix_sensitivity(h_, c, &dC[0][0], sens, pitchT, lexiOrder ? 1 : 0);
+    if (s == OTM_ERR_NOT_CONVERGED)
+      std::printf("\033[31mFailed to converge\033[0m\n");
+    else
+      check(s, "Homogenization_H::heatMatrix");
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) C[i][j] = c[i * 3 + j];
+  }
+
   // The reference stores the strength and never uses it (homogenization.cpp:83-87).
   void ConfigDiagPrecondition(float strength) { diag_strength = strength; }
 

@@ -49,6 +49,20 @@ int main() {
   for (float v : s) ssum += v;
   std::printf("C %.9e %.9e %.9e %.9e %.9e %.9e\n", C[0][0], C[0][1], C[0][2], C[1][1], C[1][2], C[2][2]);
   std::printf("sens_sum %.9e\n", ssum);
+  {
+    // K^H and the sensitivity in one element pass (a handle of its own, the same field)
+    homo::Homogenization_H hom2(config, opt);
+    hom2.update(rho_d, pitchT);
+    double C2[3][3];
+    hom2.heatMatrix(C2, dC, sens_d, pitchT, true);
+    std::vector<float> s2(h.size());
+    cudaMemcpy(s2.data(), sens_d, s2.size() * sizeof(float), cudaMemcpyDeviceToHost);
+    bool same = true;
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) same = same && C2[i][j] == C[i][j];
+    for (size_t i = 0; i < s.size(); i++) same = same && s2[i] == s[i];
+    std::printf("fused_same %d\n", int(same));
+  }
 
   // MG_H view: re-solve from zero with a tighter tolerance
   homo::MG_H mg(hom);

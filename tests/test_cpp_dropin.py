@@ -49,6 +49,7 @@ def test_dropin_program_matches_python_path(tmp_path):
     # bits, so the two solves agree to the solver tolerance, not bitwise
     assert np.abs(got - want).max() / np.abs(want).max() <= 1e-6
     assert vals["relres"][0] <= 1e-7
+    assert vals["fused_same"] == [1.0]  # heatMatrix(C, dC, sens, ...) == heatMatrix + Sensitivity, bit for bit
     # same OC inputs through the oracle: filtered sensitivities, then the 20-step bisection
     import oracle as ora
     n3 = n ** 3
