@@ -80,9 +80,17 @@ __device__ __forceinline__ float3 cprolong_site(const float4* cb, int ux, int uy
 }
 
 // One colour pass over the tile: the thread's vertex of colour (CX, CY, CZ).
+// The operands of this thread's vertex in colour pass (CX, CY, CZ) that do not depend on u: its
+// 27 stencil values and its right-hand side. They are fetched one pass ahead (while the previous
+// pass computes), so the passes wait on shared memory only, not on L2.
+struct CPassOps {
+  float s[27];
+  float f[3];
+};
+
 template <int CX, int CY, int CZ>
-__device__ __forceinline__ void ctile_pass(float4* sm, const Dims& d, int x0, int y0, int z0,
-                                           const float* __restrict__ st, const float* __restrict__ f) {
+__device__ __forceinline__ void ctile_fetch(const Dims& d, int x0, int y0, int z0, const float* __restrict__ st,
+                                            const float* __restrict__ f, CPassOps& ops) {
   const int t = int(threadIdx.x);
   const int i = t & 7, j = (t >> 3) & 3, k = t >> 5;
   const int lx = 1 + 2 * i + CX, ly = 1 + 2 * j + CY, lz = 1 + 2 * k + CZ;
@@ -90,12 +98,20 @@ __device__ __forceinline__ void ctile_pass(float4* sm, const Dims& d, int x0, in
   const size_t nv = d.nv();
   const size_t v = size_t(X) + size_t(d.nx) * (size_t(Y) + size_t(d.ny) * Z);
   const size_t sb = cb_index(d, X, Y, Z);
-  float s[27];
 #pragma unroll
-  for (int o = 0; o < 27; o++) s[o] = __ldg(st + size_t(o) * nv + sb);
-  float acc[3];
+  for (int o = 0; o < 27; o++) ops.s[o] = __ldg(st + size_t(o) * nv + sb);
 #pragma unroll
-  for (int c = 0; c < 3; c++) acc[c] = __ldg(f + c * nv + v);
+  for (int c = 0; c < 3; c++) ops.f[c] = __ldg(f + c * nv + v);
+}
+
+// One colour pass (CX, CY, CZ) of the tile's interior from fetched operands: each thread updates
+// one vertex (128 threads: 8 x 4 x 4 vertices of the colour in the 16 x 8 x 8 tile).
+template <int CX, int CY, int CZ>
+__device__ __forceinline__ void ctile_apply(float4* sm, const CPassOps& ops) {
+  const int t = int(threadIdx.x);
+  const int i = t & 7, j = (t >> 3) & 3, k = t >> 5;
+  const int lx = 1 + 2 * i + CX, ly = 1 + 2 * j + CY, lz = 1 + 2 * k + CZ;
+  float acc[3] = {ops.f[0], ops.f[1], ops.f[2]};
   const float4* b = sm + csite(lx, ly, lz);
   // neighbour offsets: the parity of lx is fixed by the pass, so left / right are compile-time
   constexpr int oL = (CX == 0) ? -kCSHalf : kCSHalf - 1;  // lx odd for CX = 0
@@ -106,12 +122,22 @@ __device__ __forceinline__ void ctile_pass(float4* sm, const Dims& d, int x0, in
     const int ox = o % 3 - 1, oy = (o / 3) % 3 - 1, oz = o / 9 - 1;
     const int off = (ox < 0 ? oL : (ox > 0 ? oR : 0)) + oy * kCSRow + oz * kCSPlane;
     const float4 n = b[off];
-    acc[0] -= s[o] * n.x;
-    acc[1] -= s[o] * n.y;
-    acc[2] -= s[o] * n.z;
+    acc[0] -= ops.s[o] * n.x;
+    acc[1] -= ops.s[o] * n.y;
+    acc[2] -= ops.s[o] * n.z;
   }
-  const float inv = 1.0f / s[13];
+  const float inv = 1.0f / ops.s[13];
   sm[csite(lx, ly, lz)] = make_float4(acc[0] * inv, acc[1] * inv, acc[2] * inv, 0.f);
+}
+
+// Colour pass A from its fetched operands, with the operands of the next pass B fetched first.
+// No barrier here: the caller separates the passes.
+template <int AX, int AY, int AZ, int BX, int BY, int BZ>
+__device__ __forceinline__ void ctile_step(float4* sm, const Dims& d, int x0, int y0, int z0,
+                                           const float* __restrict__ st, const float* __restrict__ f,
+                                           const CPassOps& cur, CPassOps& next) {
+  ctile_fetch<BX, BY, BZ>(d, x0, y0, z0, st, f, next);
+  ctile_apply<AX, AY, AZ>(sm, cur);
 }
 
 // One Gauss-Seidel sweep of a coarse level on the tiles of tiling `shift`: stage u from zero, from
@@ -132,6 +158,12 @@ __global__ void __launch_bounds__(kCThreads)
   ctile_origin(d, blockIdx.x, shift, x0, y0, z0);
   const size_t nv = d.nv();
   const int t = int(threadIdx.x);
+  // the first pass's stencils and right-hand side, in flight during the staging
+  CPassOps first;
+  if (!reverse)
+    ctile_fetch<0, 0, 0>(d, x0, y0, z0, st, f, first);
+  else
+    ctile_fetch<1, 1, 1>(d, x0, y0, z0, st, f, first);
   const int c0x = x0 / 2 - 1, c0y = y0 / 2 - 1, c0z = z0 / 2 - 1;
   // staging: every thread first issues all its global loads (the coarser block, then the sites of
   // the staged box in natural order), then stores
@@ -195,38 +227,39 @@ __global__ void __launch_bounds__(kCThreads)
     }
   }
   __syncthreads();
+  CPassOps oa, ob;
   if (!reverse) {
-    ctile_pass<0, 0, 0>(csm, d, x0, y0, z0, st, f);
+    ctile_step<0, 0, 0, 1, 0, 0>(csm, d, x0, y0, z0, st, f, first, ob);
     __syncthreads();
-    ctile_pass<1, 0, 0>(csm, d, x0, y0, z0, st, f);
+    ctile_step<1, 0, 0, 0, 1, 0>(csm, d, x0, y0, z0, st, f, ob, oa);
     __syncthreads();
-    ctile_pass<0, 1, 0>(csm, d, x0, y0, z0, st, f);
+    ctile_step<0, 1, 0, 1, 1, 0>(csm, d, x0, y0, z0, st, f, oa, ob);
     __syncthreads();
-    ctile_pass<1, 1, 0>(csm, d, x0, y0, z0, st, f);
+    ctile_step<1, 1, 0, 0, 0, 1>(csm, d, x0, y0, z0, st, f, ob, oa);
     __syncthreads();
-    ctile_pass<0, 0, 1>(csm, d, x0, y0, z0, st, f);
+    ctile_step<0, 0, 1, 1, 0, 1>(csm, d, x0, y0, z0, st, f, oa, ob);
     __syncthreads();
-    ctile_pass<1, 0, 1>(csm, d, x0, y0, z0, st, f);
+    ctile_step<1, 0, 1, 0, 1, 1>(csm, d, x0, y0, z0, st, f, ob, oa);
     __syncthreads();
-    ctile_pass<0, 1, 1>(csm, d, x0, y0, z0, st, f);
+    ctile_step<0, 1, 1, 1, 1, 1>(csm, d, x0, y0, z0, st, f, oa, ob);
     __syncthreads();
-    ctile_pass<1, 1, 1>(csm, d, x0, y0, z0, st, f);
+    ctile_apply<1, 1, 1>(csm, ob);
   } else {
-    ctile_pass<1, 1, 1>(csm, d, x0, y0, z0, st, f);
+    ctile_step<1, 1, 1, 0, 1, 1>(csm, d, x0, y0, z0, st, f, first, ob);
     __syncthreads();
-    ctile_pass<0, 1, 1>(csm, d, x0, y0, z0, st, f);
+    ctile_step<0, 1, 1, 1, 0, 1>(csm, d, x0, y0, z0, st, f, ob, oa);
     __syncthreads();
-    ctile_pass<1, 0, 1>(csm, d, x0, y0, z0, st, f);
+    ctile_step<1, 0, 1, 0, 0, 1>(csm, d, x0, y0, z0, st, f, oa, ob);
     __syncthreads();
-    ctile_pass<0, 0, 1>(csm, d, x0, y0, z0, st, f);
+    ctile_step<0, 0, 1, 1, 1, 0>(csm, d, x0, y0, z0, st, f, ob, oa);
     __syncthreads();
-    ctile_pass<1, 1, 0>(csm, d, x0, y0, z0, st, f);
+    ctile_step<1, 1, 0, 0, 1, 0>(csm, d, x0, y0, z0, st, f, oa, ob);
     __syncthreads();
-    ctile_pass<0, 1, 0>(csm, d, x0, y0, z0, st, f);
+    ctile_step<0, 1, 0, 1, 0, 0>(csm, d, x0, y0, z0, st, f, ob, oa);
     __syncthreads();
-    ctile_pass<1, 0, 0>(csm, d, x0, y0, z0, st, f);
+    ctile_step<1, 0, 0, 0, 0, 0>(csm, d, x0, y0, z0, st, f, oa, ob);
     __syncthreads();
-    ctile_pass<0, 0, 0>(csm, d, x0, y0, z0, st, f);
+    ctile_apply<0, 0, 0>(csm, ob);
   }
   __syncthreads();
   for (int s = t; s < kCTX * kCTY * kCTZ; s += kCThreads) {
