@@ -20,6 +20,7 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <vector>
 
 #include "otm_mg_kernels.cuh"
 
@@ -58,6 +59,8 @@ struct ClDesc {
   int nc;          // unknowns of the coarsest level
   int gather_off;  // float offset of the coarsest right-hand-side gather buffer (3 nc floats)
   int tab_base;    // float offset of the plane tables (ints)
+  int ntab;        // their entries (cl_tables), copied from tab_g at the start of a call
+  const int* tab_g;
   ClLevel lv[kClMaxLevels];
   const float* f_in;  // right-hand side of the first level (global, case-major)
   float* u_out;       // its correction (global)
@@ -428,25 +431,9 @@ static __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads)
   if (threadIdx.x < kCl) rb[threadIdx.x] = int(threadIdx.x) == rank ? sm : cluster.map_shared_rank(sm, int(threadIdx.x));
   int* tab = reinterpret_cast<int*>(sm + cd.tab_base);
   const int L = cd.nlev;
-  // plane tables: owner and local plane of every plane; the ghost copies every plane feeds
-  for (int l = 0; l < L; l++) {
-    const ClLevel& V = cd.lv[l];
-    const int nz = V.d.nz;
-    for (int z = threadIdx.x; z < nz; z += blockDim.x) {
-      int c = 0;
-      while (c < kCl - 1 && z >= V.zstart[c + 1]) c++;
-      tab[V.tab_off + z] = (c << 16) | (z - V.zstart[c]);
-      int k = 0;
-      int* push = tab + V.tab_off + nz + 2 * z;
-      push[0] = push[1] = -1;
-      for (int q = 0; q < kCl && k < 2; q++) {
-        const int a = V.zstart[q], b = V.zstart[q + 1];
-        if (b == a) continue;
-        if (wrapm(a - 1, nz) == z) push[k++] = (q << 16) | 0;          // q's lower ghost
-        if (k < 2 && wrapm(b, nz) == z) push[k++] = (q << 16) | (b - a + 1);  // q's upper ghost
-      }
-    }
-  }
+  // plane tables (built on the host by cl_tables): owner and local plane of every plane, and the
+  // ghost copies every plane feeds
+  for (int i = threadIdx.x; i < cd.ntab; i += blockDim.x) tab[i] = __ldg(cd.tab_g + i);
   // the coarsest inverse is read once, late in the cycle: bring it into L2 now
   l2_prefetch_share(cd.Ainv, size_t(cd.nc) * size_t(cd.nc) * sizeof(double));
   // first level: zero correction (ghosts included) and, where it is staged, its right-hand side;
@@ -624,6 +611,36 @@ inline size_t cl_plan_try(const Dims* dims, int n, ClDesc* cd, bool first_smem) 
   const size_t bytes = size_t(off) * sizeof(float);
   if (bytes > size_t(kMaxDynSmem)) return 0;
   return bytes;
+}
+
+// The plane tables of a plan, cd->ntab ints: per level (at tab_off) the owner CTA and local plane
+// of every plane ((c << 16) | local), then for every plane the two ghost copies it feeds ((CTA <<
+// 16) | local ghost plane, -1 for none): plane z is the lower ghost (local plane 0) of the CTA
+// whose slab starts at z + 1 and the upper ghost (local plane slab + 1) of the CTA whose slab ends
+// at z, periodically. Built once per plan on the host, copied into shared memory by every call.
+inline void cl_tables(ClDesc* cd, std::vector<int>& tab) {
+  int n = 0;
+  for (int l = 0; l < cd->nlev; l++) n = std::max(n, cd->lv[l].tab_off + 3 * cd->lv[l].d.nz);
+  tab.assign(size_t(n), 0);
+  for (int l = 0; l < cd->nlev; l++) {
+    const ClLevel& V = cd->lv[l];
+    const int nz = V.d.nz;
+    for (int z = 0; z < nz; z++) {
+      int c = 0;
+      while (c < kCl - 1 && z >= V.zstart[c + 1]) c++;
+      tab[size_t(V.tab_off + z)] = (c << 16) | (z - V.zstart[c]);
+      int k = 0;
+      int* push = tab.data() + V.tab_off + nz + 2 * z;
+      push[0] = push[1] = -1;
+      for (int q = 0; q < kCl && k < 2; q++) {
+        const int a = V.zstart[q], b = V.zstart[q + 1];
+        if (b == a) continue;
+        if ((a - 1 + nz) % nz == z) push[k++] = (q << 16) | 0;           // q's lower ghost
+        if (k < 2 && b % nz == z) push[k++] = (q << 16) | (b - a + 1);   // q's upper ghost
+      }
+    }
+  }
+  cd->ntab = n;
 }
 
 // Host-side layout of the cluster part (see cl_plan_try): the first level's stencils in shared

@@ -157,7 +157,7 @@ __global__ void __launch_bounds__(256) k_conv_tiled(Dims d, const float* __restr
 #pragma unroll
   for (int tz = 0; tz < kTZ; tz++) sum[tz] = wsv[tz] = 0.f;
   const int base = H * SX * SY + (threadIdx.y + H) * SX + (threadIdx.x + H);
-#pragma unroll 2
+#pragma unroll 8
   for (int t = 0; t < tl.n; t++) {
     const float w = tl.w[t];
     const int li = base + (kFwd ? tl.doff[t] : -tl.doff[t]);

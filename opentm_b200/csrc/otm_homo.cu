@@ -312,6 +312,11 @@ otm_status Homo::build(const otm_config& c, cudaStream_t ext_stream, cudaMemPool
             cd.lv[i].rg = lv[t + i].r;
           }
           cd.Ainv = Ainv;
+          cl_tables(&cd, cl_tab_host);
+          OTM_TRY(alloc((void**)&cl_tab, cl_tab_host.size() * sizeof(int)));
+          OTM_CUDA(cudaMemcpyAsync(cl_tab, cl_tab_host.data(), cl_tab_host.size() * sizeof(int),
+                                   cudaMemcpyHostToDevice, stream));
+          cd.tab_g = cl_tab;
           cl_desc = cd;
           cluster_l = t;
           cluster_smem = bytes;

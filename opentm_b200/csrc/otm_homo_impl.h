@@ -79,6 +79,8 @@ struct Homo {
   // fine level smoothed by the tile kernels (one launch per smoothing leg); the post-smoothing
   // leg writes the preconditioned residual to the residual buffer (lv[0].r, or r16)
   bool tiled = false;
+  std::vector<int> cl_tab_host;  // plane tables of the cluster plan (kept: the copy is asynchronous)
+  int* cl_tab = nullptr;          // their device copy
   CUtensorMap fmap{};  // TMA map of the fine right-hand side (3 cases, FP32) for the tile kernels
   int tail_l = -1;          // first level handled by the single-CTA tail kernel (-1: none)
   size_t tail_smem = 0;     // its dynamic shared memory

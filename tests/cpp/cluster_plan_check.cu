@@ -79,6 +79,31 @@ static void check_stack(Dims d0) {
       CHECK(k <= 2, "level %d plane %d feeds %d ghost copies", l, z, k);
     }
   }
+  // the host-built plane tables (cl_tables): every plane's owner and local plane, and the ghost
+  // copies it feeds, as restated here
+  std::vector<int> tab;
+  cl_tables(&cd, tab);
+  CHECK(cd.ntab == tab_total && int(tab.size()) == tab_total, "plane tables: %d entries, %d expected", cd.ntab,
+        tab_total);
+  for (int l = 0; l < cd.nlev && int(tab.size()) == tab_total; l++) {
+    const ClLevel& V = cd.lv[l];
+    const int nz = V.d.nz;
+    for (int z = 0; z < nz; z++) {
+      int c = 0;
+      while (V.zstart[c + 1] <= z) c++;
+      CHECK(tab[V.tab_off + z] == ((c << 16) | (z - V.zstart[c])), "level %d plane %d: owner entry", l, z);
+      std::vector<int> want;
+      for (int q = 0; q < kCl; q++) {
+        const int a = V.zstart[q], b = V.zstart[q + 1];
+        if (a == b) continue;
+        if (wrapz(a - 1, nz) == z) want.push_back((q << 16) | 0);
+        if (wrapz(b, nz) == z) want.push_back((q << 16) | (b - a + 1));
+      }
+      while (want.size() < 2) want.push_back(-1);
+      const int* push = tab.data() + V.tab_off + nz + 2 * z;
+      CHECK(push[0] == want[0] && push[1] == want[1], "level %d plane %d: ghost pushes", l, z);
+    }
+  }
   add(cd.gather_off, 3L * cd.nc, "coarsest gather", -1);
   add(cd.tab_base, long(tab_total), "plane tables", -1);
   CHECK(tab_total <= kClMaxTab, "plane tables: %d entries", tab_total);
