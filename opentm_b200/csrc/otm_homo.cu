@@ -336,6 +336,8 @@ otm_status Homo::build(const otm_config& c, cudaStream_t ext_stream, cudaMemPool
     OTM_TRY(tile_attributes());
     // the second buffer of the sweep ping-pong (the fine correction's storage type)
     OTM_TRY(alloc(&u2, 3 * lv[0].d.nv() * (mixed ? 2 : sizeof(float))));
+    // per-tile partial sums of the tiled direction update (p . q)
+    OTM_TRY(alloc((void**)&tile_partials, size_t(tile_count(lv[0].d)) * 3 * sizeof(double)));
     tiled = true;
   }
   // coarse levels smoothed by the tile kernels: the levels between the fine level and the cluster
@@ -366,6 +368,7 @@ otm_status Homo::build(const otm_config& c, cudaStream_t ext_stream, cudaMemPool
 // {nx, ny, nz, 3 cases} of FP32 read in boxes {8, 8, 4, 3}, eight per tile.
 otm_status Homo::tile_attributes() {
   const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  OTM_CUDA(cudaFuncSetAttribute(k_tile_apply_dot, a, int(kTileSmemResid)));
   OTM_CUDA(cudaFuncSetAttribute(k_tile_sweep<kFromZero, float, float>, a, int(kTileSmemSweep)));
   OTM_CUDA(cudaFuncSetAttribute(k_tile_sweep<kFromU, float, float>, a, int(kTileSmemSweep)));
   OTM_CUDA(cudaFuncSetAttribute(k_tile_sweep<kFromUProlong, float, float>, a, int(kTileSmemProlong)));
@@ -826,7 +829,11 @@ void Homo::pcg_direction(const VT* z, const float* r, bool face, int nb) {
   const Dims d0 = lv[0].d;
   const size_t nv = d0.nv();
   launch_pdl(k_dot_rz<VT>, dim3(nb), dim3(kBlock), 0, stream, nv, r, z, partials, sc);
-  if (face)
+  // FP32 with the tile smoother: the tiled direction update (z's neighbours from shared memory)
+  if (tiled && std::is_same<VT, float>::value && !face)
+    launch_pdl(k_tile_apply_dot, dim3(tile_count(d0)), dim3(kResidThreads), kTileSmemResid, stream, d0,
+               (const float*)ks, op, (const float*)z, p, q, tile_partials, sc);
+  else if (face)
     launch_pdl(k_update_p_apply_dot<true, VT>, dim3(nb), dim3(kBlock), 0, stream, d0, ks, op, z, p, q, partials, sc);
   else
     launch_pdl(k_update_p_apply_dot<false, VT>, dim3(nb), dim3(kBlock), 0, stream, d0, ks, op, z, p, q, partials, sc);

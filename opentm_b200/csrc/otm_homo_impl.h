@@ -79,6 +79,7 @@ struct Homo {
   // fine level smoothed by the tile kernels (one launch per smoothing leg); the post-smoothing
   // leg writes the preconditioned residual to the residual buffer (lv[0].r, or r16)
   bool tiled = false;
+  double* tile_partials = nullptr;  // 3 partial sums per fine tile (k_tile_apply_dot)
   std::vector<int> cl_tab_host;  // plane tables of the cluster plan (kept: the copy is asynchronous)
   int* cl_tab = nullptr;          // their device copy
   CUtensorMap fmap{};  // TMA map of the fine right-hand side (3 cases, FP32) for the tile kernels

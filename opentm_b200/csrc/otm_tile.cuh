@@ -668,4 +668,119 @@ __global__ void __launch_bounds__(kResidThreads, 2)
   }
 }
 
+// The PCG direction update and operator product of k_update_p_apply_dot on tiles (FP32, cube
+// elements): p = (z - zbar) + beta p, q = A z + beta q (A p = A z + beta A p_old, A annihilating
+// constants), and the p . q partial sums of the tile, reduced by the last CTA into alpha = rho /
+// (p . q). z is staged like u in k_tile_resid (tiling 0, one thread per column streaming its 10
+// planes) so its 20 neighbours come from shared memory; beta == 0 (the first iteration) ignores
+// the old p and q. part: 3 doubles per tile.
+static __global__ void __launch_bounds__(kResidThreads, 2)
+    k_tile_apply_dot(Dims d, const float* __restrict__ ks, FineOp op, const float* __restrict__ z,
+                     float* __restrict__ p, float* __restrict__ q, double* part, SolveScalars* sc) {
+  unsigned char* base = tile_smem_base();
+  float4* sm = reinterpret_cast<float4*>(base + kOffSites);
+  pdl_wait();
+  if (solve_done(sc)) return;
+  int x0, y0, z0;
+  tile_origin(d, blockIdx.x, 0, x0, y0, z0);
+  const size_t nv = d.nv();
+  float be[3], zb[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    be[c] = float(sc->beta[c]);
+    zb[c] = float(sc->zmean[c]);
+  }
+  stage_tile<true, kResidThreads, false>(d, d, x0, y0, z0, ks, z, (const float*)nullptr, sm, (float4*)nullptr);
+  __syncthreads();
+  const int lx = 1 + (int(threadIdx.x) & 15), ly = 1 + (int(threadIdx.x) >> 4);
+  const size_t col = size_t(x0 + lx - 1) + size_t(d.nx) * size_t(y0 + ly - 1);
+  const size_t pl = size_t(d.nx) * d.ny;
+  float Kp[4] = {0.f, 0.f, 0.f, 0.f};
+  PlaneCoef Cp;
+  // minus the off-diagonal sums of the vertices P - 1, P, P + 1
+  float accA[3] = {0.f, 0.f, 0.f}, accB[3] = {0.f, 0.f, 0.f}, accC[3] = {0.f, 0.f, 0.f};
+  float dA = 0.f, dB = 0.f;
+  float uA[3] = {0.f, 0.f, 0.f}, uB[3] = {0.f, 0.f, 0.f};  // z of the vertices P - 1, P
+  double v[3] = {0, 0, 0};
+#pragma unroll 1
+  for (int P = 0; P < kSZ; P++) {
+    const float4* b = sm + rsite(lx, ly, P);
+    float4 nb[8];
+    nb[0] = b[-kSRow - 1];
+    nb[1] = b[-kSRow];
+    nb[2] = b[-kSRow + 1];
+    nb[3] = b[-1];
+    nb[4] = b[1];
+    nb[5] = b[kSRow - 1];
+    nb[6] = b[kSRow];
+    nb[7] = b[kSRow + 1];
+    const float4 own = b[0];
+    const float K[4] = {nb[0].w, nb[1].w, nb[3].w, own.w};
+    const float sK = (K[0] + K[1]) + (K[2] + K[3]);
+    PlaneCoef C;
+    C.make(K, op);
+    float dC = 0.f;
+    if (P + 1 <= kTZ) {  // vertex P + 1: lower element plane P
+#pragma unroll
+      for (int c = 0; c < 3; c++) accC[c] = 0.f;
+      sub_plane(accC, C, nb);
+      dC = sK;
+    }
+    if (P >= 1 && P <= kTZ) {  // vertex P: in-plane corners and its own value
+      sub_inplane(accB, Kp, K, op, nb);
+      dB += sK;
+      uB[0] = own.x;
+      uB[1] = own.y;
+      uB[2] = own.z;
+    }
+    if (P >= 2) {  // vertex P - 1: upper element plane P - 1, then the update
+      sub_plane(accA, Cp, nb);
+      const float diag = op.c0 * dA;
+      const size_t g = col + size_t(z0 + P - 2) * pl;
+      float po[3], qo[3];  // all loads of the vertex before its stores
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        po[c] = be[c] != 0.f ? p[c * nv + g] : 0.f;
+        qo[c] = be[c] != 0.f ? q[c * nv + g] : 0.f;
+      }
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        float pc = uA[c] - zb[c], qc = diag * uA[c] - accA[c];  // accA = -(off-diagonal sum)
+        if (be[c] != 0.f) {
+          pc += be[c] * po[c];
+          qc += be[c] * qo[c];
+        }
+        p[c * nv + g] = pc;
+        q[c * nv + g] = qc;
+        v[c] += double(pc) * qc;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      accA[c] = accB[c];
+      accB[c] = accC[c];
+      uA[c] = uB[c];
+    }
+    dA = dB;
+    dB = dC;
+#pragma unroll
+    for (int q4 = 0; q4 < 4; q4++) Kp[q4] = K[q4];
+    Cp = C;
+  }
+  double* red = reinterpret_cast<double*>(sm);  // the tile is no longer read
+  __syncthreads();
+  block_reduce_f64<3>(v, red);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int i = 0; i < 3; i++) part[size_t(blockIdx.x) * 3 + i] = v[i];
+  if (last_block(&sc->counter[T_PQ])) {
+    double t[3];
+    reduce_partials<3>(part, int(gridDim.x), t, red);
+    if (threadIdx.x == 0) {
+      for (int c = 0; c < 3; c++) sc->alpha[c] = t[c] != 0.0 ? sc->rz[c] / t[c] : 0.0;
+      sc->counter[T_PQ] = 0;
+    }
+  }
+}
+
 }  // namespace otm
