@@ -214,14 +214,35 @@ __device__ __forceinline__ void dot_rz_body(size_t nv, const float* __restrict__
 #pragma unroll
     for (int c = 0; c < 3; c++) zs[c] = sc->xscale[c];
   double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  for (size_t i = size_t(blk) * blockDim.x + threadIdx.x; i < nv; i += size_t(nblk) * blockDim.x) {
+  if (!kScaled && (nv & 3) == 0) {
+    // FP32 z: four consecutive vertices per step with 16-byte loads (case planes are 16-byte aligned
+    // when nv is a multiple of 4)
+    const size_t n4 = nv >> 2;
+    const float4* r4 = reinterpret_cast<const float4*>(r);
+    const float4* z4 = reinterpret_cast<const float4*>(z);
+    for (size_t i = size_t(blk) * blockDim.x + threadIdx.x; i < n4; i += size_t(nblk) * blockDim.x) {
 #pragma unroll
-    for (int c = 0; c < 3; c++) {
-      const double rc = r[c * nv + i];
-      const double zc = kScaled ? zs[c] * double(ld(z + c * nv + i)) : double(ld(z + c * nv + i));
-      v[c] += rc * zc;
-      v[3 + c] += zc;
-      v[6 + c] += rc;
+      for (int c = 0; c < 3; c++) {
+        const float4 a = r4[c * n4 + i], b = __ldg(z4 + c * n4 + i);
+        const double ra[4] = {a.x, a.y, a.z, a.w}, zb[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          v[c] += ra[e] * zb[e];
+          v[3 + c] += zb[e];
+          v[6 + c] += ra[e];
+        }
+      }
+    }
+  } else {
+    for (size_t i = size_t(blk) * blockDim.x + threadIdx.x; i < nv; i += size_t(nblk) * blockDim.x) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        const double rc = r[c * nv + i];
+        const double zc = kScaled ? zs[c] * double(ld(z + c * nv + i)) : double(ld(z + c * nv + i));
+        v[c] += rc * zc;
+        v[3 + c] += zc;
+        v[6 + c] += rc;
+      }
     }
   }
   block_reduce_f64<9>(v, smem);
@@ -400,13 +421,41 @@ __device__ __forceinline__ void update_xr_body(size_t nv, float* __restrict__ x,
 #pragma unroll
   for (int c = 0; c < 3; c++) al[c] = float(sc->alpha[c]);
   double v[3] = {0, 0, 0};
-  for (size_t i = size_t(blk) * blockDim.x + threadIdx.x; i < nv; i += size_t(nblk) * blockDim.x) {
+  if ((nv & 3) == 0) {
+    // four consecutive vertices per step with 16-byte accesses
+    const size_t n4 = nv >> 2;
+    float4* x4 = reinterpret_cast<float4*>(x);
+    float4* r4 = reinterpret_cast<float4*>(r);
+    const float4* p4 = reinterpret_cast<const float4*>(p);
+    const float4* q4 = reinterpret_cast<const float4*>(q);
+    for (size_t i = size_t(blk) * blockDim.x + threadIdx.x; i < n4; i += size_t(nblk) * blockDim.x) {
 #pragma unroll
-    for (int c = 0; c < 3; c++) {
-      x[c * nv + i] += al[c] * p[c * nv + i];
-      const float rc = r[c * nv + i] - al[c] * q[c * nv + i];
-      r[c * nv + i] = rc;
-      v[c] += double(rc) * rc;
+      for (int c = 0; c < 3; c++) {
+        const size_t j = c * n4 + i;
+        float4 xv = x4[j], rv = r4[j];
+        const float4 pv = p4[j], qv = q4[j];
+        xv.x += al[c] * pv.x;
+        xv.y += al[c] * pv.y;
+        xv.z += al[c] * pv.z;
+        xv.w += al[c] * pv.w;
+        rv.x -= al[c] * qv.x;
+        rv.y -= al[c] * qv.y;
+        rv.z -= al[c] * qv.z;
+        rv.w -= al[c] * qv.w;
+        x4[j] = xv;
+        r4[j] = rv;
+        v[c] += double(rv.x) * rv.x + double(rv.y) * rv.y + double(rv.z) * rv.z + double(rv.w) * rv.w;
+      }
+    }
+  } else {
+    for (size_t i = size_t(blk) * blockDim.x + threadIdx.x; i < nv; i += size_t(nblk) * blockDim.x) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        x[c * nv + i] += al[c] * p[c * nv + i];
+        const float rc = r[c * nv + i] - al[c] * q[c * nv + i];
+        r[c * nv + i] = rc;
+        v[c] += double(rc) * rc;
+      }
     }
   }
   block_reduce_f64<3>(v, smem);
