@@ -344,8 +344,10 @@ __device__ __forceinline__ float3 prolong_site(const float4* cb, int ux, int uy,
 }
 
 // The prolongation at the 4 fine sites xs .. xs + 3 of a row (xs even, unwrapped), reading the 3
-// coarse columns under them once per coarse row instead of 8 coarse sites per fine site; the
-// per-site expression and weights are those of prolong_site.
+// coarse columns under them once per coarse row instead of 8 coarse sites per fine site. The
+// trilinear weights are separable: each coarse column is first interpolated over (y, z), then the
+// even sites take their column's value and the odd ones the mean of two columns (the weights of
+// prolong_site, summed in another order).
 __device__ __forceinline__ void prolong_quad(const float4* cb, int xs, int uy, int uz, int c0x, int c0y, int c0z,
                                              float3 (&o)[4]) {
   const int ax = (xs >> 1) - c0x;  // coarse columns ax, ax + 1, ax + 2
@@ -355,27 +357,18 @@ __device__ __forceinline__ void prolong_quad(const float4* cb, int xs, int uy, i
   const float wy0 = 1.f - wy1, wz0 = 1.f - wz1;
   const float4* rows[4] = {cb + (ay0 + kCY * az0) * kCX + ax, cb + (ay1 + kCY * az0) * kCX + ax,
                            cb + (ay0 + kCY * az1) * kCX + ax, cb + (ay1 + kCY * az1) * kCX + ax};
-  float4 v[4][3];
+  float3 col[3];
 #pragma unroll
-  for (int r = 0; r < 4; r++)
-#pragma unroll
-    for (int a = 0; a < 3; a++) v[r][a] = rows[r][a];
-#pragma unroll
-  for (int e = 0; e < 4; e++) {
-    // site xs + e: coarse columns (e / 2) and (e / 2 + (e & 1)), weights 1/0 or 1/2, 1/2
-    const int a0 = e >> 1, a1 = (e >> 1) + (e & 1);
-    const float wx1 = (e & 1) ? 0.5f : 0.f, wx0 = 1.f - wx1;
-    float xr[4][3];
-#pragma unroll
-    for (int r = 0; r < 4; r++) {
-      xr[r][0] = wx0 * v[r][a0].x + wx1 * v[r][a1].x;
-      xr[r][1] = wx0 * v[r][a0].y + wx1 * v[r][a1].y;
-      xr[r][2] = wx0 * v[r][a0].z + wx1 * v[r][a1].z;
-    }
-    o[e].x = wz0 * (wy0 * xr[0][0] + wy1 * xr[1][0]) + wz1 * (wy0 * xr[2][0] + wy1 * xr[3][0]);
-    o[e].y = wz0 * (wy0 * xr[0][1] + wy1 * xr[1][1]) + wz1 * (wy0 * xr[2][1] + wy1 * xr[3][1]);
-    o[e].z = wz0 * (wy0 * xr[0][2] + wy1 * xr[1][2]) + wz1 * (wy0 * xr[2][2] + wy1 * xr[3][2]);
+  for (int a = 0; a < 3; a++) {
+    const float4 v0 = rows[0][a], v1 = rows[1][a], v2 = rows[2][a], v3 = rows[3][a];
+    col[a].x = wz0 * (wy0 * v0.x + wy1 * v1.x) + wz1 * (wy0 * v2.x + wy1 * v3.x);
+    col[a].y = wz0 * (wy0 * v0.y + wy1 * v1.y) + wz1 * (wy0 * v2.y + wy1 * v3.y);
+    col[a].z = wz0 * (wy0 * v0.z + wy1 * v1.z) + wz1 * (wy0 * v2.z + wy1 * v3.z);
   }
+  o[0] = col[0];
+  o[1] = make_float3(0.5f * (col[0].x + col[1].x), 0.5f * (col[0].y + col[1].y), 0.5f * (col[0].z + col[1].z));
+  o[2] = col[1];
+  o[3] = make_float3(0.5f * (col[1].x + col[2].x), 0.5f * (col[1].y + col[2].y), 0.5f * (col[1].z + col[2].z));
 }
 
 // Stages the tile's sites {u_case0, u_case1, u_case2, k_e} in shared memory (parity-split order
