@@ -740,14 +740,46 @@ static __global__ void __launch_bounds__(kBlock) k_update_x64r(size_t nv, double
 #pragma unroll
   for (int c = 0; c < 3; c++) al[c] = sc->alpha[c];
   double v[3] = {0, 0, 0}, mx[3] = {0, 0, 0};
-  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nv; i += size_t(gridDim.x) * blockDim.x) {
+  if ((nv & 3) == 0) {
+    // four consecutive vertices per step: 16-byte accesses to the FP32 vectors, two to x64
+    const size_t n4 = nv >> 2;
+    float4* r4 = reinterpret_cast<float4*>(r);
+    const float4* p4 = reinterpret_cast<const float4*>(p);
+    const float4* q4 = reinterpret_cast<const float4*>(q);
+    double2* x2 = reinterpret_cast<double2*>(x64);
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n4; i += size_t(gridDim.x) * blockDim.x) {
 #pragma unroll
-    for (int c = 0; c < 3; c++) {
-      x64[c * nv + i] += al[c] * double(p[c * nv + i]);
-      const float rc = r[c * nv + i] - float(al[c]) * q[c * nv + i];
-      r[c * nv + i] = rc;
-      v[c] += double(rc) * rc;
-      mx[c] = fmax(mx[c], fabs(double(rc)));
+      for (int c = 0; c < 3; c++) {
+        const size_t j = c * n4 + i;
+        const float4 pv = p4[j], qv = q4[j];
+        float4 rv = r4[j];
+        double2 xa = x2[2 * j], xb = x2[2 * j + 1];
+        xa.x += al[c] * double(pv.x);
+        xa.y += al[c] * double(pv.y);
+        xb.x += al[c] * double(pv.z);
+        xb.y += al[c] * double(pv.w);
+        x2[2 * j] = xa;
+        x2[2 * j + 1] = xb;
+        const float a = float(al[c]);
+        rv.x -= a * qv.x;
+        rv.y -= a * qv.y;
+        rv.z -= a * qv.z;
+        rv.w -= a * qv.w;
+        r4[j] = rv;
+        v[c] += double(rv.x) * rv.x + double(rv.y) * rv.y + double(rv.z) * rv.z + double(rv.w) * rv.w;
+        mx[c] = fmax(mx[c], fmax(fmax(fabs(double(rv.x)), fabs(double(rv.y))), fmax(fabs(double(rv.z)), fabs(double(rv.w)))));
+      }
+    }
+  } else {
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nv; i += size_t(gridDim.x) * blockDim.x) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        x64[c * nv + i] += al[c] * double(p[c * nv + i]);
+        const float rc = r[c * nv + i] - float(al[c]) * q[c * nv + i];
+        r[c * nv + i] = rc;
+        v[c] += double(rc) * rc;
+        mx[c] = fmax(mx[c], fabs(double(rc)));
+      }
     }
   }
   block_reduce_f64<3>(v, smem);
