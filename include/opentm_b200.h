@@ -56,8 +56,8 @@ typedef enum otm_smoother {
   OTM_SMOOTHER_TILED = 1  /* fine level in 16 x 16 x 8 shared-memory tiles, one launch per sweep:
                              colour-ordered Gauss-Seidel inside a tile, the tile halo held at the
                              sweep's starting values, consecutive sweeps on two tilings shifted by
-                             half a tile; used with the PCG solver when nx, ny are multiples of 16
-                             and nz of 8, else the colour passes */
+                             half a tile; used with the PCG solver, at least 2 sweeps in each leg,
+                             and nx, ny multiples of 16 and nz of 8, else the colour passes */
 } otm_smoother;
 
 typedef enum otm_solver {
@@ -100,7 +100,7 @@ typedef struct otm_solve_stats {
   int coarsest_reso[3];   /* coarsest level cells per axis */
   int cluster_level;      /* first level of the one-launch cluster cycle, -1 when not used */
   int smoother;           /* otm_smoother the fine level runs with (OTM_SMOOTHER_TILED only with the PCG
-                             solver and nx, ny multiples of 16, nz of 8) */
+                             solver, at least 2 sweeps per leg and nx, ny multiples of 16, nz of 8) */
 } otm_solve_stats;
 
 /* Event-timed fine-level smoother sweeps collected while profile != 0. */
