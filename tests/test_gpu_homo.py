@@ -360,6 +360,15 @@ def test_vcycle_solver_keeps_color_passes():
     assert H.stats().smoother == 1
 
 
+def test_single_sweep_legs_keep_color_passes():
+    """With one smoothing sweep per leg the tilings of the tile smoother could not alternate (the
+    post leg mirrors the pre leg), so V(1,1) uses the colour passes on every level."""
+    k, _ = random_k((32, 32, 32), seed=6)
+    H, C, E, sens = gpu_run(k, tol=1e-7, pre=1, post=1, smoother="tiled")
+    assert H.stats().smoother == 0
+    check_against_oracle(k, C, E, sens)
+
+
 def test_tiled_graphs_and_repeat_bitwise():
     k, _ = random_k((32, 32, 32), seed=72)
     _, C1, E1, s1 = gpu_run(k, use_graphs=True, smoother="tiled")
